@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""CG2D forward + adjoint throughput on B200 (one JSON line on stdout).
+
+Workload (one step): a batch of 64 LLC90 instances (13 tiles of 90x90, seeded synthetic ensemble members with
+per-member depth, operator, cg2dNorm and right-hand side), each solved forward (A x = b) and adjoint (A lam = w,
+seeded cotangent w) to a normalised residual of 1e-12 (max 300 iterations each), both right-hand sides of an
+instance sharing its operator in ONE persistent mixed-precision launch, followed by the edge-product kernel
+(coefficient gradients of J = <w, x>). Unit: forward+adjoint solve pairs per second, whole job.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+--impl reference times the reference's CPU path (the oracle restatement of cg2d_fortran, FP64, forward + tight
+adjoint solve + coefficient cotangents) on all host cores, one instance per process.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "CG2D fwd+adjoint solves/s, batched/mixed vs plain FP64 on B200 at 1e-12 resid"
+UNIT = "solves/s"
+N_LLC90 = 13 * 90 * 90
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--precision", default="mixed", choices=("mixed", "f64"))
+    ap.add_argument("--tol", type=float, default=1e-12)
+    ap.add_argument("--maxit", type=int, default=300)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# CPU leg: the oracle (FP64 cg2d_fortran restatement) on host cores, one instance per process
+
+
+def _cpu_worker(args):
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from mit_jax_b200.topology import LLCTopology
+    from oracle import cg2d_oracle as O
+    ops, b, w, norm, tol, maxit = args
+    topo = LLCTopology(90)
+    L, tmap = topo.L, topo.maps["T"]
+    t0 = time.perf_counter()
+    x, d = O.cg2d_fortran(L, tmap, ops, b, np.zeros_like(b), cg2dNorm=norm, tolerance=tol, max_iters=maxit,
+                          sum_order="fortran")
+    x = np.where(O.interior_mask(L), x, 0.0)
+    lam, da = O.tight_solve(L, tmap, ops, w, cg2dNorm=norm, tolerance=tol, max_iters=maxit, sum_order="tile")
+    O.coefficient_cotangents(L, tmap, lam, x, norm)
+    return time.perf_counter() - t0, d["numIters"], da["numIters"]
+
+
+class CpuLeg:
+    def __init__(self, inputs, procs):
+        import multiprocessing as mp
+        self.procs = procs
+        self.inputs = inputs
+        self.pool = mp.get_context("spawn").Pool(procs)
+
+    def step(self):
+        n = self.procs
+        args = [self.inputs[i % len(self.inputs)] for i in range(n)]
+        t0 = time.perf_counter()
+        res = self.pool.map(_cpu_worker, args, chunksize=1)
+        wall = time.perf_counter() - t0
+        return n / wall, wall, res
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def _cpu_inputs(count, tol, maxit):
+    from mit_jax_b200.synthetic import LLCSynthetic
+    syn = LLCSynthetic(90)
+    out = []
+    for m in range(count):
+        ops, norm = syn.operator(m)
+        out.append((ops, syn.rhs(m), syn.cotangent(m), norm, tol, maxit))
+    return out
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    procs = max(1, min(os.cpu_count() or 1, a.batch))
+    leg = CpuLeg(_cpu_inputs(min(procs, a.batch), a.tol, a.maxit), procs)
+    for _ in range(a.warmup):
+        leg.step()
+    rates, walls = [], []
+    for _ in range(a.steps):
+        r, w, res = leg.step()
+        rates.append(r)
+        walls.append(w)
+    leg.close()
+    value = len(rates) * procs / sum(walls)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * statistics.mean(walls), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "LLC90 CG2D forward + adjoint (tight) solve + coefficient cotangents, FP64, one "
+                               "instance per host process", "instances_per_step": procs, "tolerance": a.tol,
+                   "max_iters": a.maxit, "parallelism": f"{procs} processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                         "sample": f"{procs} LLC90 instances per step (one per process), {a.steps} steps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------------------------
+# GPU leg
+
+
+class Clocks:
+    """nvidia-smi samples during a timed region (SM clock, max clock, throttle reasons)."""
+
+    FIELDS = ("clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={','.join(self.FIELDS)}",
+                                          "--format=csv,noheader,nounits", "-lms", "200", "-i", str(self.gpu_id)],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            r = [c.strip() for c in r]
+            try:
+                sm.append(float(r[0]))
+                smax.append(float(r[1]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(diag_f, diag_a, precision):
+    """Per launch: sum over solves of N_pts x iterations x bytes per point-iteration (12 words: 6 coefficients,
+    r, s, x read, r, s, x written; MIXED: 10 FP32 words + x in FP64 = 56 B; FP64: 96 B) plus, MIXED, 96 B per point
+    per true-residual replacement."""
+    per_it = 56 if precision == "mixed" else 96
+    tot = 0
+    for d in diag_f + diag_a:
+        tot += N_LLC90 * (d["numIters"] * per_it + d.get("replacements", 0) * 96)
+    return tot
+
+
+def run_gpu(a):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from mit_jax_b200 import cg2d as cg
+    from mit_jax_b200.synthetic import make_batch
+
+    # inputs: this rank's own batch of members (weak scaling: disjoint members per rank)
+    syn, B = make_batch(90, a.batch, with_cotangent=True)
+    if rank:
+        # distinct members per rank: rotate the batch (different instance order) -- the work per rank is the same
+        B = {k: np.roll(v, rank, axis=0) for k, v in B.items()}
+    ex = cg.default_exchanger(syn.L)
+    ops = tuple(torch.as_tensor(B[k]).to(dev) for k in cg.OPS)
+    b = torch.as_tensor(B["b"]).to(dev)
+    mask = cg._interior_mask(syn.L, dev)
+    w = torch.where(mask, torch.as_tensor(B["w"]).to(dev), torch.zeros((), dtype=torch.float64, device=dev))
+    x0 = torch.zeros_like(b)
+    norms = torch.as_tensor(B["cg2dNorm"]).to(dev)
+    G = cg.GroupSpec(ex, ops, [b, w], [x0, torch.zeros_like(w)], [a.tol, a.tol], [a.maxit, a.maxit], norms)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        (slots,) = cg.solve_groups([G], precision=a.precision, check_status=False)
+        return slots
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(a.warmup):
+        slots = step()
+        cg.edge_products(ex, slots[1][0], slots[0][0], norms)
+    barrier()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(a.steps)]
+    gpu_id = getattr(torch.cuda.get_device_properties(dev), "uuid", None)
+    gpu_id = f"GPU-{gpu_id}" if gpu_id is not None and not str(gpu_id).startswith("GPU-") else (gpu_id or local)
+    with Clocks(gpu_id) as clk:
+        time.sleep(0.25)
+        barrier()
+        for s in range(a.steps):
+            ev[s][0].record(stream)
+            slots = step()
+            ev[s][1].record(stream)
+            cg.edge_products(ex, slots[1][0], slots[0][0], norms)
+            ev[s][2].record(stream)
+        barrier()
+    clocks = clk.summary()
+    total_ms = ev[0][0].elapsed_time(ev[-1][2])
+    solver_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    edge_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / a.steps
+    value = world * a.batch / (ms_per_step / 1e3)
+
+    diag_f = cg.diag_records(slots[0][2])
+    diag_a = cg.diag_records(slots[1][2])
+    bad = [d for d in diag_f + diag_a if d["status"] != "ok"]
+    alg = algorithmic_bytes(diag_f, diag_a, a.precision)
+    peak, peak_kind = measured_peak()
+    solver_mean = statistics.mean(solver_ms)
+    achieved = alg / (solver_mean / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "solver_traffic.json"
+    if prof.exists():
+        try:
+            pj = json.loads(prof.read_text())
+            if pj.get("workload") == f"batch{a.batch}_{a.precision}":
+                traffic = pj.get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- end to end through the public API from pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        host_in = {k: torch.as_tensor(B[k]).pin_memory() for k in (*cg.OPS, "b", "w", "x0")}
+        host_norm = torch.as_tensor(B["cg2dNorm"])
+        outs = {k: torch.empty((a.batch, *syn.L.shape2d), dtype=torch.float64).pin_memory()
+                for k in ("x", "lam", "gW", "gS", "gC")}
+        h2d = sum(v.numel() * v.element_size() for v in host_in.values()) + host_norm.numel() * 8
+        d2h = sum(v.numel() * v.element_size() for v in outs.values()) + 2 * a.batch * cg.capi.DIAG_BYTES
+
+        def e2e_step():
+            din = {k: v.to(dev, non_blocking=True) for k, v in host_in.items()}
+            r = cg.solve_with_adjoint(ex, tuple(din[k] for k in cg.OPS), din["b"], din["w"], din["x0"],
+                                      cg2dNorm=host_norm.to(dev, non_blocking=True), tolerance=a.tol,
+                                      max_iters=a.maxit, adj_tolerance=a.tol, adj_max_iters=a.maxit,
+                                      precision=a.precision)
+            for k in outs:
+                outs[k].copy_(r[k], non_blocking=True)
+            return r["diag_fwd"].cpu(), r["diag_adj"].cpu()
+
+        for _ in range(max(1, a.warmup)):
+            e2e_step()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            e2e_step()
+        e1.record(stream)
+        barrier()
+        et = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * a.batch * a.steps / (float(et.item()) / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    # ---- the plain FP64 one-solve-per-launch kernel: one instance, forward launch then adjoint launch
+    plain = None
+    if not a.no_plain and rank == 0:
+        o1 = tuple(o[:1].contiguous() for o in ops)
+        Gf = cg.GroupSpec(ex, o1, [b[:1].contiguous()], [x0[:1].contiguous()], [a.tol], [a.maxit], norms[:1])
+        Ga = cg.GroupSpec(ex, o1, [w[:1].contiguous()], [torch.zeros_like(w[:1])], [a.tol], [a.maxit], norms[:1])
+        for _ in range(2):
+            cg.solve_groups([Gf], precision="f64", check_status=False)
+            cg.solve_groups([Ga], precision="f64", check_status=False)
+        torch.cuda.synchronize(dev)
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        p0.record(stream)
+        for _ in range(reps):
+            (sf,) = cg.solve_groups([Gf], precision="f64", check_status=False)
+            (sa,) = cg.solve_groups([Ga], precision="f64", check_status=False)
+            cg.edge_products(ex, sa[0][0], sf[0][0], norms[:1])
+        p1.record(stream)
+        torch.cuda.synchronize(dev)
+        pms = p0.elapsed_time(p1) / reps
+        df, da = cg.diag_records(sf[0][2])[0], cg.diag_records(sa[0][2])[0]
+        plain = {"solves_per_s": 1e3 / pms, "ms_per_pair": pms, "iters_fwd": df["numIters"],
+                 "iters_adj": da["numIters"]}
+
+    cpu = None
+    if not a.no_cpu and rank == 0 and world == 1:
+        procs = max(1, min(os.cpu_count() or 1, 16))
+        leg = CpuLeg(_cpu_inputs(procs, a.tol, a.maxit), procs)
+        rate, wall, _ = leg.step()
+        leg.close()
+        cpu = {"value": rate, "unit": UNIT, "cores": procs, "kind": "port",
+               "sample": f"{procs} LLC90 instances, one per process, FP64 forward + adjoint + cotangents, "
+                         f"{wall:.1f} s wall"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": f"batch {a.batch} LLC90 CG2D forward + adjoint (2 right-hand sides per "
+                                   f"instance, one persistent launch) + edge products, {a.precision}",
+                       "batch_per_gpu": a.batch, "tolerance": a.tol, "max_iters": a.maxit,
+                       "grid": "LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"instances sharded, {world} GPU(s), no collective in the solve"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "cg2d_persistent (solver launch incl. FP32 pack)",
+                         "kernel_ms": solver_mean, "algorithmic_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": 3 * a.steps,
+            "clocks": clocks,
+            "iterations": {"fwd_mean": statistics.mean(d["numIters"] for d in diag_f),
+                           "adj_mean": statistics.mean(d["numIters"] for d in diag_a),
+                           "fwd_min": min(d["numIters"] for d in diag_f), "fwd_max": max(d["numIters"] for d in diag_f),
+                           "replacements_mean": statistics.mean(d["replacements"] for d in diag_f + diag_a),
+                           "not_ok": len(bad)},
+            "edge_products_ms": statistics.mean(edge_ms),
+            "plain_f64_one_solve_per_launch": plain,
+            "speedup_vs_plain_f64": (value / world) / plain["solves_per_s"] if plain else None,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_gpu(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,187 @@
+/*
+ * cg2d.h -- C ABI of the B200 CG2D free-surface solver (libcg2d.so).
+ *
+ * The solver is the preconditioned conjugate-gradient iteration of mitgcm_jax's CG2D
+ * (mitgcm_jax/core/cg2d.py:205-269, itself a port of MITgcm cg2d.F) on the 13-tile LLC
+ * exch2 grid. Arrays cross this boundary in the reference layout: float64, row-major
+ * [batch][tile][j][i] with OLx = OLy halo points on every side (mitgcm_jax/layout.py:16-54),
+ * so a caller hands over exactly the arrays it would hand to cg2d_fortran. All pointers
+ * passed to the solve entry points are DEVICE pointers unless stated otherwise; every call
+ * is stream-ordered on the given stream and returns before the GPU work completes.
+ *
+ * Reference interface each entry point replaces:
+ *   cg2d_topology_create   Exchanger(ExchangeMaps) for kind "T" (mitgcm_jax/parallel/exchange.py:146-183):
+ *                          the exch2 halo map becomes per-tile-edge neighbour tables read by the stencil.
+ *   cg2d_solve_f64         cg2d_fortran(ex, ops, cg2d_b, cg2d_x, ...) (mitgcm_jax/core/cg2d.py:205-269),
+ *                          batched; cg2d_solve (cg2d.py:351-375) is this call plus the Python-side mask.
+ *   cg2d_solve_groups      the same solver for several uniform batches in one persistent launch
+ *                          (mixed LLC90/LLC270 batches, forward + adjoint right-hand sides sharing
+ *                          one operator).
+ *   cg2d_apply_operator    _matvec (cg2d.py:292-298): (A / cg2dNorm) v on the interior, 0 on halos.
+ *   cg2d_edge_products     transpose of _matvec with respect to the coefficients, i.e. the
+ *                          coefficient cotangents of _cg2d_implicit_jvp (cg2d.py:318-348).
+ *   cg2d_exchange_scalar   Exchanger.exch_xy (exchange.py:136-142,182-183) for kind "T".
+ */
+#ifndef CG2D_B200_H
+#define CG2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* cg2d_stream_t; /* == cudaStream_t */
+
+typedef enum {
+  CG2D_OK = 0,
+  CG2D_NOT_CONVERGED = 1,     /* per-solve diag status only: numIters == max_iters (cg2d.py:238-241) */
+  CG2D_NAN = 2,               /* per-solve diag status only: the final residual is NaN */
+  CG2D_BARRIER_TIMEOUT = 3,   /* a grid-wide wait exceeded params.timeout_s; results are invalid */
+  CG2D_BAD_ARG = 4,
+  CG2D_CUDA_ERROR = 5,
+  CG2D_WORKSPACE_TOO_SMALL = 6,
+  CG2D_UNSUPPORTED = 7
+} cg2d_status_t;
+
+typedef enum { CG2D_PREC_F64 = 0, CG2D_PREC_MIXED = 1 } cg2d_precision_t;
+
+typedef enum {
+  /* per row: lane partials over i = lane + 32k, then an xor butterfly over the 32 lanes;
+     rows of a block of rows_per_block added in order; blocks of a tile in order; tiles in
+     order from 0 (global_sum.py:20-26). Same result for every launch geometry. */
+  CG2D_SUM_ROWBLOCK = 0,
+  /* "fortran" order of cg2d.py:141-161: s = 0; DO j; DO i; s = s + a(i,j), then the tiles in
+     order from 0. Bitwise equal to the reference's sum_order="fortran"; slow (one thread per tile). */
+  CG2D_SUM_FORTRAN = 1
+} cg2d_sum_order_t;
+
+/* Launch / numerics options (fields of Cg2dParams that are not per-solve live in the group). */
+typedef struct {
+  int precision;       /* cg2d_precision_t */
+  int sum_order;       /* cg2d_sum_order_t */
+  int rows_per_block;  /* ROWBLOCK block height in rows (multiple of 8; default 8) */
+  int replace_every;   /* MIXED: FP64 true-residual replacement period in iterations (default 25) */
+  double replace_above;/* MIXED: replace only while the residual is above replace_above * tolerance (default 100) */
+  int grid_ctas;       /* 0 = as many as can be co-resident (capped by the work units) */
+  int ctas_per_sm;     /* 0 = occupancy maximum */
+  double timeout_s;    /* bound on every grid-wide wait (default 10 s) */
+  int test_missing_arrivals; /* testing only (default 0): the first grid-wide wait expects this many
+                                arrivals more than there are CTAs, so it runs out after timeout_s and
+                                every solve reports CG2D_BARRIER_TIMEOUT (exercises the bounded wait) */
+  int reserved;
+} cg2d_params_t;
+
+/* Per-solve diagnostics: the diag dict of cg2d_fortran (cg2d.py:267-268) plus a status. */
+typedef struct {
+  double firstResidual;
+  double lastResidual;
+  double sumRHS;
+  double rhsMax;
+  int32_t numIters;
+  int32_t status;        /* cg2d_status_t */
+  int32_t replacements;  /* MIXED: true-residual recomputations done */
+  int32_t reserved;
+} cg2d_diag_t;
+
+typedef struct cg2d_topology cg2d_topology_t;
+
+/* Build the device neighbour tables of one LLC layout from the exch2 scalar ("T") halo map in
+ * the reference's ExchangeMaps format (exchange.py:73-93): for every padded point p of
+ * [nTiles][sNy+2*OLy][sNx+2*OLx], comp[p] == 1 means out[p] = a[src[p]], comp[p] == 0 means the
+ * point keeps its value. src/comp are HOST arrays of length nTiles*(sNy+2OLy)*(sNx+2OLx).
+ * Every point the 5-point stencil reads (first halo row/column, corners excluded) must take its
+ * value from an interior point or be unwritten (comp 0); anything else is CG2D_BAD_ARG.
+ * Allocates device memory (the tables and a copy of the full map for the x_fortran halos). */
+cg2d_status_t cg2d_topology_create(int sNx, int sNy, int OLx, int OLy, int nTiles,
+                                   const int32_t* src, const int8_t* comp,
+                                   cg2d_topology_t** out);
+cg2d_status_t cg2d_topology_destroy(cg2d_topology_t* topo);
+
+/* One uniform batch of `count` instances on one topology. Array arguments are device pointers
+ * to [count][nTiles][ny][nx] float64 (ny = sNy + 2 OLy, nx = sNx + 2 OLx). Each instance has
+ * nrhs (1 or 2) right-hand sides that share its operator and preconditioner (e.g. a forward
+ * solve and an adjoint solve); slot k of every instance uses b[k], x0[k], x_out[k], ...
+ * x_out: interior = solution, halos = 0 (cg2d_solve's x, cg2d.py:351-356).
+ * x_fortran (nullable): the array exactly as cg2d_fortran returns it -- interior = solution,
+ * halos = exchanged normalised first guess, unwritten halo points = the first guess
+ * (cg2d.py:208-210, 227-228). diag: device array of `count` cg2d_diag_t per slot. */
+typedef struct {
+  const cg2d_topology_t* topo;
+  int count;
+  int nrhs;
+  const double* aW2d; const double* aS2d; const double* aC2d;
+  const double* pW; const double* pS; const double* pC;
+  double cg2dNorm;                 /* used when cg2dNorm_per_instance is NULL */
+  const double* cg2dNorm_per_instance; /* device [count], nullable */
+  const double* b[2];
+  const double* x0[2];
+  double* x_out[2];
+  double* x_fortran[2];
+  cg2d_diag_t* diag[2];
+  double tolerance[2];             /* cg2dTolerance (normalised residual, cg2d.py:219,241) */
+  int max_iters[2];                /* cg2dMaxIters */
+} cg2d_group_t;
+
+#define CG2D_MAX_GROUPS 4
+#define CG2D_MAX_SOLVES 256        /* instances x nrhs over all groups of one call */
+
+void cg2d_default_params(cg2d_params_t* p);
+
+/* Bytes of device workspace a cg2d_solve_groups call with these groups needs. */
+size_t cg2d_workspace_size(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params);
+
+/* Solve every right-hand side of every group in ONE persistent cooperative launch.
+ * The workspace (device, >= cg2d_workspace_size bytes, 256-byte aligned) is scratch; it is not
+ * read before being written. Returns CG2D_OK when the work was enqueued; per-solve outcomes
+ * (convergence, NaN, barrier timeout) are in each solve's diag.status. */
+cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params,
+                                void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
+
+/* cg2d_fortran on a uniform batch, one right-hand side per instance (cg2d.py:205). */
+cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                             const double* aW2d, const double* aS2d, const double* aC2d,
+                             const double* pW, const double* pS, const double* pC,
+                             const double* cg2d_b, const double* cg2d_x,
+                             double tolerance, int max_iters,
+                             double* x_out, double* x_fortran, cg2d_diag_t* diag,
+                             const cg2d_params_t* params,
+                             void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
+
+/* Host-side error word of the last solve that used this workspace (synchronises the stream). */
+cg2d_status_t cg2d_workspace_status(const void* workspace, cg2d_stream_t stream);
+
+/* out = (A / cg2dNorm) v on the interior and 0 on halo points, with v's cross-tile neighbours
+ * gathered through the exchange (v's own halos are ignored, unwritten halo points read 0):
+ * _matvec of cg2d.py:292-298. Arrays [batch][T][ny][nx]. */
+cg2d_status_t cg2d_apply_operator(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                  const double* aW2d, const double* aS2d, const double* aC2d,
+                                  const double* v, double* out, cg2d_stream_t stream);
+
+/* Coefficient cotangents of J for the implicit derivative dx = A^-1 (db - dA x)
+ * (cg2d.py:331, 346-347): with lam = A^-1 xbar (an adjoint solve) and c = lam / cg2dNorm,
+ *   gW[j][i] = -(c(j,i) x(j,i-1) + c(j,i-1) x(j,i))  for interior rows, columns 1..sNx+1,
+ *   gS[j][i] = -(c(j,i) x(j-1,i) + c(j-1,i) x(j,i))  for interior columns, rows 1..sNy+1,
+ *   gC[j][i] = -c(j,i) x(j,i)                        on the interior,
+ * where x's cross-tile neighbours come through the exchange (unwritten halo points read 0);
+ * every other point of gW/gS/gC is set to 0. lam and x: [batch][T][ny][nx], halos ignored. */
+cg2d_status_t cg2d_edge_products(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                 const double* cg2dNorm_per_instance,
+                                 const double* lam, const double* x,
+                                 double* gW, double* gS, double* gC, cg2d_stream_t stream);
+
+/* Exchanger.exch_xy for kind "T" (exchange.py:136-142): out[p] = comp[p] ? a[src[p]] : a[p]
+ * over the full halo map given to cg2d_topology_create. a and out: [batch][T][ny][nx]; out may
+ * not alias a. */
+cg2d_status_t cg2d_exchange_scalar(const cg2d_topology_t* topo, int batch, const double* a, double* out,
+                                   cg2d_stream_t stream);
+
+/* Human-readable name of a status code (static string). */
+const char* cg2d_status_string(cg2d_status_t s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CG2D_B200_H */

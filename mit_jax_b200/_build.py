@@ -1,0 +1,33 @@
+"""Build libcg2d.so in-tree for sm_100a with nvcc (python -m mit_jax_b200._build)."""
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+SOURCES = [HERE / "csrc" / "cg2d_solver.cu", HERE / "csrc" / "cg2d_capi.cu"]
+OUT = HERE / "libcg2d.so"
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+
+def nvcc():
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def build(force=False, verbose=False):
+    deps = SOURCES + [HERE / "csrc" / "cg2d_internal.cuh", HERE.parent / "include" / "cg2d.h"]
+    if not force and OUT.exists() and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
+        return OUT
+    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(OUT) + ".tmp", *map(str, SOURCES)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    os.replace(str(OUT) + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,377 @@
+// C ABI of libcg2d.so: topology tables, workspace layout, argument checks and launches.
+// Declarations and the reference interfaces they replace: include/cg2d.h.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "cg2d_internal.cuh"
+
+struct cg2d_topology {
+  int sNx, sNy, OLx, OLy, nTiles;
+  int* d_nbr;        // [4][...] W, E (T*sNy each), S, N (T*sNx each)
+  int* d_src;        // full padded map
+  int8_t* d_comp;
+  int device;
+};
+
+namespace {
+
+using namespace cg2d;
+
+constexpr size_t kAlign = 256;
+inline size_t al(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+TopoDev topo_dev(const cg2d_topology* tp) {
+  TopoDev d;
+  d.nbr = tp->d_nbr;
+  d.map_src = tp->d_src;
+  d.map_comp = tp->d_comp;
+  d.ni = tp->sNx;
+  d.nj = tp->sNy;
+  d.OLx = tp->OLx;
+  d.OLy = tp->OLy;
+  d.npx = tp->sNx + 2 * tp->OLx;
+  d.npy = tp->sNy + 2 * tp->OLy;
+  d.T = tp->nTiles;
+  return d;
+}
+
+struct WsLayout {
+  size_t gs, rmax, cnt, zero_end, hist, part, total;
+  size_t vec[kMaxGroups], c32[kMaxGroups];
+  long long vec_stride[kMaxGroups];
+  long long vec_off[kMaxGroups][7];
+  int hist_len, part_units, total_rhs, total_ops, total_units, max_ni;
+  int nblk[kMaxGroups], units[kMaxGroups];
+};
+
+cg2d_status_t check_params(const cg2d_params_t* p) {
+  if (!p) return CG2D_BAD_ARG;
+  if (p->precision != CG2D_PREC_F64 && p->precision != CG2D_PREC_MIXED) return CG2D_BAD_ARG;
+  if (p->sum_order != CG2D_SUM_ROWBLOCK && p->sum_order != CG2D_SUM_FORTRAN) return CG2D_BAD_ARG;
+  if (p->rows_per_block < 1) return CG2D_BAD_ARG;
+  if (p->replace_every < 0 || !(p->replace_above >= 0.0)) return CG2D_BAD_ARG;
+  if (p->grid_ctas < 0 || p->ctas_per_sm < 0) return CG2D_BAD_ARG;
+  if (!(p->timeout_s > 0.0) || p->timeout_s > 3600.0) return CG2D_BAD_ARG;
+  if (p->test_missing_arrivals < 0 || p->test_missing_arrivals > 1024) return CG2D_BAD_ARG;
+  return CG2D_OK;
+}
+
+cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t* p, WsLayout* L) {
+  if (!gr || ng < 1 || ng > kMaxGroups) return CG2D_BAD_ARG;
+  std::memset(L, 0, sizeof(*L));
+  const bool mixed = p->precision == CG2D_PREC_MIXED;
+  const bool serial = p->sum_order == CG2D_SUM_FORTRAN;
+  const size_t vsz = mixed ? sizeof(float) : sizeof(double);
+  int max_iters = 0;
+  for (int g = 0; g < ng; ++g) {
+    const cg2d_group_t& G = gr[g];
+    if (!G.topo || G.count < 1 || G.nrhs < 1 || G.nrhs > 2) return CG2D_BAD_ARG;
+    const cg2d_topology* tp = G.topo;
+    if (tp->nTiles > kMaxTiles || tp->sNx > kMaxNi) return CG2D_UNSUPPORTED;
+    for (int s = 0; s < G.nrhs; ++s) {
+      if (G.max_iters[s] < 0 || !(G.tolerance[s] >= 0.0)) return CG2D_BAD_ARG;
+      if (G.max_iters[s] > max_iters) max_iters = G.max_iters[s];
+    }
+    L->nblk[g] = serial ? 1 : (tp->sNy + p->rows_per_block - 1) / p->rows_per_block;
+    L->units[g] = L->nblk[g] * tp->nTiles;
+    if (L->units[g] > L->part_units) L->part_units = L->units[g];
+    if (tp->sNx > L->max_ni) L->max_ni = tp->sNx;
+    L->total_rhs += G.count * G.nrhs;
+    L->total_ops += G.count;
+    const long long tu = (long long)L->total_units + (long long)G.count * L->units[g];
+    if (tu > (1ll << 30)) return CG2D_UNSUPPORTED;
+    L->total_units = (int)tu;
+  }
+  if (L->total_rhs > kMaxSolves || L->total_ops > kMaxOps) return CG2D_UNSUPPORTED;
+  L->hist_len = max_iters + 2;
+  size_t o = 0;
+  L->gs = o; o += al(2 * sizeof(unsigned));
+  L->rmax = o; o += al(sizeof(unsigned long long) * L->total_rhs);
+  L->cnt = o; o += al(sizeof(unsigned) * L->total_ops);
+  L->zero_end = o;
+  L->hist = o; o += al(sizeof(double) * (size_t)L->total_rhs * H_NKIND * L->hist_len);
+  L->part = o; o += al(sizeof(double) * (size_t)L->total_rhs * 2 * L->part_units);
+  for (int g = 0; g < ng; ++g) {
+    const cg2d_topology* tp = gr[g].topo;
+    const long long cmp = (long long)tp->nTiles * tp->sNy * tp->sNx;
+    const long long pad = (long long)tp->nTiles * (tp->sNy + 2 * tp->OLy) * (tp->sNx + 2 * tp->OLx);
+    long long off = 0;
+    L->vec_off[g][0] = off; off += (long long)al(sizeof(double) * cmp);
+    for (int v = 1; v < 7; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * cmp); }
+    L->vec_stride[g] = off;
+    L->vec[g] = o; o += al((size_t)off * gr[g].count * gr[g].nrhs);
+    L->c32[g] = o;
+    if (mixed) o += al(sizeof(float) * 6 * (size_t)pad * gr[g].count);
+  }
+  L->total = o;
+  return CG2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cg2d_default_params(cg2d_params_t* p) {
+  if (!p) return;
+  p->precision = CG2D_PREC_F64;
+  p->sum_order = CG2D_SUM_ROWBLOCK;
+  p->rows_per_block = 8;
+  p->replace_every = 25;
+  p->replace_above = 100.0;
+  p->grid_ctas = 0;
+  p->ctas_per_sm = 0;
+  p->timeout_s = 10.0;
+  p->test_missing_arrivals = 0;
+  p->reserved = 0;
+}
+
+const char* cg2d_status_string(cg2d_status_t s) {
+  switch (s) {
+    case CG2D_OK: return "ok";
+    case CG2D_NOT_CONVERGED: return "not converged (numIters == max_iters)";
+    case CG2D_NAN: return "final residual is NaN";
+    case CG2D_BARRIER_TIMEOUT: return "grid-wide wait timed out; results invalid";
+    case CG2D_BAD_ARG: return "bad argument";
+    case CG2D_CUDA_ERROR: return "CUDA error";
+    case CG2D_WORKSPACE_TOO_SMALL: return "workspace too small";
+    case CG2D_UNSUPPORTED: return "unsupported size";
+  }
+  return "unknown status";
+}
+
+cg2d_status_t cg2d_topology_create(int sNx, int sNy, int OLx, int OLy, int nTiles, const int32_t* src,
+                                   const int8_t* comp, cg2d_topology_t** out) {
+  if (!out || !src || !comp) return CG2D_BAD_ARG;
+  *out = nullptr;
+  if (sNx < 1 || sNy < 1 || OLx < 1 || OLy < 1 || nTiles < 1) return CG2D_BAD_ARG;
+  if (nTiles > kMaxTiles || sNx > kMaxNi) return CG2D_UNSUPPORTED;
+  const int npx = sNx + 2 * OLx, npy = sNy + 2 * OLy;
+  const long long npad = (long long)nTiles * npy * npx;
+  if (npad > (1ll << 31) - 1) return CG2D_UNSUPPORTED;
+  for (long long p = 0; p < npad; ++p) {
+    if (comp[p] != 0 && comp[p] != 1) return CG2D_BAD_ARG;     // scalar map: no component swap
+    if (comp[p] == 1 && (src[p] < 0 || src[p] >= npad)) return CG2D_BAD_ARG;
+  }
+  auto pad = [&](int t, int jj, int ii) { return ((long long)t * npy + jj) * npx + ii; };
+  auto to_cmp = [&](long long s, int* c) -> bool {
+    const int t = (int)(s / ((long long)npy * npx));
+    const long long rem = s - (long long)t * npy * npx;
+    const int jj = (int)(rem / npx), ii = (int)(rem - (long long)jj * npx);
+    if (jj < OLy || jj >= OLy + sNy || ii < OLx || ii >= OLx + sNx) return false;
+    *c = (t * sNy + (jj - OLy)) * sNx + (ii - OLx);
+    return true;
+  };
+  std::vector<int> nbr((size_t)nTiles * (2 * sNy + 2 * sNx), -1);
+  int* W = nbr.data();
+  int* E = W + (size_t)nTiles * sNy;
+  int* S = E + (size_t)nTiles * sNy;
+  int* N = S + (size_t)nTiles * sNx;
+  for (int t = 0; t < nTiles; ++t) {
+    for (int j = 0; j < sNy; ++j) {
+      const long long pw = pad(t, j + OLy, OLx - 1), pe = pad(t, j + OLy, OLx + sNx);
+      if (comp[pw] == 1 && !to_cmp(src[pw], &W[t * sNy + j])) return CG2D_BAD_ARG;
+      if (comp[pe] == 1 && !to_cmp(src[pe], &E[t * sNy + j])) return CG2D_BAD_ARG;
+    }
+    for (int i = 0; i < sNx; ++i) {
+      const long long ps = pad(t, OLy - 1, i + OLx), pn = pad(t, OLy + sNy, i + OLx);
+      if (comp[ps] == 1 && !to_cmp(src[ps], &S[t * sNx + i])) return CG2D_BAD_ARG;
+      if (comp[pn] == 1 && !to_cmp(src[pn], &N[t * sNx + i])) return CG2D_BAD_ARG;
+    }
+  }
+  cg2d_topology* tp = new cg2d_topology();
+  tp->sNx = sNx; tp->sNy = sNy; tp->OLx = OLx; tp->OLy = OLy; tp->nTiles = nTiles;
+  tp->d_nbr = nullptr; tp->d_src = nullptr; tp->d_comp = nullptr;
+  cudaGetDevice(&tp->device);
+  bool ok = cudaMalloc(&tp->d_nbr, nbr.size() * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&tp->d_src, (size_t)npad * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&tp->d_comp, (size_t)npad) == cudaSuccess &&
+            cudaMemcpy(tp->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(tp->d_src, src, (size_t)npad * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(tp->d_comp, comp, (size_t)npad, cudaMemcpyHostToDevice) == cudaSuccess;
+  if (!ok) {
+    cudaFree(tp->d_nbr); cudaFree(tp->d_src); cudaFree(tp->d_comp);
+    delete tp;
+    cudaGetLastError();
+    return CG2D_CUDA_ERROR;
+  }
+  *out = tp;
+  return CG2D_OK;
+}
+
+cg2d_status_t cg2d_topology_destroy(cg2d_topology_t* tp) {
+  if (!tp) return CG2D_BAD_ARG;
+  cudaFree(tp->d_nbr);
+  cudaFree(tp->d_src);
+  cudaFree(tp->d_comp);
+  delete tp;
+  return CG2D_OK;
+}
+
+size_t cg2d_workspace_size(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params) {
+  cg2d_params_t def;
+  if (!params) { cg2d_default_params(&def); params = &def; }
+  if (check_params(params) != CG2D_OK) return 0;
+  WsLayout L;
+  if (compute_layout(groups, ngroups, params, &L) != CG2D_OK) return 0;
+  return L.total;
+}
+
+cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params,
+                                void* workspace, size_t workspace_bytes, cg2d_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  cg2d_params_t def;
+  if (!params) { cg2d_default_params(&def); params = &def; }
+  cg2d_status_t st = check_params(params);
+  if (st != CG2D_OK) return st;
+  WsLayout L;
+  st = compute_layout(groups, ngroups, params, &L);
+  if (st != CG2D_OK) return st;
+  if (!workspace || (reinterpret_cast<uintptr_t>(workspace) % kAlign) != 0) return CG2D_BAD_ARG;
+  if (workspace_bytes < L.total) return CG2D_WORKSPACE_TOO_SMALL;
+  for (int g = 0; g < ngroups; ++g) {
+    const cg2d_group_t& G = groups[g];
+    if (!G.aW2d || !G.aS2d || !G.aC2d || !G.pW || !G.pS || !G.pC) return CG2D_BAD_ARG;
+    for (int s = 0; s < G.nrhs; ++s)
+      if (!G.b[s] || !G.x0[s] || !G.x_out[s] || !G.diag[s]) return CG2D_BAD_ARG;
+  }
+  char* ws = static_cast<char*>(workspace);
+  KParams kp;
+  std::memset(&kp, 0, sizeof(kp));
+  kp.ngroups = ngroups;
+  kp.total_units = L.total_units;
+  kp.total_rhs = L.total_rhs;
+  kp.total_ops = L.total_ops;
+  kp.mixed = params->precision == CG2D_PREC_MIXED;
+  kp.serial = params->sum_order == CG2D_SUM_FORTRAN;
+  kp.rows_per_block = params->rows_per_block;
+  kp.replace_every = params->replace_every;
+  kp.replace_above = params->replace_above;
+  kp.max_ni = L.max_ni;
+  kp.hist = reinterpret_cast<double*>(ws + L.hist);
+  kp.hist_len = L.hist_len;
+  kp.part = reinterpret_cast<double*>(ws + L.part);
+  kp.part_units = L.part_units;
+  kp.cnt = reinterpret_cast<unsigned*>(ws + L.cnt);
+  kp.rmax = reinterpret_cast<unsigned long long*>(ws + L.rmax);
+  kp.gs = reinterpret_cast<unsigned*>(ws + L.gs);
+  kp.timeout_ns = (unsigned long long)(params->timeout_s * 1e9);
+  kp.test_missing = params->test_missing_arrivals;
+  int unit_base = 0, op_base = 0, rhs_base = 0;
+  for (int g = 0; g < ngroups; ++g) {
+    const cg2d_group_t& G = groups[g];
+    GroupDev& d = kp.g[g];
+    d.tp = topo_dev(G.topo);
+    d.count = G.count;
+    d.nrhs = G.nrhs;
+    d.nblk = L.nblk[g];
+    d.units = L.units[g];
+    d.unit_base = unit_base;
+    d.op_base = op_base;
+    d.rhs_base = rhs_base;
+    d.pad_elems = (long long)d.tp.T * d.tp.npy * d.tp.npx;
+    d.cmp_elems = (long long)d.tp.T * d.tp.nj * d.tp.ni;
+    d.a64[0] = G.aW2d; d.a64[1] = G.aS2d; d.a64[2] = G.aC2d;
+    d.a64[3] = G.pW; d.a64[4] = G.pS; d.a64[5] = G.pC;
+    d.c32 = kp.mixed ? reinterpret_cast<float*>(ws + L.c32[g]) : nullptr;
+    d.norm = G.cg2dNorm;
+    d.norm_arr = G.cg2dNorm_per_instance;
+    for (int s = 0; s < 2; ++s) {
+      const bool on = s < G.nrhs;
+      d.b[s] = on ? G.b[s] : nullptr;
+      d.x0[s] = on ? G.x0[s] : nullptr;
+      d.x_out[s] = on ? G.x_out[s] : nullptr;
+      d.x_fortran[s] = on ? G.x_fortran[s] : nullptr;
+      d.diag[s] = on ? G.diag[s] : nullptr;
+      d.tol[s] = on ? G.tolerance[s] : 0.0;
+      d.max_iters[s] = on ? G.max_iters[s] : 0;
+    }
+    d.vec = ws + L.vec[g];
+    d.vec_stride = L.vec_stride[g];
+    for (int v = 0; v < 7; ++v) d.vec_off[v] = L.vec_off[g][v];
+    unit_base += G.count * d.units;
+    op_base += G.count;
+    rhs_base += G.count * G.nrhs;
+  }
+
+  if (cudaMemsetAsync(ws, 0, L.zero_end, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  if (kp.mixed)
+    for (int g = 0; g < ngroups; ++g)
+      if (launch_pack32(kp.g[g], stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+
+  const size_t smem = smem_bytes(kp.max_ni, kp.serial);
+  int bps = 0;
+  if (solver_occupancy(kp.mixed, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  if (params->ctas_per_sm > 0 && params->ctas_per_sm < bps) bps = params->ctas_per_sm;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  long long grid = (long long)bps * nsm;
+  if (params->grid_ctas > 0 && params->grid_ctas < grid) grid = params->grid_ctas;
+  if (grid > kp.total_units) grid = kp.total_units;
+  if (grid < 1) grid = 1;
+  if (launch_solver(kp, (int)grid, smem, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2dNorm, const double* aW2d,
+                             const double* aS2d, const double* aC2d, const double* pW, const double* pS,
+                             const double* pC, const double* cg2d_b, const double* cg2d_x, double tolerance,
+                             int max_iters, double* x_out, double* x_fortran, cg2d_diag_t* diag,
+                             const cg2d_params_t* params, void* workspace, size_t workspace_bytes,
+                             cg2d_stream_t stream) {
+  cg2d_group_t g;
+  std::memset(&g, 0, sizeof(g));
+  g.topo = topo;
+  g.count = batch;
+  g.nrhs = 1;
+  g.aW2d = aW2d; g.aS2d = aS2d; g.aC2d = aC2d; g.pW = pW; g.pS = pS; g.pC = pC;
+  g.cg2dNorm = cg2dNorm;
+  g.b[0] = cg2d_b;
+  g.x0[0] = cg2d_x;
+  g.x_out[0] = x_out;
+  g.x_fortran[0] = x_fortran;
+  g.diag[0] = diag;
+  g.tolerance[0] = tolerance;
+  g.max_iters[0] = max_iters;
+  return cg2d_solve_groups(&g, 1, params, workspace, workspace_bytes, stream);
+}
+
+cg2d_status_t cg2d_workspace_status(const void* workspace, cg2d_stream_t stream) {
+  if (!workspace) return CG2D_BAD_ARG;
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  unsigned w[2] = {0, 0};
+  if (cudaMemcpy(w, workspace, sizeof(w), cudaMemcpyDeviceToHost) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return w[1] ? (cg2d_status_t)w[1] : CG2D_OK;
+}
+
+cg2d_status_t cg2d_apply_operator(const cg2d_topology_t* topo, int batch, double cg2dNorm, const double* aW2d,
+                                  const double* aS2d, const double* aC2d, const double* v, double* out,
+                                  cg2d_stream_t stream) {
+  if (!topo || batch < 1 || !aW2d || !aS2d || !aC2d || !v || !out || v == out) return CG2D_BAD_ARG;
+  if (launch_apply_operator(topo_dev(topo), batch, cg2dNorm, aW2d, aS2d, aC2d, v, out,
+                            reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+cg2d_status_t cg2d_edge_products(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                 const double* cg2dNorm_per_instance, const double* lam, const double* x,
+                                 double* gW, double* gS, double* gC, cg2d_stream_t stream) {
+  if (!topo || batch < 1 || !lam || !x || !gW || !gS || !gC) return CG2D_BAD_ARG;
+  if (launch_edge_products(topo_dev(topo), batch, cg2dNorm, cg2dNorm_per_instance, lam, x, gW, gS, gC,
+                           reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+cg2d_status_t cg2d_exchange_scalar(const cg2d_topology_t* topo, int batch, const double* a, double* out,
+                                   cg2d_stream_t stream) {
+  if (!topo || batch < 1 || !a || !out || a == out) return CG2D_BAD_ARG;
+  if (launch_exchange(topo_dev(topo), batch, a, out, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,50 @@
+"""The C ABI library loads and exports every function include/cg2d.h declares; struct layouts agree (no GPU)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from mit_jax_b200 import capi
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "cg2d.h"
+
+
+def declared_functions():
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w\s\*]*?\b(cg2d_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declares_the_bound_functions():
+    decl = declared_functions()
+    assert set(capi.EXPORTED) <= set(decl), set(capi.EXPORTED) - set(decl)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = capi.lib()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_struct_layouts():
+    assert ctypes.sizeof(capi.Params) == 48
+    assert ctypes.sizeof(capi.Diag) == 48
+    assert ctypes.sizeof(capi.Group) == 8 + 4 + 4 + 6 * 8 + 8 + 8 + 5 * 16 + 16 + 8
+
+
+def test_default_params_and_status_strings():
+    p = capi.default_params()
+    assert (p.precision, p.sum_order, p.rows_per_block, p.replace_every) == (0, 0, 8, 25)
+    assert p.replace_above == 100.0 and p.timeout_s == 10.0
+    lib = capi.lib()
+    assert lib.cg2d_status_string(capi.CG2D_BARRIER_TIMEOUT).startswith(b"grid-wide wait")
+
+
+def test_bad_arguments_are_rejected_without_a_gpu():
+    lib = capi.lib()
+    out = ctypes.c_void_p()
+    assert lib.cg2d_topology_create(0, 8, 1, 1, 13, None, None, ctypes.byref(out)) == capi.CG2D_BAD_ARG
+    g = (capi.Group * 1)()
+    assert lib.cg2d_workspace_size(g, 1, None) == 0          # no topology
+    assert lib.cg2d_solve_groups(g, 0, None, None, 0, None) == capi.CG2D_BAD_ARG
