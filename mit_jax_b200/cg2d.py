@@ -378,7 +378,7 @@ class Cg2dSolve(torch.autograd.Function):
                            p.adj_tolerance, p.adj_max_iters, "rowblock", want_fortran=False)
         lam = torch.where(mask, lam, torch.zeros((), dtype=lam.dtype, device=lam.device))
         gW = gS = gC = None
-        if not p.stop_coeff_grad and any(ctx.needs_input_grad[2:5]):
+        if not p.stop_coeff_grad and any(ctx.needs_input_grad[3:6]):
             gW, gS, gC = edge_products(ex, lam, x, p.cg2dNorm)
         return None, None, None, gW, gS, gC, None, None, None, lam, None
 

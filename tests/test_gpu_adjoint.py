@@ -67,9 +67,20 @@ def test_gradients_match_central_differences(prob):
     (x * _t(w)).sum().backward()
     grads = [aW_t.grad.cpu().numpy(), aC_t.grad.cpu().numpy(), b_t.grad.cpu().numpy()]
     base = [ops[0], ops[2], syn.rhs()]
-    # a wet 3x3 window in the middle of tile 4
-    t, j0, i0 = 4, L.jj(7), L.ii(7)
-    assert np.all(ops[2][t, j0:j0 + 3, i0:i0 + 3] != 0) and np.all(ops[0][t, j0:j0 + 3, i0:i0 + 3] != 0)
+    # a 3x3 window whose west faces are all wet (first one found scanning tile 4, then the others)
+    J, I = L.interior
+    found = None
+    for t in (4, 3, 5, 1, 7, 8):
+        for j in range(J.start, J.stop - 2):
+            for i in range(I.start, I.stop - 2):
+                if np.all(ops[0][t, j:j + 3, i:i + 3] != 0):
+                    found = (t, j, i)
+                    break
+            if found:
+                break
+        if found:
+            break
+    t, j0, i0 = found
     for k, name, hs, tol in ((0, "aW2d", (1e-2, 1e-3, 1e-4, 1e-5), 1e-6), (1, "aC2d", (1e-3, 1e-4, 1e-5), 1e-5),
                              (2, "cg2d_b", (1e-1, 1e-2, 1e-3), 1e-8)):
         win = base[k][t, j0:j0 + 3, i0:i0 + 3]

@@ -55,7 +55,11 @@ def test_rowblock_order_bitwise_equals_oracle(name):
     np.testing.assert_array_equal(_diag_vec(d), _diag_vec(do))
     if name not in ("llc8_cap", "llc8_zero_iters", "llc8_onemore"):
         assert abs(d["numIters"] - c.numIters) <= 1
-        assert _rel(x, c.x_fortran, c.L) < 1e-12
+        if name == "llc8_zero_rhs":      # the exact solution is 0: compare absolutely
+            J, I = c.L.interior
+            assert np.abs(x[:, J, I] - c.x_fortran[:, J, I]).max() < 1e-10
+        else:
+            assert _rel(x, c.x_fortran, c.L) < 1e-12
 
 
 @pytest.fixture(scope="module")
@@ -151,12 +155,12 @@ def test_two_rhs_share_the_operator():
     ops = tuple(t(a) for a in c.ops)
     w = np.random.default_rng(3).standard_normal(c.L.shape2d)
     G2 = cg.GroupSpec(ex, ops, [t(c.b), t(w)], [t(c.x0), t(np.zeros_like(w))], [1e-12, 1e-13], [300, 2000], c.norm)
-    (r2,), = cg.solve_groups([G2])
+    (slots2,) = cg.solve_groups([G2])
     for slot, (b, x0, tol, mi) in enumerate(((c.b, c.x0, 1e-12, 300), (w, np.zeros_like(w), 1e-13, 2000))):
         G1 = cg.GroupSpec(ex, ops, [t(b)], [t(x0)], [tol], [mi], c.norm)
-        (r1,), = cg.solve_groups([G1])
-        np.testing.assert_array_equal(r2[slot][0].cpu().numpy(), r1[0][0].cpu().numpy())
-        assert cg.diag_records(r2[slot][2]) == cg.diag_records(r1[0][2])
+        (slots1,) = cg.solve_groups([G1])
+        np.testing.assert_array_equal(slots2[slot][0].cpu().numpy(), slots1[0][0].cpu().numpy())
+        assert cg.diag_records(slots2[slot][2]) == cg.diag_records(slots1[0][2])
 
 
 def test_mixed_size_groups_llc270_and_llc90():
@@ -227,9 +231,9 @@ def test_barrier_time_limit_reports_status():
     dev = torch.device("cuda")
     t = lambda a: torch.as_tensor(a).to(dev)[None]          # noqa: E731
     G = cg.GroupSpec(ex, tuple(t(a) for a in c.ops), [t(c.b)], [t(c.x0)], [c.tol], [c.maxit], c.norm)
-    (res,), = cg.solve_groups([G], timeout_s=0.2, check_status=False, test_missing_arrivals=1)
+    ((xo, xf, dg),), = cg.solve_groups([G], timeout_s=0.2, check_status=False, test_missing_arrivals=1)
     torch.cuda.synchronize()
-    assert cg.diag_records(res[0][2])[0]["status"] == "barrier_timeout"
+    assert cg.diag_records(dg)[0]["status"] == "barrier_timeout"
     x, d = cg.cg2d_fortran(ex, c.ops, c.b, c.x0, cg2dNorm=c.norm, tolerance=c.tol, max_iters=c.maxit,
                            sum_order="fortran")
     np.testing.assert_array_equal(x, c.x_fortran)          # the next solve on the same context is fine
