@@ -12,7 +12,9 @@
 
 struct cg2d_topology {
   int sNx, sNy, OLx, OLy, nTiles;
+  int njp, nip;      // halo slice pitches (multiples of 4)
   int* d_nbr;        // [4][...] W, E (T*sNy each), S, N (T*sNx each)
+  int* d_tg;         // [T][2 sNy + 2 sNx][2] halo slots each tile-edge point is pushed to
   int* d_src;        // full padded map
   int8_t* d_comp;
   int device;
@@ -28,6 +30,9 @@ inline size_t al(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 TopoDev topo_dev(const cg2d_topology* tp) {
   TopoDev d;
   d.nbr = tp->d_nbr;
+  d.tg = tp->d_tg;
+  d.njp = tp->njp;
+  d.nip = tp->nip;
   d.map_src = tp->d_src;
   d.map_comp = tp->d_comp;
   d.ni = tp->sNx;
@@ -41,24 +46,66 @@ TopoDev topo_dev(const cg2d_topology* tp) {
 }
 
 struct WsLayout {
-  size_t gs, rmax, cnt, zero_end, hist, part, total;
-  size_t vec[kMaxGroups], c32[kMaxGroups];
-  long long vec_stride[kMaxGroups];
-  long long vec_off[kMaxGroups][7];
+  size_t gs, rmax, cnt, halo_begin, zero_end, hist, part, total;
+  size_t vec[kMaxGroups], c32[kMaxGroups], halo[kMaxGroups];
+  long long vec_stride[kMaxGroups], halo_stride[kMaxGroups];
+  long long vec_off[kMaxGroups][V_NVEC], halo_off[kMaxGroups][V_NVEC];
+  int ldv[kMaxGroups], ldx[kMaxGroups], ldc[kMaxGroups];
   int hist_len, part_units, total_rhs, total_ops, total_units, max_ni;
   int nblk[kMaxGroups], units[kMaxGroups];
+  int ch, nstage[P_NPASS];
+  unsigned stage_bytes;
+  size_t smem;
 };
+
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 cg2d_status_t check_params(const cg2d_params_t* p) {
   if (!p) return CG2D_BAD_ARG;
   if (p->precision != CG2D_PREC_F64 && p->precision != CG2D_PREC_MIXED) return CG2D_BAD_ARG;
   if (p->sum_order != CG2D_SUM_ROWBLOCK && p->sum_order != CG2D_SUM_FORTRAN) return CG2D_BAD_ARG;
-  if (p->rows_per_block < 1) return CG2D_BAD_ARG;
+  if (p->rows_per_block < 8 || p->rows_per_block % 8 != 0) return CG2D_BAD_ARG;
   if (p->replace_every < 0 || !(p->replace_above >= 0.0)) return CG2D_BAD_ARG;
   if (p->grid_ctas < 0 || p->ctas_per_sm < 0) return CG2D_BAD_ARG;
   if (!(p->timeout_s > 0.0) || p->timeout_s > 3600.0) return CG2D_BAD_ARG;
   if (p->test_missing_arrivals < 0 || p->test_missing_arrivals > 1024) return CG2D_BAD_ARG;
   return CG2D_OK;
+}
+
+// chunk height and stage buffers: the largest chunk (8, else 4 rows) whose two stage buffers fit
+cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial, WsLayout* L) {
+  const size_t fixed = fixed_smem_bytes(L->max_ni, serial);
+  for (int ch : {8, 4}) {
+    unsigned hot = 0, rep = 0;
+    for (int g = 0; g < ng; ++g) {
+      const cg2d_topology* tp = gr[g].topo;
+      const int npx = tp->sNx + 2 * tp->OLx;
+      for (int pt : {P_S, P_X, P_Z}) {
+        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
+        if (S.total > hot) hot = S.total;
+      }
+      if (mixed) {
+        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
+        if (S.total > rep) rep = S.total;
+      }
+    }
+    // the direct-load passes stage (8 + 2) rows of (max_ni + 2) doubles per solve slot in the same area
+    const unsigned direct = (unsigned)(2 * (kWarps + 2) * (L->max_ni + 2) * sizeof(double));
+    unsigned sb = hot;
+    if (2 * sb < rep) sb = (rep + 1) / 2;
+    if (2 * sb < direct) sb = (direct + 1) / 2;
+    sb = al128(sb);
+    const size_t smem = fixed + 2 * (size_t)sb;
+    if (smem <= (size_t)kSmemLimit) {
+      L->ch = ch;
+      L->stage_bytes = sb;
+      L->smem = smem;
+      for (int i = 0; i < P_NPASS; ++i) L->nstage[i] = 2;
+      L->nstage[P_R] = (rep <= sb) ? 2 : 1;
+      return CG2D_OK;
+    }
+  }
+  return CG2D_UNSUPPORTED;
 }
 
 cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t* p, WsLayout* L) {
@@ -73,6 +120,8 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     if (!G.topo || G.count < 1 || G.nrhs < 1 || G.nrhs > 2) return CG2D_BAD_ARG;
     const cg2d_topology* tp = G.topo;
     if (tp->nTiles > kMaxTiles || tp->sNx > kMaxNi) return CG2D_UNSUPPORTED;
+    // bulk copies move whole padded coefficient rows: 16-byte multiples
+    if (((tp->sNx + 2 * tp->OLx) * 8) % 16 != 0) return CG2D_UNSUPPORTED;
     for (int s = 0; s < G.nrhs; ++s) {
       if (G.max_iters[s] < 0 || !(G.tolerance[s] >= 0.0)) return CG2D_BAD_ARG;
       if (G.max_iters[s] > max_iters) max_iters = G.max_iters[s];
@@ -81,6 +130,9 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     L->units[g] = L->nblk[g] * tp->nTiles;
     if (L->units[g] > L->part_units) L->part_units = L->units[g];
     if (tp->sNx > L->max_ni) L->max_ni = tp->sNx;
+    L->ldv[g] = round_up(tp->sNx, (int)(16 / vsz));
+    L->ldx[g] = round_up(tp->sNx, 2);
+    L->ldc[g] = round_up(tp->sNx + 2 * tp->OLx, 4);
     L->total_rhs += G.count * G.nrhs;
     L->total_ops += G.count;
     const long long tu = (long long)L->total_units + (long long)G.count * L->units[g];
@@ -88,25 +140,40 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     L->total_units = (int)tu;
   }
   if (L->total_rhs > kMaxSolves || L->total_ops > kMaxOps) return CG2D_UNSUPPORTED;
+  cg2d_status_t st = size_stages(gr, ng, mixed, serial, L);
+  if (st != CG2D_OK) return st;
   L->hist_len = max_iters + 2;
   size_t o = 0;
   L->gs = o; o += al(2 * sizeof(unsigned));
   L->rmax = o; o += al(sizeof(unsigned long long) * L->total_rhs);
   L->cnt = o; o += al(sizeof(unsigned) * L->total_ops);
+  L->halo_begin = o;
+  for (int g = 0; g < ng; ++g) {
+    const cg2d_topology* tp = gr[g].topo;
+    const long long hn = (long long)tp->nTiles * (2 * tp->njp + 2 * tp->nip);
+    long long off = 0;
+    for (int v = 0; v < V_NVEC; ++v) {
+      L->halo_off[g][v] = off;
+      off += (long long)al((v == V_X ? sizeof(double) : vsz) * hn);
+    }
+    L->halo_stride[g] = off;
+    L->halo[g] = o;
+    o += al((size_t)off * gr[g].count * gr[g].nrhs);
+  }
   L->zero_end = o;
   L->hist = o; o += al(sizeof(double) * (size_t)L->total_rhs * H_NKIND * L->hist_len);
   L->part = o; o += al(sizeof(double) * (size_t)L->total_rhs * 2 * L->part_units);
   for (int g = 0; g < ng; ++g) {
     const cg2d_topology* tp = gr[g].topo;
-    const long long cmp = (long long)tp->nTiles * tp->sNy * tp->sNx;
-    const long long pad = (long long)tp->nTiles * (tp->sNy + 2 * tp->OLy) * (tp->sNx + 2 * tp->OLx);
+    const long long rows = (long long)tp->nTiles * tp->sNy;
+    const long long npy = tp->sNy + 2 * tp->OLy;
     long long off = 0;
-    L->vec_off[g][0] = off; off += (long long)al(sizeof(double) * cmp);
-    for (int v = 1; v < 7; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * cmp); }
+    L->vec_off[g][V_X] = off; off += (long long)al(sizeof(double) * rows * L->ldx[g]);
+    for (int v = 1; v < V_NVEC; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * rows * L->ldv[g]); }
     L->vec_stride[g] = off;
     L->vec[g] = o; o += al((size_t)off * gr[g].count * gr[g].nrhs);
     L->c32[g] = o;
-    if (mixed) o += al(sizeof(float) * 6 * (size_t)pad * gr[g].count);
+    if (mixed) o += al(sizeof(float) * 6 * (size_t)tp->nTiles * npy * L->ldc[g] * gr[g].count);
   }
   L->total = o;
   return CG2D_OK;
@@ -183,18 +250,51 @@ cg2d_status_t cg2d_topology_create(int sNx, int sNy, int OLx, int OLy, int nTile
       if (comp[pn] == 1 && !to_cmp(src[pn], &N[t * sNx + i])) return CG2D_BAD_ARG;
     }
   }
+  // push targets: every halo slot (side, tile, position) with a source point is filled by that point's
+  // owner; a source must lie on its own tile's edge, with at most two slots per edge point
+  const int njp = round_up(sNy, 4), nip = round_up(sNx, 4);
+  const int perim = 2 * sNy + 2 * sNx;
+  std::vector<int> tg((size_t)nTiles * perim * 2, -1);
+  auto add_target = [&](int c, int slot) -> bool {
+    const int t = c / (sNy * sNx), rem = c - t * sNy * sNx, j = rem / sNx, i = rem - j * sNx;
+    int e;
+    if (i == 0) e = j;
+    else if (i == sNx - 1) e = sNy + j;
+    else if (j == 0) e = 2 * sNy + i;
+    else if (j == sNy - 1) e = 2 * sNy + sNx + i;
+    else return false;
+    int* q = &tg[((size_t)t * perim + e) * 2];
+    if (q[0] < 0) q[0] = slot;
+    else if (q[1] < 0) q[1] = slot;
+    else return false;
+    return true;
+  };
+  for (int t = 0; t < nTiles; ++t) {
+    for (int k = 0; k < sNy; ++k) {
+      if (W[t * sNy + k] >= 0 && !add_target(W[t * sNy + k], t * njp + k)) return CG2D_BAD_ARG;
+      if (E[t * sNy + k] >= 0 && !add_target(E[t * sNy + k], (nTiles + t) * njp + k)) return CG2D_BAD_ARG;
+    }
+    for (int k = 0; k < sNx; ++k) {
+      if (S[t * sNx + k] >= 0 && !add_target(S[t * sNx + k], 2 * nTiles * njp + t * nip + k)) return CG2D_BAD_ARG;
+      if (N[t * sNx + k] >= 0 && !add_target(N[t * sNx + k], 2 * nTiles * njp + (nTiles + t) * nip + k))
+        return CG2D_BAD_ARG;
+    }
+  }
   cg2d_topology* tp = new cg2d_topology();
   tp->sNx = sNx; tp->sNy = sNy; tp->OLx = OLx; tp->OLy = OLy; tp->nTiles = nTiles;
-  tp->d_nbr = nullptr; tp->d_src = nullptr; tp->d_comp = nullptr;
+  tp->njp = njp; tp->nip = nip;
+  tp->d_nbr = nullptr; tp->d_tg = nullptr; tp->d_src = nullptr; tp->d_comp = nullptr;
   cudaGetDevice(&tp->device);
   bool ok = cudaMalloc(&tp->d_nbr, nbr.size() * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&tp->d_tg, tg.size() * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&tp->d_src, (size_t)npad * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&tp->d_comp, (size_t)npad) == cudaSuccess &&
             cudaMemcpy(tp->d_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(tp->d_tg, tg.data(), tg.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(tp->d_src, src, (size_t)npad * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(tp->d_comp, comp, (size_t)npad, cudaMemcpyHostToDevice) == cudaSuccess;
   if (!ok) {
-    cudaFree(tp->d_nbr); cudaFree(tp->d_src); cudaFree(tp->d_comp);
+    cudaFree(tp->d_nbr); cudaFree(tp->d_tg); cudaFree(tp->d_src); cudaFree(tp->d_comp);
     delete tp;
     cudaGetLastError();
     return CG2D_CUDA_ERROR;
@@ -206,6 +306,7 @@ cg2d_status_t cg2d_topology_create(int sNx, int sNy, int OLx, int OLy, int nTile
 cg2d_status_t cg2d_topology_destroy(cg2d_topology_t* tp) {
   if (!tp) return CG2D_BAD_ARG;
   cudaFree(tp->d_nbr);
+  cudaFree(tp->d_tg);
   cudaFree(tp->d_src);
   cudaFree(tp->d_comp);
   delete tp;
@@ -236,6 +337,8 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   for (int g = 0; g < ngroups; ++g) {
     const cg2d_group_t& G = groups[g];
     if (!G.aW2d || !G.aS2d || !G.aC2d || !G.pW || !G.pS || !G.pC) return CG2D_BAD_ARG;
+    for (const double* a : {G.aW2d, G.aS2d, G.aC2d, G.pW, G.pS, G.pC})
+      if (reinterpret_cast<uintptr_t>(a) % 16 != 0) return CG2D_BAD_ARG;   // bulk-copy sources
     for (int s = 0; s < G.nrhs; ++s)
       if (!G.b[s] || !G.x0[s] || !G.x_out[s] || !G.diag[s]) return CG2D_BAD_ARG;
   }
@@ -252,6 +355,9 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   kp.replace_every = params->replace_every;
   kp.replace_above = params->replace_above;
   kp.max_ni = L.max_ni;
+  kp.ch = L.ch;
+  for (int i = 0; i < P_NPASS; ++i) kp.nstage[i] = L.nstage[i];
+  kp.stage_bytes = L.stage_bytes;
   kp.hist = reinterpret_cast<double*>(ws + L.hist);
   kp.hist_len = L.hist_len;
   kp.part = reinterpret_cast<double*>(ws + L.part);
@@ -274,7 +380,9 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
     d.op_base = op_base;
     d.rhs_base = rhs_base;
     d.pad_elems = (long long)d.tp.T * d.tp.npy * d.tp.npx;
-    d.cmp_elems = (long long)d.tp.T * d.tp.nj * d.tp.ni;
+    d.ldv = L.ldv[g];
+    d.ldx = L.ldx[g];
+    d.ldc = L.ldc[g];
     d.a64[0] = G.aW2d; d.a64[1] = G.aS2d; d.a64[2] = G.aC2d;
     d.a64[3] = G.pW; d.a64[4] = G.pS; d.a64[5] = G.pC;
     d.c32 = kp.mixed ? reinterpret_cast<float*>(ws + L.c32[g]) : nullptr;
@@ -292,7 +400,10 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
     }
     d.vec = ws + L.vec[g];
     d.vec_stride = L.vec_stride[g];
-    for (int v = 0; v < 7; ++v) d.vec_off[v] = L.vec_off[g][v];
+    for (int v = 0; v < V_NVEC; ++v) d.vec_off[v] = L.vec_off[g][v];
+    d.halo = ws + L.halo[g];
+    d.halo_stride = L.halo_stride[g];
+    for (int v = 0; v < V_NVEC; ++v) d.halo_off[v] = L.halo_off[g][v];
     unit_base += G.count * d.units;
     op_base += G.count;
     rhs_base += G.count * G.nrhs;
@@ -303,7 +414,7 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
     for (int g = 0; g < ngroups; ++g)
       if (launch_pack32(kp.g[g], stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
 
-  const size_t smem = smem_bytes(kp.max_ni, kp.serial);
+  const size_t smem = L.smem;
   int bps = 0;
   if (solver_occupancy(kp.mixed, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   if (params->ctas_per_sm > 0 && params->ctas_per_sm < bps) bps = params->ctas_per_sm;

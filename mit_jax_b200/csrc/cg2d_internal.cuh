@@ -8,27 +8,32 @@
 
 namespace cg2d {
 
-constexpr int kWarps = 8;                  // rows per chunk = warps per CTA (one warp per row)
+constexpr int kWarps = 8;                  // warps per CTA; a chunk has at most kWarps rows (one warp per row)
 constexpr int kThreads = kWarps * 32;
 constexpr int kMaxGroups = CG2D_MAX_GROUPS;
 constexpr int kMaxSolves = CG2D_MAX_SOLVES; // right-hand sides per launch (one thread owns each)
 constexpr int kMaxOps = 256;               // operators (instances) per launch
 constexpr int kMaxTiles = 256;
-constexpr int kMaxNi = 1024;               // tile width limit (shared-memory staging rows)
+constexpr int kMaxNi = 1024;               // tile width limit
+constexpr int kSmemLimit = 227 * 1024;     // dynamic shared memory per CTA on sm_100
 
 // pass kinds of the persistent kernel
-enum Pass : int { P_MAX = 0, P_INIT = 1, P_Z = 2, P_S = 3, P_X = 4 };
+enum Pass : int { P_MAX = 0, P_INIT = 1, P_Z = 2, P_S = 3, P_X = 4, P_R = 5, P_NPASS = 6 };
 // per-solve action inside a pass
-enum Act : int { A_NONE = 0, A_ACTIVE = 1, A_FIN = 2, A_REPLACE = 3 };
+enum Act : int { A_NONE = 0, A_ACTIVE = 1, A_FIN = 2 };
 // per-solve scalar history: one slot per (kind, iteration), each written at most once
 enum Hist : int { H_RRX = 0, H_ETAX = 1, H_SQ = 2, H_RRR = 3, H_ETAZ = 4, H_SUM = 5, H_NKIND = 6 };
+// per-solve vectors (compact [T][nj][pitch]) and their halo slices
+enum VecId : int { V_X = 0, V_R0 = 1, V_R1 = 2, V_S0 = 3, V_S1 = 4, V_Z = 5, V_Q = 6, V_NVEC = 7 };
 
-// neighbour tables of one tile layout (device)
+// tables of one tile layout (device)
 struct TopoDev {
   const int* nbr;           // [4][T*len]: W (len nj), E (nj), S (ni), N (ni); compact source index or -1
+  const int* tg;            // [T][2nj+2ni][2]: halo slots a tile-edge point's value is pushed to (-1 = none)
   const int* map_src;       // full padded "T" map (src), for x_fortran halos and cg2d_exchange_scalar
   const int8_t* map_comp;
   int ni, nj, OLx, OLy, npx, npy, T;
+  int njp, nip;             // halo slice pitches: W/E slices [T][njp], S/N slices [T][nip]
 };
 
 struct GroupDev {
@@ -37,9 +42,9 @@ struct GroupDev {
   int nblk, units;          // work units (row blocks) per tile / per instance
   int unit_base, op_base, rhs_base;
   long long pad_elems;      // T*npy*npx
-  long long cmp_elems;      // T*nj*ni
+  int ldv, ldx, ldc;        // row pitches (elements): V vectors, x (double), FP32 coefficient copies
   const double* a64[6];     // aW2d, aS2d, aC2d, pW, pS, pC: [count][pad_elems]
-  float* c32;               // MIXED: [count][6][pad_elems] float copies of a64
+  float* c32;               // MIXED: [count][6][T][npy][ldc] float copies of a64
   double norm;
   const double* norm_arr;   // nullable [count]
   const double* b[2];
@@ -49,9 +54,12 @@ struct GroupDev {
   cg2d_diag_t* diag[2];
   double tol[2];
   int max_iters[2];
-  char* vec;                // [count][nrhs] vector blocks (x, r0, r1, s0, s1, z, q)
+  char* vec;                // [count][nrhs] vector blocks
   long long vec_stride;     // bytes per vector block
-  long long vec_off[7];     // byte offsets of x, r0, r1, s0, s1, z, q inside a block
+  long long vec_off[V_NVEC];
+  char* halo;               // [count][nrhs] halo blocks (zeroed before the launch)
+  long long halo_stride;    // bytes per halo block
+  long long halo_off[V_NVEC];
 };
 
 struct KParams {
@@ -60,6 +68,9 @@ struct KParams {
   int mixed, serial, rows_per_block, replace_every;
   double replace_above;
   int max_ni;
+  int ch;                   // rows per chunk (<= kWarps)
+  int nstage[P_NPASS];      // pipeline depth of each pass kind (1 or 2)
+  unsigned stage_bytes;     // bytes of one stage buffer
   double* hist;             // [total_rhs][H_NKIND][hist_len]
   int hist_len;
   double* part;             // [total_rhs][2][part_units]
@@ -71,9 +82,57 @@ struct KParams {
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
 };
 
-size_t smem_bytes(int max_ni, int serial);
+// Shared-memory image of one chunk for a pipelined pass (offsets in bytes from the stage buffer).
+struct StageLay {
+  unsigned coef, coef_stride;   // 3 coefficient arrays, (ch+1) padded rows each
+  int cpitch, csize;
+  int nvec;                     // stencil vectors per solve
+  unsigned vec[2][2], vstride[2];
+  int vpitch[2], vsize[2];
+  unsigned hw[2][2], he[2][2];  // west / east cross-tile neighbours of the chunk's rows
+  unsigned xo[2];               // P_S: own rows of x (double)
+  unsigned total;
+};
+
+__host__ __device__ inline unsigned al128(unsigned x) { return (x + 127u) & ~127u; }
+__host__ __device__ inline unsigned al16(unsigned x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int npx, int ldv, int ldx,
+                                                 int ldc) {
+  StageLay L;
+  unsigned o = 0;
+  const bool coef64 = (pt == P_R) || !mixed;
+  L.csize = coef64 ? 8 : 4;
+  L.cpitch = coef64 ? npx : ldc;
+  L.coef = o;
+  L.coef_stride = al128((unsigned)((ch + 1) * L.cpitch * L.csize));
+  o += 3 * L.coef_stride;
+  L.nvec = (pt == P_Z) ? 1 : 2;
+  const int vs = mixed ? 4 : 8;
+  for (int v = 0; v < 2; ++v) {
+    L.vsize[v] = (pt == P_R && v == 0) ? 8 : vs;
+    L.vpitch[v] = (L.vsize[v] == 8) ? ldx : ldv;
+    L.vstride[v] = al128((unsigned)((ch + 2) * L.vpitch[v] * L.vsize[v]));
+  }
+  for (int s = 0; s < 2; ++s)
+    for (int v = 0; v < 2; ++v) {
+      L.vec[s][v] = L.hw[s][v] = L.he[s][v] = 0;
+      if (s < nrhs && v < L.nvec) {
+        L.vec[s][v] = o; o += L.vstride[v];
+        L.hw[s][v] = o; o += al128(al16((unsigned)(ch * L.vsize[v])));
+        L.he[s][v] = o; o += al128(al16((unsigned)(ch * L.vsize[v])));
+      }
+    }
+  for (int s = 0; s < 2; ++s) {
+    L.xo[s] = 0;
+    if (pt == P_S && s < nrhs) { L.xo[s] = o; o += al128((unsigned)(ch * ldx * 8)); }
+  }
+  L.total = al128(o);
+  return L;
+}
 
 // launchers (cg2d_solver.cu)
+size_t fixed_smem_bytes(int max_ni, int serial);
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream);
 cudaError_t solver_occupancy(int mixed, size_t smem, int* blocks_per_sm);
 cudaError_t launch_pack32(const GroupDev& g, cudaStream_t stream);

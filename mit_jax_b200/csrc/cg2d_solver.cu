@@ -9,12 +9,17 @@
 // Data movement per iteration k (per solve), two grid-wide waits:
 //   pass S_k : s_k = z_k + beta_k s_{k-1};  q_k = A s_k;  x_k = x_{k-1} + alpha_{k-1} s_{k-1};  sum s_k.q_k
 //   pass X_k : r_{k+1} = r_k - alpha_k q_k;  z_{k+1} = M r_{k+1};  sums r.r and z.r
-// The stencils need values at the four neighbours of a point; they are recomputed while staging a
-// chunk of rows into shared memory (the neighbour's s or r is formed from its z/s or r/q exactly as
-// its owner forms it), so no exchange step and no extra wait is needed. Cross-tile neighbours
-// (the exch2 halo of cg2d.py:228,235,250,260) are gathered through per-tile-edge tables.
-// The x update is deferred by one pass (it needs s_{k-1}, which pass S_k reads anyway); the
-// arithmetic is the reference's x_i = x + alpha * s_i (cg2d.py:254).
+// Work is cut into chunks of up to 8 rows of one tile. For every chunk one thread issues bulk
+// asynchronous copies (cp.async.bulk, completion counted on an mbarrier) of the coefficient rows,
+// the vector rows j-1 .. j+8 and the chunk's cross-tile neighbours into shared memory; the next
+// chunk's copies are in flight while the current one is computed (two stage buffers). Values at the
+// four neighbours of a point are formed in shared memory exactly as their owner forms them (a
+// neighbour's s_k from its z_k and s_{k-1}, its r_{k+1} from r_k and q_k), so no exchange step and no
+// extra wait is needed. Cross-tile neighbours -- the exch2 halo of cg2d.py:228,235,250,260 -- are
+// pushed by the owner of each tile-edge point into per-tile halo slices whenever it writes the
+// value, so a chunk's halo is as contiguous as its rows. The x update is deferred by one pass (it
+// needs s_{k-1}, which pass S_k reads anyway); its arithmetic is the reference's x + alpha * s
+// (cg2d.py:254).
 //
 // MIXED precision keeps r, s, z, q and the operator copies in FP32 (FP32 stencils), x and all dot
 // products in FP64, and replaces r by the FP64 true residual b - A x every replace_every iterations
@@ -84,12 +89,53 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
+// ---- bulk asynchronous copies and mbarriers
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// global -> shared bulk copy (no multicast), completion counted in bytes on `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// orders this thread's generic-proxy accesses against async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// bounded wait for an mbarrier phase
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0u && globaltimer() - t0 > limit_ns) return false;
+  }
+}
+
 // ------------------------------------------------------------------------------------------------
 // shared memory carve
 
 struct Smem {
   int* act;          // [kMaxSolves] action of each solve in the current pass
-  double* c1;        // [kMaxSolves] pass coefficient (beta in S, alpha in X)
+  double* c1;        // [kMaxSolves] pass coefficient (beta in S, alpha in X and R)
   double* c2;        // [kMaxSolves] alpha_{k-1} for the deferred x update
   double* rnorm;     // [kMaxSolves] rhsNorm
   double* norm;      // [kMaxSolves] cg2dNorm
@@ -98,41 +144,45 @@ struct Smem {
   double* rowsum;    // [2 slots][2 kinds][kWarps]
   double* tsum;      // [kMaxTiles]
   int* misc;         // [4]: barrier ok flag, last-arriver flag
-  double* stage;     // [2 slots][kWarps + 2][max_ni + 2]
+  unsigned long long* bar;  // [2] stage mbarriers
   double* prod;      // FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]
+  unsigned char* stage;     // 2 x stage_bytes (128-aligned); also the direct-load staging area
 };
 
-__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 
-size_t smem_bytes(int max_ni, int serial) {
+size_t fixed_smem_bytes(int max_ni, int serial) {
   size_t s = 0;
-  s += align16(sizeof(int) * kMaxSolves);
-  s += 4 * align16(sizeof(double) * kMaxSolves);
-  s += align16(sizeof(int) * kMaxSolves);
-  s += align16(sizeof(int) * kMaxOps);
-  s += align16(sizeof(double) * 2 * 2 * kWarps);
-  s += align16(sizeof(double) * kMaxTiles);
-  s += align16(sizeof(int) * 4);
-  s += align16(sizeof(double) * 2 * (kWarps + 2) * (size_t)(max_ni + 2));
-  if (serial) s += align16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni);
-  return s;
+  s += a16(sizeof(int) * kMaxSolves);
+  s += 4 * a16(sizeof(double) * kMaxSolves);
+  s += a16(sizeof(int) * kMaxSolves);
+  s += a16(sizeof(int) * kMaxOps);
+  s += a16(sizeof(double) * 2 * 2 * kWarps);
+  s += a16(sizeof(double) * kMaxTiles);
+  s += a16(sizeof(int) * 4);
+  s += a16(sizeof(unsigned long long) * 2);
+  if (serial) s += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni);
+  return (s + 127) & ~size_t(127);
 }
 
 __device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
   Smem m;
   size_t o = 0;
-  m.act = reinterpret_cast<int*>(base + o); o += align16(sizeof(int) * kMaxSolves);
-  m.c1 = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * kMaxSolves);
-  m.c2 = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * kMaxSolves);
-  m.rnorm = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * kMaxSolves);
-  m.norm = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * kMaxSolves);
-  m.has_alpha = reinterpret_cast<int*>(base + o); o += align16(sizeof(int) * kMaxSolves);
-  m.opp = reinterpret_cast<int*>(base + o); o += align16(sizeof(int) * kMaxOps);
-  m.rowsum = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * 2 * 2 * kWarps);
-  m.tsum = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * kMaxTiles);
-  m.misc = reinterpret_cast<int*>(base + o); o += align16(sizeof(int) * 4);
-  m.stage = reinterpret_cast<double*>(base + o); o += align16(sizeof(double) * 2 * (kWarps + 2) * (size_t)(max_ni + 2));
-  m.prod = serial ? reinterpret_cast<double*>(base + o) : nullptr;
+  m.act = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxSolves);
+  m.c1 = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
+  m.c2 = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
+  m.rnorm = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
+  m.norm = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
+  m.has_alpha = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxSolves);
+  m.opp = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxOps);
+  m.rowsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps);
+  m.tsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxTiles);
+  m.misc = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * 4);
+  m.bar = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 2);
+  m.prod = nullptr;
+  if (serial) { m.prod = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni); }
+  o = (o + 127) & ~size_t(127);
+  m.stage = base + o;
   return m;
 }
 
@@ -141,6 +191,7 @@ __device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
 // when another CTA has flagged an error, or after timeout_ns (then this CTA flags the error).
 
 __device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag) {
+  fence_proxy_async();        // this thread's stores before the next pass's bulk copies
   __syncthreads();
   if (threadIdx.x == 0) {
     target += gridDim.x;
@@ -159,6 +210,7 @@ __device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag) {
       }
     }
     __threadfence();
+    fence_proxy_async();
     *flag = ok;
   }
   __syncthreads();
@@ -173,36 +225,28 @@ __device__ __forceinline__ double* hist_ptr(const KParams& kp, int rid, int kind
   return kp.hist + ((size_t)rid * H_NKIND + kind) * (size_t)kp.hist_len + idx;
 }
 
-template <class V>
-__device__ __forceinline__ V* vec_ptr(const GroupDev& g, int inst, int slot, int which) {
-  return reinterpret_cast<V*>(g.vec + (long long)(inst * g.nrhs + slot) * g.vec_stride + g.vec_off[which]);
+template <class T>
+__device__ __forceinline__ T* vec_ptr(const GroupDev& g, int inst, int slot, int which) {
+  return reinterpret_cast<T*>(g.vec + (long long)(inst * g.nrhs + slot) * g.vec_stride + g.vec_off[which]);
 }
-enum VecId { V_X = 0, V_R0 = 1, V_R1 = 2, V_S0 = 3, V_S1 = 4, V_Z = 5, V_Q = 6 };
+template <class T>
+__device__ __forceinline__ T* halo_ptr(const GroupDev& g, int inst, int slot, int which) {
+  return reinterpret_cast<T*>(g.halo + (long long)(inst * g.nrhs + slot) * g.halo_stride + g.halo_off[which]);
+}
 
-// does a solve with action `a` stage a neighbour field in pass `pt`?
-__device__ __forceinline__ bool stages(int pt, int a) {
-  if (a == A_NONE || a == A_FIN) return false;
-  return pt == P_INIT || pt == P_Z || pt == P_S || pt == P_X;
-}
-// number of sums a solve contributes in pass `pt`
-__device__ __forceinline__ int nsums(int pt, int a) {
-  if (a == A_NONE || a == A_FIN) return 0;
-  switch (pt) {
-    case P_INIT: return 2;                     // r.r, sum(b)
-    case P_Z: return 1;                        // z.r
-    case P_S: return 1;                        // s.q
-    case P_X: return a == A_REPLACE ? 1 : 2;   // r.r (, z.r)
-    default: return 0;
-  }
-}
-__device__ __forceinline__ int hist_kind(int pt, int a, int kind) {
-  switch (pt) {
-    case P_INIT: return kind == 0 ? H_RRR : H_SUM;
-    case P_Z: return H_ETAZ;
-    case P_S: return H_SQ;
-    case P_X: return a == A_REPLACE ? H_RRR : (kind == 0 ? H_RRX : H_ETAX);
-    default: return 0;
-  }
+// store the value of point (t, j, i) into the halo slices of the tiles that read it across an edge
+template <class T>
+__device__ __forceinline__ void push(const TopoDev& tp, T* halo, int t, int j, int i, T v) {
+  int e;
+  if (i == 0) e = j;
+  else if (i == tp.ni - 1) e = tp.nj + j;
+  else if (j == 0) e = 2 * tp.nj + i;
+  else if (j == tp.nj - 1) e = 2 * tp.nj + tp.ni + i;
+  else return;
+  const int* tg = tp.tg + ((size_t)t * (2 * tp.nj + 2 * tp.ni) + e) * 2;
+  const int s0 = __ldg(tg), s1 = __ldg(tg + 1);
+  if (s0 >= 0) stcg(halo + s0, v);
+  if (s1 >= 0) stcg(halo + s1, v);
 }
 
 // compact index -> padded index of the same point
@@ -215,195 +259,212 @@ __device__ __forceinline__ long long cmp_to_pad(const TopoDev& tp, int c) {
   return ((long long)t * tp.npy + (j + tp.OLy)) * tp.npx + (i + tp.OLx);
 }
 
+// number of sums a solve contributes in pass `pt`, and where each goes
+__device__ __forceinline__ int nsums(int pt, int a) {
+  if (a != A_ACTIVE) return 0;
+  switch (pt) {
+    case P_INIT: return 2;   // r.r, sum(b)
+    case P_Z: return 1;      // z.r
+    case P_S: return 1;      // s.q
+    case P_X: return 2;      // r.r, z.r
+    case P_R: return 1;      // r.r
+    default: return 0;
+  }
+}
+__device__ __forceinline__ int hist_kind(int pt, int kind) {
+  switch (pt) {
+    case P_INIT: return kind == 0 ? H_RRR : H_SUM;
+    case P_Z: return H_ETAZ;
+    case P_S: return H_SQ;
+    case P_X: return kind == 0 ? H_RRX : H_ETAX;
+    case P_R: return H_RRR;
+    default: return 0;
+  }
+}
+
+// which solve slots of an instance take part, and their scalars
+struct SlotInfo {
+  int rid[2], act[2], has_alpha[2];
+  double c1[2], c2[2], rnorm[2], norm[2];
+};
+__device__ __forceinline__ void slot_info(const GroupDev& g, int inst, const Smem& sm, SlotInfo& si) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const bool on = s < g.nrhs;
+    const int r = g.rhs_base + inst * g.nrhs + s;
+    si.rid[s] = r;
+    si.act[s] = on ? sm.act[r] : A_NONE;
+    si.c1[s] = on ? sm.c1[r] : 0.0;
+    si.c2[s] = on ? sm.c2[r] : 0.0;
+    si.rnorm[s] = on ? sm.rnorm[r] : 1.0;
+    si.norm[s] = on ? sm.norm[r] : 1.0;
+    si.has_alpha[s] = on ? sm.has_alpha[r] : 0;
+  }
+}
+
 // ------------------------------------------------------------------------------------------------
-// one work unit: rows [j0, j1) of tile t of one instance, in chunks of kWarps rows
+// row sums of one chunk into the unit partials, and the unit partials into the instance sums
+
+// warp w holds per-lane partials lp of row w: xor butterfly (every lane ends with the same value)
+__device__ __forceinline__ void row_sums(const GroupDev& g, const double (&lp)[2][2], const Smem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = 0; s < g.nrhs; ++s)
+    for (int q = 0; q < 2; ++q) {
+      double v = lp[s][q];
+      for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (lane == 0) sm.rowsum[(s * 2 + q) * kWarps + warp] = v;
+    }
+}
+
+// thread 0: add the chunk's rows (ROWBLOCK: row sums in order; FORTRAN: every product in j, i order)
+__device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupDev& g, int pt, const SlotInfo& si,
+                                                 int nr, double (&acc)[2][2], const Smem& sm) {
+  for (int s = 0; s < g.nrhs; ++s) {
+    const int ns = nsums(pt, si.act[s]);
+    for (int q = 0; q < ns; ++q) {
+      double a = acc[s][q];
+      if (kp.serial) {
+        const double* pr = sm.prod + ((s * 2 + q) * kWarps) * kp.max_ni;
+        for (int w = 0; w < nr; ++w)
+          for (int i = 0; i < g.tp.ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
+      } else {
+        for (int w = 0; w < nr; ++w) a = add(a, sm.rowsum[(s * 2 + q) * kWarps + w]);
+      }
+      acc[s][q] = a;
+    }
+  }
+}
+
+// thread 0 writes the unit's partials; the CTA that completes an instance's last unit forms the
+// instance's sums in fixed order: blocks of a tile in order, then tiles in order from 0
+// (GLOBAL_SUM_TILE, global_sum.py:20-26)
+__device__ void finish_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int pt, int hidx,
+                            const SlotInfo& si, const double (&acc)[2][2], const Smem& sm) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int any = 0;
+  for (int s = 0; s < g.nrhs; ++s) any |= nsums(pt, si.act[s]);
+  if (!any) return;
+  if (tid == 0) {
+    for (int s = 0; s < g.nrhs; ++s) {
+      const int ns = nsums(pt, si.act[s]);
+      for (int q = 0; q < ns; ++q) stcg(kp.part + ((size_t)si.rid[s] * 2 + q) * kp.part_units + lu, acc[s][q]);
+    }
+    __threadfence();
+    const unsigned old = atomicAdd(&kp.cnt[g.op_base + inst], 1u);
+    sm.misc[1] = ((old + 1u) % (unsigned)g.units) == 0u;
+  }
+  __syncthreads();
+  if (sm.misc[1] && warp == 0) {
+    __threadfence();
+    const int T = g.tp.T;
+    for (int s = 0; s < g.nrhs; ++s) {
+      const int ns = nsums(pt, si.act[s]);
+      for (int q = 0; q < ns; ++q) {
+        const double* P = kp.part + ((size_t)si.rid[s] * 2 + q) * kp.part_units;
+        for (int tt = lane; tt < T; tt += 32) {
+          double a = 0.0;
+          for (int b = 0; b < g.nblk; ++b) a = add(a, ldcg(P + tt * g.nblk + b));
+          sm.tsum[tt] = a;
+        }
+        __syncwarp();
+        if (lane == 0) {
+          double a = 0.0;
+          for (int tt = 0; tt < T; ++tt) a = add(a, sm.tsum[tt]);
+          stcg(hist_ptr(kp, si.rid[s], hist_kind(pt, q), hidx), a);
+        }
+        __syncwarp();
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// the two passes that run once per solve (rhsMax; x, r, s initialisation): direct loads, neighbours
+// through the gather tables
 
 template <bool MIXED>
-__device__ void process_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int pt, int k, int hidx,
-                             const Smem& sm) {
+__device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int inst, int lu, int pt, const Smem& sm) {
   using V = typename Prec<MIXED>::V;
-  using C = typename Prec<MIXED>::C;
   const TopoDev& tp = g.tp;
   const int ni = tp.ni, nj = tp.nj, npx = tp.npx;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int t = lu / g.nblk, blk = lu - (lu / g.nblk) * g.nblk;
   const int R = kp.serial ? nj : kp.rows_per_block;
   const int j0 = blk * R, j1 = min(nj, j0 + R);
-  const int op = g.op_base + inst;
   const long long pe = g.pad_elems;
-  const int W = ni + 2;                                    // staged row width (cols -1..ni)
-  const int SW = (kWarps + 2) * (kp.max_ni + 2);           // staged slot size
-
-  int rid[2], act[2];
-  double c1[2], c2[2], rnorm[2], norm[2];
-  int has_alpha[2];
-  for (int s = 0; s < 2; ++s) {
-    rid[s] = g.rhs_base + inst * g.nrhs + s;
-    act[s] = (s < g.nrhs) ? sm.act[rid[s]] : A_NONE;
-    c1[s] = (s < g.nrhs) ? sm.c1[rid[s]] : 0.0;
-    c2[s] = (s < g.nrhs) ? sm.c2[rid[s]] : 0.0;
-    rnorm[s] = (s < g.nrhs) ? sm.rnorm[rid[s]] : 1.0;
-    norm[s] = (s < g.nrhs) ? sm.norm[rid[s]] : 1.0;
-    has_alpha[s] = (s < g.nrhs) ? sm.has_alpha[rid[s]] : 0;
-  }
-
-  // coefficients of this instance: FP64 (caller) and the type the CG stencils use
+  const int W = ni + 2;
+  const int SW = (kWarps + 2) * (kp.max_ni + 2);
+  double* stage = reinterpret_cast<double*>(sm.stage);
+  SlotInfo si;
+  slot_info(g, inst, sm, si);
   const double* aW = g.a64[0] + inst * pe;
   const double* aS = g.a64[1] + inst * pe;
   const double* aC = g.a64[2] + inst * pe;
-  const double* pW = g.a64[3] + inst * pe;
-  const double* pS = g.a64[4] + inst * pe;
-  const double* pC = g.a64[5] + inst * pe;
-  const C *cW, *cS, *cC, *qW, *qS, *qC;
-  if constexpr (MIXED) {
-    const float* base = g.c32 + (long long)inst * 6 * pe;
-    cW = base; cS = base + pe; cC = base + 2 * pe; qW = base + 3 * pe; qS = base + 4 * pe; qC = base + 5 * pe;
-  } else {
-    cW = aW; cS = aS; cC = aC; qW = pW; qS = pS; qC = pC;
-  }
 
-  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};   // thread 0: unit partial sums
-  unsigned long long vmax[2] = {0ull, 0ull};       // P_MAX: max |b cg2dNorm| as ordered bits (NaN wins)
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  unsigned long long vmax[2] = {0ull, 0ull};
 
   for (int jc = j0; jc < j1; jc += kWarps) {
     const int nr = min(kWarps, j1 - jc);
-
-    // ---- stage the neighbour field of every staging solve: rows jc-1 .. jc+nr, cols -1 .. ni
-    bool any_stage = false;
-    for (int s = 0; s < g.nrhs; ++s) any_stage |= stages(pt, act[s]);
-    if (any_stage) {
+    if (pt == P_INIT) {
+      // x0 scaled by rhsNorm at the chunk's rows and neighbours (cg2d.py:227-228): interior points are
+      // scaled, unwritten halo points keep cg2d_x
       const int total = (nr + 2) * W;
       for (int idx = tid; idx < total; idx += kThreads) {
-        const int rr = idx / W;
-        const int cc = idx - rr * W;
+        const int rr = idx / W, cc = idx - (idx / W) * W;
         const int j = jc + rr - 1, i = cc - 1;
-        const bool own = (rr >= 1 && rr <= nr);
-        const bool iin = (i >= 0 && i < ni);
-        if (!own && !iin) continue;           // corner cells: the 5-point stencil never reads them
+        const bool own = (rr >= 1 && rr <= nr), iin = (i >= 0 && i < ni);
+        if (!own && !iin) continue;
         int src;
-        long long hp = -1;                    // padded position of this halo cell in its own tile
+        long long hp = -1;
         if (iin && j >= 0 && j < nj) {
           src = (t * nj + j) * ni + i;
         } else {
-          if (i < 0) src = tp.nbr[0 * tp.T * nj + t * nj + j];
-          else if (i >= ni) src = tp.nbr[1 * tp.T * nj + t * nj + j];
+          if (i < 0) src = tp.nbr[t * nj + j];
+          else if (i >= ni) src = tp.nbr[tp.T * nj + t * nj + j];
           else if (j < 0) src = tp.nbr[2 * tp.T * nj + t * ni + i];
           else src = tp.nbr[2 * tp.T * nj + tp.T * ni + t * ni + i];
           hp = ((long long)t * tp.npy + (j + tp.OLy)) * npx + (i + tp.OLx);
         }
         for (int s = 0; s < g.nrhs; ++s) {
-          if (!stages(pt, act[s])) continue;
-          double v = 0.0;
-          if (pt == P_INIT) {
-            const double* x0 = g.x0[s] + inst * pe;
-            // cg2d.py:227-228: interior scaled by rhsNorm, exchanged; unwritten halo points keep cg2d_x
-            v = (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), rnorm[s]) : __ldg(x0 + hp);
-          } else if (pt == P_Z) {
-            const V* r = vec_ptr<V>(g, inst, s, (hidx & 1) ? V_R1 : V_R0);
-            v = (src >= 0) ? (double)ldcg(r + src) : 0.0;
-          } else if (pt == P_S) {
-            // s_k(nbr) = z_k(nbr) + beta_k s_{k-1}(nbr)   (cg2d.py:249; halo points never written hold 0)
-            const V* z = vec_ptr<V>(g, inst, s, V_Z);
-            const V* so = vec_ptr<V>(g, inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
-            if (src >= 0) v = (double)(V)add((double)ldcg(z + src), mul(c1[s], (double)ldcg(so + src)));
-          } else {  // P_X
-            if (act[s] == A_REPLACE) {
-              // x_{k+1}(nbr) = x_k(nbr) + alpha_k s_k(nbr); unwritten halo points keep cg2d_x
-              const double* x = vec_ptr<double>(g, inst, s, V_X);
-              const V* sk = vec_ptr<V>(g, inst, s, (k & 1) ? V_S1 : V_S0);
-              v = (src >= 0) ? add(ldcg(x + src), mul(c1[s], (double)ldcg(sk + src)))
-                             : __ldg(g.x0[s] + inst * pe + hp);
-            } else {
-              // r_{k+1}(nbr) = r_k(nbr) - alpha_k q_k(nbr)   (cg2d.py:255)
-              const V* ro = vec_ptr<V>(g, inst, s, (k & 1) ? V_R1 : V_R0);
-              const V* q = vec_ptr<V>(g, inst, s, V_Q);
-              if (src >= 0) v = (double)(V)sub((double)ldcg(ro + src), mul(c1[s], (double)ldcg(q + src)));
-            }
-          }
-          sm.stage[s * SW + rr * W + cc] = v;
+          if (si.act[s] != A_ACTIVE) continue;
+          const double* x0 = g.x0[s] + inst * pe;
+          stage[s * SW + rr * W + cc] =
+              (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), si.rnorm[s]) : __ldg(x0 + hp);
         }
       }
       __syncthreads();
     }
-
-    // ---- compute: warp w owns row jc + w, lane owns i = lane + 32m
     double lp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
     if (warp < nr) {
       const int j = jc + warp;
-      const long long prow = ((long long)t * tp.npy + (j + tp.OLy)) * npx + tp.OLx;   // padded (j, 0)
-      const int crow = (t * nj + j) * ni;                                               // compact (j, 0)
+      const long long prow = ((long long)t * tp.npy + (j + tp.OLy)) * npx + tp.OLx;
       for (int i = lane; i < ni; i += 32) {
         const long long po = prow + i;
-        const int pc = crow + i;
-        const int sc = (warp + 1) * W + (i + 1);   // staged centre
         for (int s = 0; s < g.nrhs; ++s) {
-          const int a = act[s];
-          if (a == A_NONE) continue;
-          const double* st = sm.stage + s * SW;
+          if (si.act[s] != A_ACTIVE) continue;
           double p0 = 0.0, p1 = 0.0;
           if (pt == P_MAX) {
             const double bv = __ldg(g.b[s] + inst * pe + po);
-            const unsigned long long m = (unsigned long long)__double_as_longlong(fabs(mul(bv, norm[s])));  // cg2d.py:222-223
+            const unsigned long long m =
+                (unsigned long long)__double_as_longlong(fabs(mul(bv, si.norm[s])));   // cg2d.py:222-223
             vmax[s] = m > vmax[s] ? m : vmax[s];
-          } else if (pt == P_INIT) {
+          } else {
+            const double* st = stage + s * SW;
+            const int sc = (warp + 1) * W + (i + 1);
             const double vc = st[sc], vw = st[sc - 1], ve = st[sc + 1], vs = st[sc - W], vn = st[sc + W];
-            stcg(vec_ptr<double>(g, inst, s, V_X) + pc, vc);
-            const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), norm[s]), rnorm[s]);   // cg2d.py:221,226
+            stcg(vec_ptr<double>(g, inst, s, V_X) + (t * nj + j) * g.ldx + i, vc);
+            const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), si.norm[s]), si.rnorm[s]);   // cg2d.py:221,226
             const double ax = op_A<double>(__ldg(aW + po), __ldg(aW + po + 1), __ldg(aS + po), __ldg(aS + po + npx),
                                            __ldg(aC + po), vw, ve, vs, vn, vc);
             const V r0 = (V)sub(bn, ax);                                                   // cg2d.py:232
-            stcg(vec_ptr<V>(g, inst, s, V_R0) + pc, r0);
-            stcg(vec_ptr<V>(g, inst, s, V_S1) + pc, (V)0);                                 // s = 0 (cg2d.py:231)
+            stcg(vec_ptr<V>(g, inst, s, V_R0) + (t * nj + j) * g.ldv + i, r0);
+            push(tp, halo_ptr<V>(g, inst, s, V_R0), t, j, i, r0);
+            stcg(vec_ptr<V>(g, inst, s, V_S1) + (t * nj + j) * g.ldv + i, (V)0);         // s = 0 (cg2d.py:231)
             p0 = mul((double)r0, (double)r0);
             p1 = bn;
-          } else if (pt == P_Z) {
-            const C vc = (C)st[sc], vw = (C)st[sc - 1], ve = (C)st[sc + 1], vs = (C)st[sc - W], vn = (C)st[sc + W];
-            const V z = (V)op_M<C>(__ldg(qC + po), __ldg(qW + po), __ldg(qW + po + 1), __ldg(qS + po),
-                                   __ldg(qS + po + npx), vc, vw, ve, vs, vn);
-            stcg(vec_ptr<V>(g, inst, s, V_Z) + pc, z);
-            p0 = mul((double)z, (double)vc);                     // cg2d.py:246
-          } else if (pt == P_S) {
-            const V* so = vec_ptr<V>(g, inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
-            double* x = vec_ptr<double>(g, inst, s, V_X);
-            if (a == A_FIN) {
-              double xv = ldcg(x + pc);
-              if (has_alpha[s]) xv = add(xv, mul(c2[s], (double)ldcg(so + pc)));   // cg2d.py:254
-              const double xf = __ddiv_rn(xv, rnorm[s]);                          // cg2d.py:266
-              g.x_out[s][inst * pe + po] = xf;
-              if (g.x_fortran[s]) g.x_fortran[s][inst * pe + po] = xf;
-            } else {
-              const C vc = (C)st[sc], vw = (C)st[sc - 1], ve = (C)st[sc + 1], vs = (C)st[sc - W], vn = (C)st[sc + W];
-              stcg(vec_ptr<V>(g, inst, s, (k & 1) ? V_S1 : V_S0) + pc, (V)vc);
-              const V q = (V)op_A<C>(__ldg(cW + po), __ldg(cW + po + 1), __ldg(cS + po), __ldg(cS + po + npx),
-                                     __ldg(cC + po), vw, ve, vs, vn, vc);                 // cg2d.py:251
-              stcg(vec_ptr<V>(g, inst, s, V_Q) + pc, q);
-              if (has_alpha[s]) {
-                const double xv = ldcg(x + pc);
-                stcg(x + pc, add(xv, mul(c2[s], (double)ldcg(so + pc))));
-              }
-              p0 = mul((double)vc, (double)q);                                             // cg2d.py:252
-            }
-          } else {  // P_X
-            V* rn = vec_ptr<V>(g, inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
-            if (a == A_REPLACE) {
-              const double vc = st[sc], vw = st[sc - 1], ve = st[sc + 1], vs = st[sc - W], vn = st[sc + W];
-              const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), norm[s]), rnorm[s]);
-              const double ax = op_A<double>(__ldg(aW + po), __ldg(aW + po + 1), __ldg(aS + po),
-                                             __ldg(aS + po + npx), __ldg(aC + po), vw, ve, vs, vn, vc);
-              const V r = (V)sub(bn, ax);
-              stcg(rn + pc, r);
-              p0 = mul((double)r, (double)r);
-            } else {
-              const C vc = (C)st[sc], vw = (C)st[sc - 1], ve = (C)st[sc + 1], vs = (C)st[sc - W], vn = (C)st[sc + W];
-              stcg(rn + pc, (V)vc);
-              const V z = (V)op_M<C>(__ldg(qC + po), __ldg(qW + po), __ldg(qW + po + 1), __ldg(qS + po),
-                                     __ldg(qS + po + npx), vc, vw, ve, vs, vn);            // cg2d.py:245
-              stcg(vec_ptr<V>(g, inst, s, V_Z) + pc, z);
-              p0 = mul((double)vc, (double)vc);                                            // cg2d.py:256
-              p1 = mul((double)z, (double)vc);                                             // cg2d.py:246
-            }
           }
-          if (kp.serial) {
+          if (kp.serial && pt != P_MAX) {
             double* pr = sm.prod + ((s * 2 + 0) * kWarps + warp) * kp.max_ni;
             pr[i] = p0;
             pr[kWarps * kp.max_ni + i] = p1;
@@ -423,95 +484,412 @@ __device__ void process_unit(const KParams& kp, const GroupDev& g, int inst, int
           vmax[s] = m;
         }
       } else if (!kp.serial) {
-        // row sum: xor butterfly over the lanes (every lane ends with the same value)
-        for (int s = 0; s < g.nrhs; ++s)
-          for (int q = 0; q < 2; ++q) {
-            double v = lp[s][q];
-            for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
-            if (lane == 0) sm.rowsum[(s * 2 + q) * kWarps + warp] = v;
-          }
+        row_sums(g, lp, sm);
       }
     }
     if (pt == P_MAX) {
-      if (warp < nr && lane == 0) {
+      if (warp < nr && lane == 0)
         for (int s = 0; s < g.nrhs; ++s)
-          if (act[s] != A_NONE)
-            atomicMax(&kp.rmax[rid[s]], vmax[s]);
-      }
+          if (si.act[s] == A_ACTIVE) atomicMax(&kp.rmax[si.rid[s]], vmax[s]);
       __syncthreads();
       continue;
     }
     __syncthreads();
-    if (tid == 0) {
-      for (int s = 0; s < g.nrhs; ++s) {
-        const int ns = nsums(pt, act[s]);
-        for (int q = 0; q < ns; ++q) {
-          double a = acc[s][q];
-          if (kp.serial) {
-            const double* pr = sm.prod + ((s * 2 + q) * kWarps) * kp.max_ni;
-            for (int w = 0; w < nr; ++w)
-              for (int i = 0; i < ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
-          } else {
-            for (int w = 0; w < nr; ++w) a = add(a, sm.rowsum[(s * 2 + q) * kWarps + w]);
-          }
-          acc[s][q] = a;
-        }
-      }
-    }
+    if (tid == 0) accumulate_chunk(kp, g, pt, si, nr, acc, sm);
   }
-
   if (pt == P_MAX) return;
-
-  // ---- unit partials, then the last unit of the instance forms the instance's sums in fixed order
-  int any_sum = 0;
-  for (int s = 0; s < g.nrhs; ++s) any_sum |= nsums(pt, act[s]);
-  if (!any_sum) return;
-  if (tid == 0) {
-    for (int s = 0; s < g.nrhs; ++s) {
-      const int ns = nsums(pt, act[s]);
-      for (int q = 0; q < ns; ++q) stcg(kp.part + ((size_t)rid[s] * 2 + q) * kp.part_units + lu, acc[s][q]);
-    }
-    __threadfence();
-    const unsigned old = atomicAdd(&kp.cnt[op], 1u);
-    sm.misc[1] = ((old + 1u) % (unsigned)g.units) == 0u;
-  }
-  __syncthreads();
-  if (sm.misc[1] && warp == 0) {
-    __threadfence();
-    for (int s = 0; s < g.nrhs; ++s) {
-      const int ns = nsums(pt, act[s]);
-      for (int q = 0; q < ns; ++q) {
-        const double* P = kp.part + ((size_t)rid[s] * 2 + q) * kp.part_units;
-        for (int tt = lane; tt < tp.T; tt += 32) {       // tile partial: blocks in order from 0
-          double a = 0.0;
-          for (int b = 0; b < g.nblk; ++b) a = add(a, ldcg(P + tt * g.nblk + b));
-          sm.tsum[tt] = a;
-        }
-        __syncwarp();
-        if (lane == 0) {                                  // GLOBAL_SUM_TILE: tiles in order from 0
-          double a = 0.0;
-          for (int tt = 0; tt < tp.T; ++tt) a = add(a, sm.tsum[tt]);
-          stcg(hist_ptr(kp, rid[s], hist_kind(pt, act[s], q), hidx), a);
-        }
-        __syncwarp();
-      }
-    }
-  }
+  finish_unit(kp, g, inst, lu, pt, 0, si, acc, sm);
 }
 
 template <bool MIXED>
-__device__ void run_pass(const KParams& kp, int pt, int k, int hidx, const Smem& sm) {
+__device__ void run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
   for (int u = blockIdx.x; u < kp.total_units; u += gridDim.x) {
     int gi = 0;
     while (gi + 1 < kp.ngroups && u >= kp.g[gi + 1].unit_base) ++gi;
     const GroupDev& g = kp.g[gi];
     const int rel = u - g.unit_base;
     const int inst = rel / g.units;
-    const int lu = rel - inst * g.units;
     if (!sm.opp[g.op_base + inst]) continue;
-    process_unit<MIXED>(kp, g, inst, lu, pt, k, hidx, sm);
+    process_unit_direct<MIXED>(kp, g, inst, rel - inst * g.units, pt, sm);
   }
 }
+
+// x halo slices at the start: the exchanged normalised first guess; unwritten points keep cg2d_x
+// (cg2d.py:227-228). Later values are pushed by the owners as x is updated.
+__device__ void init_x_halo(const KParams& kp, const Smem& sm) {
+  const long long gstride = (long long)gridDim.x * kThreads;
+  for (int gg = 0; gg < kp.ngroups; ++gg) {
+    const GroupDev& g = kp.g[gg];
+    const TopoDev& tp = g.tp;
+    const long long per = (long long)tp.T * (2 * tp.njp + 2 * tp.nip);
+    const long long tot = per * g.count * g.nrhs;
+    for (long long idx = (long long)blockIdx.x * kThreads + threadIdx.x; idx < tot; idx += gstride) {
+      const long long ins_slot = idx / per;
+      const int h = (int)(idx - ins_slot * per);
+      const int inst = (int)(ins_slot / g.nrhs), s = (int)(ins_slot - (long long)inst * g.nrhs);
+      int t, kk, j, i, src;
+      if (h < 2 * tp.T * tp.njp) {
+        const int side = h / (tp.T * tp.njp);
+        const int r = h - side * tp.T * tp.njp;
+        t = r / tp.njp; kk = r - t * tp.njp;
+        if (kk >= tp.nj) continue;
+        j = kk; i = side == 0 ? -1 : tp.ni;
+        src = tp.nbr[side * tp.T * tp.nj + t * tp.nj + kk];
+      } else {
+        const int h2 = h - 2 * tp.T * tp.njp;
+        const int side = h2 / (tp.T * tp.nip);
+        const int r = h2 - side * tp.T * tp.nip;
+        t = r / tp.nip; kk = r - t * tp.nip;
+        if (kk >= tp.ni) continue;
+        i = kk; j = side == 0 ? -1 : tp.nj;
+        src = tp.nbr[2 * tp.T * tp.nj + side * tp.T * tp.ni + t * tp.ni + kk];
+      }
+      const double* x0 = g.x0[s] + inst * g.pad_elems;
+      const double rn = sm.rnorm[g.rhs_base + inst * g.nrhs + s];
+      const double v = (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), rn)
+                                  : __ldg(x0 + ((long long)t * tp.npy + (j + tp.OLy)) * tp.npx + (i + tp.OLx));
+      halo_ptr<double>(g, inst, s, V_X)[h] = v;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// pipelined passes: chunks of this CTA in order, bulk copies into two stage buffers
+
+struct Chunk {
+  int u, gi, inst, lu, t, j0u, j1u, jc, nr;
+};
+
+__device__ bool chunk_unit(const KParams& kp, const Smem& sm, int u, Chunk& c) {
+  for (; u < kp.total_units; u += gridDim.x) {
+    int gi = 0;
+    while (gi + 1 < kp.ngroups && u >= kp.g[gi + 1].unit_base) ++gi;
+    const GroupDev& g = kp.g[gi];
+    const int rel = u - g.unit_base;
+    const int inst = rel / g.units;
+    if (!sm.opp[g.op_base + inst]) continue;
+    const int lu = rel - inst * g.units;
+    const int t = lu / g.nblk, blk = lu - t * g.nblk;
+    const int R = kp.serial ? g.tp.nj : kp.rows_per_block;
+    c.u = u; c.gi = gi; c.inst = inst; c.lu = lu; c.t = t;
+    c.j0u = blk * R;
+    c.j1u = min(g.tp.nj, c.j0u + R);
+    c.jc = c.j0u;
+    c.nr = min(kp.ch, c.j1u - c.jc);
+    return true;
+  }
+  return false;
+}
+__device__ bool chunk_next(const KParams& kp, const Smem& sm, Chunk& c) {
+  if (c.jc + kp.ch < c.j1u) {
+    c.jc += kp.ch;
+    c.nr = min(kp.ch, c.j1u - c.jc);
+    return true;
+  }
+  return chunk_unit(kp, sm, c.u + gridDim.x, c);
+}
+
+// the vectors a pass stages (with their neighbours) for an active solve
+__device__ __forceinline__ void pass_vectors(int pt, int k, int hidx, int (&ids)[2]) {
+  if (pt == P_S) { ids[0] = V_Z; ids[1] = ((k + 1) & 1) ? V_S1 : V_S0; }
+  else if (pt == P_X) { ids[0] = (k & 1) ? V_R1 : V_R0; ids[1] = V_Q; }
+  else if (pt == P_R) { ids[0] = V_X; ids[1] = (k & 1) ? V_S1 : V_S0; }
+  else { ids[0] = (hidx & 1) ? V_R1 : V_R0; ids[1] = -1; }
+}
+
+// thread 0: bulk copies of chunk c into the stage buffer sb, completion on bar
+template <bool MIXED>
+__device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, int hidx, const Smem& sm,
+                            unsigned char* sb, unsigned long long* bar) {
+  const GroupDev& g = kp.g[c.gi];
+  const TopoDev& tp = g.tp;
+  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.npx, g.ldv, g.ldx, g.ldc);
+  int act[2], hasal[2];
+  bool any = false;
+  for (int s = 0; s < 2; ++s) {
+    const int r = g.rhs_base + c.inst * g.nrhs + s;
+    act[s] = s < g.nrhs ? sm.act[r] : A_NONE;
+    hasal[s] = s < g.nrhs ? sm.has_alpha[r] : 0;
+    any |= act[s] == A_ACTIVE;
+  }
+  // two passes over the same plan: count the bytes and arm the mbarrier, then issue the copies
+  const int first = (pt == P_X || pt == P_Z) ? 3 : 0;   // M = (pW, pS, pC) or A = (aW2d, aS2d, aC2d)
+  int ids[2];
+  pass_vectors(pt, k, hidx, ids);
+  const int jlo = max(c.jc - 1, 0), jhi = min(c.jc + c.nr, tp.nj - 1);
+  unsigned total = 0;
+  for (int go = 0; go < 2; ++go) {
+    auto cp = [&](void* d, const void* s_, unsigned bytes) {
+      if (go) bulk_g2s(d, s_, bytes, bar);
+      else total += bytes;
+    };
+    if (any) {
+      for (int a = 0; a < 3; ++a) {
+        const void* base;
+        if (L.csize == 8)
+          base = g.a64[first + a] + (long long)c.inst * g.pad_elems +
+                 ((long long)c.t * tp.npy + c.jc + tp.OLy) * tp.npx;
+        else
+          base = g.c32 + (((long long)c.inst * 6 + first + a) * tp.T * tp.npy + (long long)c.t * tp.npy + c.jc +
+                          tp.OLy) * g.ldc;
+        cp(sb + L.coef + a * L.coef_stride, base, (unsigned)((c.nr + 1) * L.cpitch * L.csize));
+      }
+    }
+    for (int s = 0; s < g.nrhs; ++s) {
+      if (act[s] != A_ACTIVE) continue;
+      for (int v = 0; v < L.nvec; ++v) {
+        const int sz = L.vsize[v], P = L.vpitch[v];
+        const char* vb = vec_ptr<const char>(g, c.inst, s, ids[v]);
+        const char* hb = halo_ptr<const char>(g, c.inst, s, ids[v]);
+        cp(sb + L.vec[s][v] + (jlo - c.jc + 1) * P * sz, vb + (long long)(c.t * tp.nj + jlo) * P * sz,
+           (unsigned)((jhi - jlo + 1) * P * sz));
+        const unsigned hbytes = al16((unsigned)(c.nr * sz));
+        cp(sb + L.hw[s][v], hb + ((long long)c.t * tp.njp + c.jc) * sz, hbytes);
+        cp(sb + L.he[s][v], hb + ((long long)(tp.T + c.t) * tp.njp + c.jc) * sz, hbytes);
+        if (c.jc == 0)
+          cp(sb + L.vec[s][v], hb + ((long long)2 * tp.T * tp.njp + (long long)c.t * tp.nip) * sz,
+             al16((unsigned)(tp.ni * sz)));
+        if (c.jc + c.nr == tp.nj)
+          cp(sb + L.vec[s][v] + (c.nr + 1) * P * sz,
+             hb + ((long long)2 * tp.T * tp.njp + (long long)(tp.T + c.t) * tp.nip) * sz, al16((unsigned)(tp.ni * sz)));
+      }
+      if (pt == P_S && hasal[s]) {
+        const char* xb = vec_ptr<const char>(g, c.inst, s, V_X);
+        cp(sb + L.xo[s], xb + (long long)(c.t * tp.nj + c.jc) * g.ldx * 8, (unsigned)(c.nr * g.ldx * 8));
+      }
+    }
+    if (!go) {
+      fence_proxy_async();
+      mbar_arrive_expect_tx(bar, total);
+    }
+  }
+}
+
+// compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m
+template <bool MIXED>
+__device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const SlotInfo& si,
+                              const unsigned char* sb, double (&lp)[2][2], const Smem& sm) {
+  using V = typename Prec<MIXED>::V;
+  using C = typename Prec<MIXED>::C;
+  const GroupDev& g = kp.g[c.gi];
+  const TopoDev& tp = g.tp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp >= c.nr) return;
+  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.npx, g.ldv, g.ldx, g.ldc);
+  const int ni = tp.ni, nj = tp.nj, t = c.t, w = warp, j = c.jc + w;
+  const int CP = L.cpitch, col0 = tp.OLx;
+  const int crv = (t * nj + j) * g.ldv, crx = (t * nj + j) * g.ldx;
+  const long long pe = g.pad_elems;
+  const long long prow = (long long)c.inst * pe + ((long long)t * tp.npy + j + tp.OLy) * tp.npx + tp.OLx;
+
+  auto emit = [&](int s, int i, double p0, double p1) {
+    if (kp.serial) {
+      double* pr = sm.prod + ((s * 2) * kWarps + w) * kp.max_ni;
+      pr[i] = p0;
+      pr[kWarps * kp.max_ni + i] = p1;
+    } else {
+      lp[s][0] = add(lp[s][0], p0);
+      lp[s][1] = add(lp[s][1], p1);
+    }
+  };
+
+  for (int s = 0; s < g.nrhs; ++s) {
+    const int a = si.act[s];
+    if (a == A_NONE) continue;
+    if (a == A_FIN) {
+      // pass S after convergence: the pending x update, un-normalised (cg2d.py:254, 266)
+      const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
+      const double* x = vec_ptr<double>(g, c.inst, s, V_X);
+      for (int i = lane; i < ni; i += 32) {
+        double xv = ldcg(x + crx + i);
+        if (si.has_alpha[s]) xv = add(xv, mul(si.c2[s], (double)ldcg(so + crv + i)));
+        const double xf = __ddiv_rn(xv, si.rnorm[s]);
+        g.x_out[s][prow + i] = xf;
+        if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
+      }
+      continue;
+    }
+    const unsigned char* cb = sb + L.coef;
+    if (pt == P_S) {
+      const V* zr = reinterpret_cast<const V*>(sb + L.vec[s][0]);
+      const V* so = reinterpret_cast<const V*>(sb + L.vec[s][1]);
+      const V* hwz = reinterpret_cast<const V*>(sb + L.hw[s][0]);
+      const V* hws = reinterpret_cast<const V*>(sb + L.hw[s][1]);
+      const V* hez = reinterpret_cast<const V*>(sb + L.he[s][0]);
+      const V* hes = reinterpret_cast<const V*>(sb + L.he[s][1]);
+      const double* xo = reinterpret_cast<const double*>(sb + L.xo[s]);
+      const C* cw = reinterpret_cast<const C*>(cb);
+      const C* cs = reinterpret_cast<const C*>(cb + L.coef_stride);
+      const C* cc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
+      const int P = L.vpitch[0];
+      const double beta = si.c1[s], alpha_prev = si.c2[s];
+      const bool upd = si.has_alpha[s] != 0;
+      V* s_out = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
+      V* s_halo = halo_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
+      V* q_out = vec_ptr<V>(g, c.inst, s, V_Q);
+      V* q_halo = halo_ptr<V>(g, c.inst, s, V_Q);
+      double* x_out = vec_ptr<double>(g, c.inst, s, V_X);
+      double* x_halo = halo_ptr<double>(g, c.inst, s, V_X);
+      // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike
+      auto sn = [&](V zz, V ss) -> V { return (V)add((double)zz, mul(beta, (double)ss)); };
+      for (int i = lane; i < ni; i += 32) {
+        const int rc = (w + 1) * P + i;
+        const V vc = sn(zr[rc], so[rc]);
+        const V vw = (i > 0) ? sn(zr[rc - 1], so[rc - 1]) : sn(hwz[w], hws[w]);
+        const V ve = (i < ni - 1) ? sn(zr[rc + 1], so[rc + 1]) : sn(hez[w], hes[w]);
+        const V vs = sn(zr[rc - P], so[rc - P]);
+        const V vn = sn(zr[rc + P], so[rc + P]);
+        const int cr = w * CP + col0 + i;
+        const V q = (V)op_A<C>(cw[cr], cw[cr + 1], cs[cr], cs[cr + CP], cc[cr], (C)vw, (C)ve, (C)vs, (C)vn,
+                               (C)vc);                                                        // cg2d.py:251
+        stcg(s_out + crv + i, vc);
+        push(tp, s_halo, t, j, i, vc);
+        stcg(q_out + crv + i, q);
+        push(tp, q_halo, t, j, i, q);
+        if (upd) {
+          const double xn = add(xo[w * g.ldx + i], mul(alpha_prev, (double)so[rc]));         // cg2d.py:254
+          stcg(x_out + crx + i, xn);
+          push(tp, x_halo, t, j, i, xn);
+        }
+        emit(s, i, mul((double)vc, (double)q), 0.0);                                          // cg2d.py:252
+      }
+    } else if (pt == P_X) {
+      const V* ro = reinterpret_cast<const V*>(sb + L.vec[s][0]);
+      const V* qv = reinterpret_cast<const V*>(sb + L.vec[s][1]);
+      const V* hwr = reinterpret_cast<const V*>(sb + L.hw[s][0]);
+      const V* hwq = reinterpret_cast<const V*>(sb + L.hw[s][1]);
+      const V* her = reinterpret_cast<const V*>(sb + L.he[s][0]);
+      const V* heq = reinterpret_cast<const V*>(sb + L.he[s][1]);
+      const C* pw = reinterpret_cast<const C*>(cb);
+      const C* ps = reinterpret_cast<const C*>(cb + L.coef_stride);
+      const C* pc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
+      const int P = L.vpitch[0];
+      const double alpha = si.c1[s];
+      V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
+      V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
+      V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
+      V* z_halo = halo_ptr<V>(g, c.inst, s, V_Z);
+      // r_{k+1} = r_k - alpha_k q_k (cg2d.py:255)
+      auto rn = [&](V rr, V qq) -> V { return (V)sub((double)rr, mul(alpha, (double)qq)); };
+      for (int i = lane; i < ni; i += 32) {
+        const int rc = (w + 1) * P + i;
+        const V vc = rn(ro[rc], qv[rc]);
+        const V vw = (i > 0) ? rn(ro[rc - 1], qv[rc - 1]) : rn(hwr[w], hwq[w]);
+        const V ve = (i < ni - 1) ? rn(ro[rc + 1], qv[rc + 1]) : rn(her[w], heq[w]);
+        const V vs = rn(ro[rc - P], qv[rc - P]);
+        const V vn = rn(ro[rc + P], qv[rc + P]);
+        const int cr = w * CP + col0 + i;
+        const V z = (V)op_M<C>(pc[cr], pw[cr], pw[cr + 1], ps[cr], ps[cr + CP], (C)vc, (C)vw, (C)ve, (C)vs,
+                               (C)vn);                                                        // cg2d.py:245
+        stcg(r_out + crv + i, vc);
+        push(tp, r_halo, t, j, i, vc);
+        stcg(z_out + crv + i, z);
+        push(tp, z_halo, t, j, i, z);
+        emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));                 // cg2d.py:256, 246
+      }
+    } else if (pt == P_Z) {
+      const V* rr_ = reinterpret_cast<const V*>(sb + L.vec[s][0]);
+      const V* hw = reinterpret_cast<const V*>(sb + L.hw[s][0]);
+      const V* he = reinterpret_cast<const V*>(sb + L.he[s][0]);
+      const C* pw = reinterpret_cast<const C*>(cb);
+      const C* ps = reinterpret_cast<const C*>(cb + L.coef_stride);
+      const C* pc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
+      const int P = L.vpitch[0];
+      V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
+      V* z_halo = halo_ptr<V>(g, c.inst, s, V_Z);
+      for (int i = lane; i < ni; i += 32) {
+        const int rc = (w + 1) * P + i;
+        const V vc = rr_[rc];
+        const V vw = (i > 0) ? rr_[rc - 1] : hw[w];
+        const V ve = (i < ni - 1) ? rr_[rc + 1] : he[w];
+        const int cr = w * CP + col0 + i;
+        const V z = (V)op_M<C>(pc[cr], pw[cr], pw[cr + 1], ps[cr], ps[cr + CP], (C)vc, (C)vw, (C)ve,
+                               (C)rr_[rc - P], (C)rr_[rc + P]);
+        stcg(z_out + crv + i, z);
+        push(tp, z_halo, t, j, i, z);
+        emit(s, i, mul((double)z, (double)vc), 0.0);
+      }
+    } else {  // P_R: the FP64 true residual b - A x_{k+1}
+      const double* xr = reinterpret_cast<const double*>(sb + L.vec[s][0]);
+      const V* sk = reinterpret_cast<const V*>(sb + L.vec[s][1]);
+      const double* hwx = reinterpret_cast<const double*>(sb + L.hw[s][0]);
+      const V* hws = reinterpret_cast<const V*>(sb + L.hw[s][1]);
+      const double* hex = reinterpret_cast<const double*>(sb + L.he[s][0]);
+      const V* hes = reinterpret_cast<const V*>(sb + L.he[s][1]);
+      const double* aw = reinterpret_cast<const double*>(cb);
+      const double* as = reinterpret_cast<const double*>(cb + L.coef_stride);
+      const double* ac = reinterpret_cast<const double*>(cb + 2 * L.coef_stride);
+      const int PX = L.vpitch[0], PS = L.vpitch[1];
+      const double alpha = si.c1[s];
+      V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
+      V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
+      auto x1 = [&](double xx, V ss) -> double { return add(xx, mul(alpha, (double)ss)); };
+      for (int i = lane; i < ni; i += 32) {
+        const int rx = (w + 1) * PX + i, rs = (w + 1) * PS + i;
+        const double vc = x1(xr[rx], sk[rs]);
+        const double vw = (i > 0) ? x1(xr[rx - 1], sk[rs - 1]) : x1(hwx[w], hws[w]);
+        const double ve = (i < ni - 1) ? x1(xr[rx + 1], sk[rs + 1]) : x1(hex[w], hes[w]);
+        const double vs = x1(xr[rx - PX], sk[rs - PS]);
+        const double vn = x1(xr[rx + PX], sk[rs + PS]);
+        const int cr = w * CP + col0 + i;
+        const double bn = mul(mul(__ldg(g.b[s] + prow + i), si.norm[s]), si.rnorm[s]);
+        const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + CP], ac[cr], vw, ve, vs, vn, vc));
+        stcg(r_out + crv + i, r);
+        push(tp, r_halo, t, j, i, r);
+        emit(s, i, mul((double)r, (double)r), 0.0);
+      }
+    }
+  }
+}
+
+template <bool MIXED>
+__device__ bool run_pass_tma(const KParams& kp, int pt, int k, int hidx, const Smem& sm, unsigned& phase) {
+  const int tid = threadIdx.x;
+  Chunk cur;
+  if (!chunk_unit(kp, sm, blockIdx.x, cur)) return true;
+  const int ns = kp.nstage[pt];
+  int st = 0;
+  if (tid == 0) issue_chunk<MIXED>(kp, cur, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
+  Chunk nxt = cur;
+  bool have_next = chunk_next(kp, sm, nxt);
+  bool have = true;
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  while (have) {
+    if (ns == 2 && have_next && tid == 0)
+      issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage + (st ^ 1) * kp.stage_bytes, &sm.bar[st ^ 1]);
+    const bool ok = mbar_wait(&sm.bar[st], (phase >> st) & 1u, kp.timeout_ns);
+    phase ^= 1u << st;
+    if (__syncthreads_or(!ok)) {
+      // a copy did not complete in time: flag the error, give the copies in flight a bounded time to land
+      if (tid == 0) atomicCAS(&kp.gs[1], 0u, (unsigned)CG2D_BARRIER_TIMEOUT);
+      mbar_wait(&sm.bar[st], ((phase >> st) & 1u) ^ 1u, kp.timeout_ns);
+      if (ns == 2 && have_next) mbar_wait(&sm.bar[st ^ 1], (phase >> (st ^ 1)) & 1u, kp.timeout_ns);
+      __syncthreads();
+      return false;
+    }
+    const GroupDev& g = kp.g[cur.gi];
+    SlotInfo si;
+    slot_info(g, cur.inst, sm, si);
+    if (tid == 0 && cur.jc == cur.j0u) acc[0][0] = acc[0][1] = acc[1][0] = acc[1][1] = 0.0;
+    double lp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    compute_chunk<MIXED>(kp, cur, pt, k, si, sm.stage + st * kp.stage_bytes, lp, sm);
+    if ((tid >> 5) < cur.nr && !kp.serial) row_sums(g, lp, sm);
+    __syncthreads();
+    if (tid == 0) accumulate_chunk(kp, g, pt, si, cur.nr, acc, sm);
+    if (cur.jc + cur.nr >= cur.j1u) finish_unit(kp, g, cur.inst, cur.lu, pt, hidx, si, acc, sm);
+    if (ns == 1 && have_next) {
+      __syncthreads();
+      if (tid == 0) issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
+    }
+    cur = nxt;
+    have = have_next;
+    if (have) have_next = chunk_next(kp, sm, nxt);
+    if (ns == 2) st ^= 1;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------------------------------------
 
 // which group / instance / slot a global solve index belongs to
 __device__ __forceinline__ void locate(const KParams& kp, int r, int& gi, int& inst, int& slot) {
@@ -542,10 +920,17 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_constant__ KParams kp) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const Smem sm = carve(smem_raw, kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
   unsigned target = (unsigned)kp.test_missing;
+  unsigned phase = 0;
+  if (tid == 0) {
+    mbar_init(&sm.bar[0], 1);
+    mbar_init(&sm.bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
 
   // state of solve `tid` (identical in every CTA: computed from the same write-once sums)
   const bool own = tid < kp.total_rhs;
@@ -567,7 +952,7 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
 
   // ---- rhsMax = max |b cg2dNorm| (cg2d.py:221-225)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  run_pass<MIXED>(kp, P_MAX, 0, 0, sm);
+  run_pass_direct<MIXED>(kp, P_MAX, sm);
   ok = grid_barrier(kp, target, sm.misc);
   if (!ok) goto epilogue;
   if (own) {
@@ -577,14 +962,15 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
   }
   // ---- x = x0 rhsNorm, r = b - A x, s = 0, err^2, sumRHS (cg2d.py:226-236)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  run_pass<MIXED>(kp, P_INIT, 0, 0, sm);
+  run_pass_direct<MIXED>(kp, P_INIT, sm);
+  init_x_halo(kp, sm);
   ok = grid_barrier(kp, target, sm.misc);
   if (!ok) goto epilogue;
   if (own) rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  run_pass<MIXED>(kp, P_Z, 0, 0, sm);
-  ok = grid_barrier(kp, target, sm.misc);
+  ok = run_pass_tma<MIXED>(kp, P_Z, 0, 0, sm, phase);
+  ok = grid_barrier(kp, target, sm.misc) && ok;
   if (!ok) goto epilogue;
   if (own) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
 
@@ -607,8 +993,8 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
-    run_pass<MIXED>(kp, P_S, k, k, sm);
-    ok = grid_barrier(kp, target, sm.misc);
+    ok = run_pass_tma<MIXED>(kp, P_S, k, k, sm, phase);
+    ok = grid_barrier(kp, target, sm.misc) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
     if (a == A_ACTIVE) {
@@ -616,32 +1002,37 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
       alpha = __ddiv_rn(eta, sq);                           // cg2d.py:252-253
       has_alpha = 1;
     }
-    // ---- r, z, err^2, next eta
-    int ax = A_NONE;
-    if (a == A_ACTIVE)
-      ax = (kp.mixed && kp.replace_every > 0 && ((k + 1) % kp.replace_every) == 0 && rr > rep2) ? A_REPLACE
-                                                                                                : A_ACTIVE;
-    set_actions(kp, sm, ax, alpha, 0.0);
-    run_pass<MIXED>(kp, P_X, k, k + 1, sm);
-    ok = grid_barrier(kp, target, sm.misc);
-    if (!ok) goto epilogue;
-    if (ax == A_ACTIVE) {
-      rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
-      eta = __ldcg(hist_ptr(kp, tid, H_ETAX, k + 1));
-    } else if (ax == A_REPLACE) {
-      rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
-      ++nrep;
+    // ---- r, z, err^2 and the next eta; or, every replace_every iterations (MIXED), the true residual
+    int ax = A_NONE, ar = A_NONE;
+    if (a == A_ACTIVE) {
+      const bool rep = kp.mixed && kp.replace_every > 0 && ((k + 1) % kp.replace_every) == 0 && rr > rep2;
+      if (rep) ar = A_ACTIVE;
+      else ax = A_ACTIVE;
     }
-    if (kp.mixed) {
-      // z = M r and eta from a replaced residual
-      const int az = (ax == A_REPLACE) ? A_ACTIVE : A_NONE;
-      if (__syncthreads_or(az != A_NONE)) {
-        set_actions(kp, sm, az, 0.0, 0.0);
-        run_pass<MIXED>(kp, P_Z, k, k + 1, sm);
-        ok = grid_barrier(kp, target, sm.misc);
-        if (!ok) goto epilogue;
-        if (az == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
+    if (__syncthreads_or(ax != A_NONE)) {
+      set_actions(kp, sm, ax, alpha, 0.0);
+      ok = run_pass_tma<MIXED>(kp, P_X, k, k + 1, sm, phase);
+      ok = grid_barrier(kp, target, sm.misc) && ok;
+      if (!ok) goto epilogue;
+      if (ax == A_ACTIVE) {
+        rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
+        eta = __ldcg(hist_ptr(kp, tid, H_ETAX, k + 1));
       }
+    }
+    if (__syncthreads_or(ar != A_NONE)) {
+      set_actions(kp, sm, ar, alpha, 0.0);
+      ok = run_pass_tma<MIXED>(kp, P_R, k, k + 1, sm, phase);
+      ok = grid_barrier(kp, target, sm.misc) && ok;
+      if (!ok) goto epilogue;
+      if (ar == A_ACTIVE) {
+        rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
+        ++nrep;
+      }
+      set_actions(kp, sm, ar, 0.0, 0.0);
+      ok = run_pass_tma<MIXED>(kp, P_Z, k, k + 1, sm, phase);
+      ok = grid_barrier(kp, target, sm.misc) && ok;
+      if (!ok) goto epilogue;
+      if (ar == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
     }
   }
 
@@ -673,8 +1064,8 @@ epilogue:
           if (tp.map_comp[p] == 1) {
             const int sp = tp.map_src[p];
             const int spl = sp % plane;
-            const int sj = spl / tp.npx, si = spl - (spl / tp.npx) * tp.npx;
-            const bool sin = sj >= tp.OLy && sj < tp.OLy + tp.nj && si >= tp.OLx && si < tp.OLx + tp.ni;
+            const int sj = spl / tp.npx, si_ = spl - (spl / tp.npx) * tp.npx;
+            const bool sin = sj >= tp.OLy && sj < tp.OLy + tp.nj && si_ >= tp.OLx && si_ < tp.OLx + tp.ni;
             const double rn = sm.rnorm[g.rhs_base + in * g.nrhs + s];
             v = sin ? mul(__ldg(x0 + sp), rn) : __ldg(x0 + sp);
           }
@@ -703,18 +1094,21 @@ epilogue:
 }
 
 // ------------------------------------------------------------------------------------------------
-// MIXED: FP32 copies of the six coefficient arrays, [inst][6][pad_elems]
+// MIXED: FP32 copies of the six coefficient arrays, [inst][6][T][npy][ldc] (row pitch ldc)
 
 __global__ void pack32_kernel(GroupDev g) {
-  const long long pe = g.pad_elems;
-  const long long tot = pe * 6 * g.count;
+  const TopoDev& tp = g.tp;
+  const long long rows = (long long)tp.T * tp.npy;
+  const long long tot = rows * g.ldc * 6 * g.count;
   for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < tot;
        idx += (long long)gridDim.x * blockDim.x) {
-    const long long in = idx / (6 * pe);
-    const long long rem = idx - in * 6 * pe;
-    const int which = (int)(rem / pe);
-    const long long p = rem - (long long)which * pe;
-    g.c32[idx] = __double2float_rn(g.a64[which][in * pe + p]);
+    const long long row = idx / g.ldc;
+    const int col = (int)(idx - row * g.ldc);
+    const long long ia = row / rows;             // inst * 6 + which
+    const long long r = row - ia * rows;
+    const int which = (int)(ia % 6);
+    const long long in = ia / 6;
+    g.c32[idx] = col < tp.npx ? __double2float_rn(g.a64[which][in * g.pad_elems + r * tp.npx + col]) : 0.0f;
   }
 }
 
@@ -776,7 +1170,7 @@ __global__ void edge_products_kernel(TopoDev tp, int batch, double norm, const d
     const double* xi = x + in * pe;
     const bool jin = j >= 0 && j < tp.nj, iin = i >= 0 && i < tp.ni;
     double w = 0.0, s = 0.0, c = 0.0;
-    // interior lam / cg2dNorm at (t, jj, ii) (0 off the interior)
+    // interior lam / cg2dNorm at (t, jj, ii)
     auto cl = [&](int jj, int ii) -> double {
       return __ddiv_rn(li[((long long)t * tp.npy + jj + tp.OLy) * tp.npx + ii + tp.OLx], nrm);
     };
@@ -834,7 +1228,8 @@ cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t
 }
 
 cudaError_t launch_pack32(const GroupDev& g, cudaStream_t stream) {
-  pack32_kernel<<<grid_for(g.pad_elems * 6 * g.count), 256, 0, stream>>>(g);
+  const long long tot = (long long)g.tp.T * g.tp.npy * g.ldc * 6 * g.count;
+  pack32_kernel<<<grid_for(tot), 256, 0, stream>>>(g);
   return cudaGetLastError();
 }
 
