@@ -70,7 +70,7 @@ typedef struct {
   int test_missing_arrivals; /* testing only (default 0): the first grid-wide wait expects this many
                                 arrivals more than there are CTAs, so it runs out after timeout_s and
                                 every solve reports CG2D_BARRIER_TIMEOUT (exercises the bounded wait) */
-  int reserved;
+  int profile;         /* 1: record per-CTA phase times in the workspace (cg2d_workspace_profile) */
 } cg2d_params_t;
 
 /* Per-solve diagnostics: the diag dict of cg2d_fortran (cg2d.py:267-268) plus a status. */
@@ -176,6 +176,14 @@ cg2d_status_t cg2d_edge_products(const cg2d_topology_t* topo, int batch, double 
  * not alias a. */
 cg2d_status_t cg2d_exchange_scalar(const cg2d_topology_t* topo, int batch, const double* a, double* out,
                                    cg2d_stream_t stream);
+
+/* Phase times of the last solve that used this workspace with params->profile = 1 (synchronises the
+ * stream). out (host, >= 1 + 8 * cap values): out[0] = number of CTAs G, then for CTA c the
+ * nanoseconds its thread 0 spent in [grid-wide waits, bulk-copy waits, copy issue, compute, unit
+ * finish (partials and fixed-order sums), direct passes, other, total] at out[1 + 8c .. 8c + 8].
+ * Returns CG2D_BAD_ARG when the groups/params do not describe that workspace's layout. */
+cg2d_status_t cg2d_workspace_profile(const void* workspace, const cg2d_group_t* groups, int ngroups,
+                                     const cg2d_params_t* params, uint64_t* out, int cap, cg2d_stream_t stream);
 
 /* Human-readable name of a status code (static string). */
 const char* cg2d_status_string(cg2d_status_t s);

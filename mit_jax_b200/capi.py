@@ -30,14 +30,14 @@ STATUS_NAMES = {0: "ok", 1: "not_converged", 2: "nan", 3: "barrier_timeout", 4: 
 
 EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_params", "cg2d_workspace_size",
             "cg2d_solve_groups", "cg2d_solve_f64", "cg2d_workspace_status", "cg2d_apply_operator",
-            "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string")
+            "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string", "cg2d_workspace_profile")
 
 
 class Params(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("sum_order", ctypes.c_int), ("rows_per_block", ctypes.c_int),
                 ("replace_every", ctypes.c_int), ("replace_above", ctypes.c_double), ("grid_ctas", ctypes.c_int),
                 ("ctas_per_sm", ctypes.c_int), ("timeout_s", ctypes.c_double),
-                ("test_missing_arrivals", ctypes.c_int), ("reserved", ctypes.c_int)]
+                ("test_missing_arrivals", ctypes.c_int), ("profile", ctypes.c_int)]
 
 
 class Diag(ctypes.Structure):
@@ -94,6 +94,8 @@ def lib():
     L.cg2d_edge_products.restype = i
     L.cg2d_exchange_scalar.argtypes = [_P, i, _P, _P, _P]
     L.cg2d_exchange_scalar.restype = i
+    L.cg2d_workspace_profile.argtypes = [_P, ctypes.POINTER(Group), i, ctypes.POINTER(Params), _P, i, _P]
+    L.cg2d_workspace_profile.restype = i
     L.cg2d_status_string.argtypes = [i]
     L.cg2d_status_string.restype = ctypes.c_char_p
     _LIB = L

@@ -59,7 +59,7 @@ class Cg2dParams:
 
 
 def _params_struct(precision="f64", sum_order="rowblock", rows_per_block=8, replace_every=25, replace_above=100.0,
-                   timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, test_missing_arrivals=0):
+                   timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, test_missing_arrivals=0, profile=False):
     p = capi.default_params()
     p.precision = capi.PREC_MIXED if precision == "mixed" else capi.PREC_F64
     p.sum_order = capi.SUM_FORTRAN if sum_order == "fortran" else capi.SUM_ROWBLOCK
@@ -70,6 +70,7 @@ def _params_struct(precision="f64", sum_order="rowblock", rows_per_block=8, repl
     p.grid_ctas = grid_ctas
     p.ctas_per_sm = ctas_per_sm
     p.test_missing_arrivals = test_missing_arrivals
+    p.profile = 1 if profile else 0
     return p
 
 
@@ -194,15 +195,18 @@ class GroupSpec:
 
 def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8, replace_every=25,
                  replace_above=100.0, timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, check_status=True,
-                 test_missing_arrivals=0):
+                 test_missing_arrivals=0, profile=False):
     """Run every right-hand side of every group in one persistent launch (cg2d_solve_groups).
 
-    Returns per group a list (one entry per slot) of (x_out, x_fortran or None, diag ndarray of cg2d_diag_t)."""
+    Returns per group a list (one entry per slot) of (x_out, x_fortran or None, diag ndarray of cg2d_diag_t).
+    profile=True records per-CTA phase times; they are left in `solve_groups.last_profile` as an array
+    [ctas, 8] of nanoseconds (grid-wide waits, bulk-copy waits, copy issue, compute, unit finish, direct passes,
+    other, total)."""
     if not 1 <= len(groups) <= 4:
         raise ValueError("1 to 4 groups")
     dev = groups[0].b[0].device
     params = _params_struct(precision, sum_order, rows_per_block, replace_every, replace_above, timeout_s,
-                            grid_ctas, ctas_per_sm, test_missing_arrivals)
+                            grid_ctas, ctas_per_sm, test_missing_arrivals, profile)
     arr = (capi.Group * len(groups))()
     keep, outs = [], []
     for gi, G in enumerate(groups):
@@ -247,6 +251,11 @@ def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8
         for xo, xf, dg in slot_out:
             res.append((xo, xf, dg))
         result.append(res)
+    if profile:
+        buf = np.zeros(1 + 8 * 1184, np.uint64)
+        capi.check(L.cg2d_workspace_profile(base + off, arr, len(groups), ctypes.byref(params), buf.ctypes.data, 1184,
+                                            _stream(dev)), "cg2d_workspace_profile")
+        solve_groups.last_profile = buf[1:1 + 8 * int(buf[0])].reshape(-1, 8)
     if check_status:
         st = L.cg2d_workspace_status(base + off, _stream(dev))
         if st != capi.CG2D_OK:

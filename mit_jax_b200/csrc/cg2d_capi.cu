@@ -14,7 +14,7 @@ struct cg2d_topology {
   int sNx, sNy, OLx, OLy, nTiles;
   int njp, nip;      // halo slice pitches (multiples of 4)
   int* d_nbr;        // [4][...] W, E (T*sNy each), S, N (T*sNx each)
-  int* d_tg;         // [T][2 sNy + 2 sNx][2] halo slots each tile-edge point is pushed to
+  int* d_tg;         // push targets: W, E [T][njp][2], S, N [T][nip][2] (halo slots, -1 = none)
   int* d_src;        // full padded map
   int8_t* d_comp;
   int device;
@@ -46,7 +46,7 @@ TopoDev topo_dev(const cg2d_topology* tp) {
 }
 
 struct WsLayout {
-  size_t gs, rmax, cnt, halo_begin, zero_end, hist, part, total;
+  size_t gs, rmax, cnt, prof, halo_begin, zero_end, hist, part, total;
   size_t vec[kMaxGroups], c32[kMaxGroups], halo[kMaxGroups];
   long long vec_stride[kMaxGroups], halo_stride[kMaxGroups];
   long long vec_off[kMaxGroups][V_NVEC], halo_off[kMaxGroups][V_NVEC];
@@ -81,17 +81,19 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
       const cg2d_topology* tp = gr[g].topo;
       const int npx = tp->sNx + 2 * tp->OLx;
       for (int pt : {P_S, P_X, P_Z}) {
-        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
+        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, tp->sNx, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
         if (S.total > hot) hot = S.total;
       }
       if (mixed) {
-        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
+        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, tp->sNx, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
         if (S.total > rep) rep = S.total;
       }
     }
     // the direct-load passes stage (8 + 2) rows of (max_ni + 2) doubles per solve slot in the same area
     const unsigned direct = (unsigned)(2 * (kWarps + 2) * (L->max_ni + 2) * sizeof(double));
+    const unsigned red = (unsigned)(4 * L->part_units * sizeof(double));   // partials gathered by a reducer
     unsigned sb = hot;
+    if (2 * sb < red) sb = (red + 1) / 2;
     if (2 * sb < rep) sb = (rep + 1) / 2;
     if (2 * sb < direct) sb = (direct + 1) / 2;
     sb = al128(sb);
@@ -147,6 +149,8 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
   L->gs = o; o += al(2 * sizeof(unsigned));
   L->rmax = o; o += al(sizeof(unsigned long long) * L->total_rhs);
   L->cnt = o; o += al(sizeof(unsigned) * L->total_ops);
+  L->prof = o;
+  if (p->profile) o += al(sizeof(unsigned long long) * (1 + (size_t)kMaxCtas * 8));
   L->halo_begin = o;
   for (int g = 0; g < ng; ++g) {
     const cg2d_topology* tp = gr[g].topo;
@@ -194,7 +198,7 @@ void cg2d_default_params(cg2d_params_t* p) {
   p->ctas_per_sm = 0;
   p->timeout_s = 10.0;
   p->test_missing_arrivals = 0;
-  p->reserved = 0;
+  p->profile = 0;
 }
 
 const char* cg2d_status_string(cg2d_status_t s) {
@@ -253,17 +257,18 @@ cg2d_status_t cg2d_topology_create(int sNx, int sNy, int OLx, int OLy, int nTile
   // push targets: every halo slot (side, tile, position) with a source point is filled by that point's
   // owner; a source must lie on its own tile's edge, with at most two slots per edge point
   const int njp = round_up(sNy, 4), nip = round_up(sNx, 4);
-  const int perim = 2 * sNy + 2 * sNx;
-  std::vector<int> tg((size_t)nTiles * perim * 2, -1);
+  // target lists by side: a point with i == 0 uses the W list (row j), i == sNx-1 the E list, otherwise
+  // j == 0 the S list (column i) and j == sNy-1 the N list
+  std::vector<int> tg((size_t)nTiles * (2 * njp + 2 * nip) * 2, -1);
   auto add_target = [&](int c, int slot) -> bool {
     const int t = c / (sNy * sNx), rem = c - t * sNy * sNx, j = rem / sNx, i = rem - j * sNx;
-    int e;
-    if (i == 0) e = j;
-    else if (i == sNx - 1) e = sNy + j;
-    else if (j == 0) e = 2 * sNy + i;
-    else if (j == sNy - 1) e = 2 * sNy + sNx + i;
+    size_t e;
+    if (i == 0) e = (size_t)t * njp + j;
+    else if (i == sNx - 1) e = (size_t)(nTiles + t) * njp + j;
+    else if (j == 0) e = (size_t)2 * nTiles * njp + (size_t)t * nip + i;
+    else if (j == sNy - 1) e = (size_t)2 * nTiles * njp + (size_t)(nTiles + t) * nip + i;
     else return false;
-    int* q = &tg[((size_t)t * perim + e) * 2];
+    int* q = &tg[e * 2];
     if (q[0] < 0) q[0] = slot;
     else if (q[1] < 0) q[1] = slot;
     else return false;
@@ -367,6 +372,7 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   kp.gs = reinterpret_cast<unsigned*>(ws + L.gs);
   kp.timeout_ns = (unsigned long long)(params->timeout_s * 1e9);
   kp.test_missing = params->test_missing_arrivals;
+  kp.prof = params->profile ? reinterpret_cast<unsigned long long*>(ws + L.prof) : nullptr;
   int unit_base = 0, op_base = 0, rhs_base = 0;
   for (int g = 0; g < ngroups; ++g) {
     const cg2d_group_t& G = groups[g];
@@ -424,6 +430,7 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   long long grid = (long long)bps * nsm;
   if (params->grid_ctas > 0 && params->grid_ctas < grid) grid = params->grid_ctas;
   if (grid > kp.total_units) grid = kp.total_units;
+  if (grid > kMaxCtas) grid = kMaxCtas;
   if (grid < 1) grid = 1;
   if (launch_solver(kp, (int)grid, smem, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return CG2D_OK;
@@ -458,6 +465,18 @@ cg2d_status_t cg2d_workspace_status(const void* workspace, cg2d_stream_t stream)
   unsigned w[2] = {0, 0};
   if (cudaMemcpy(w, workspace, sizeof(w), cudaMemcpyDeviceToHost) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return w[1] ? (cg2d_status_t)w[1] : CG2D_OK;
+}
+
+cg2d_status_t cg2d_workspace_profile(const void* workspace, const cg2d_group_t* groups, int ngroups,
+                                     const cg2d_params_t* params, uint64_t* out, int cap, cg2d_stream_t stream) {
+  if (!workspace || !out || cap < 1 || !params || !params->profile) return CG2D_BAD_ARG;
+  WsLayout L;
+  if (check_params(params) != CG2D_OK || compute_layout(groups, ngroups, params, &L) != CG2D_OK) return CG2D_BAD_ARG;
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  const size_t n = 1 + (size_t)(cap < kMaxCtas ? cap : kMaxCtas) * 8;
+  if (cudaMemcpy(out, static_cast<const char*>(workspace) + L.prof, n * sizeof(uint64_t), cudaMemcpyDeviceToHost) !=
+      cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
 }
 
 cg2d_status_t cg2d_apply_operator(const cg2d_topology_t* topo, int batch, double cg2dNorm, const double* aW2d,

@@ -29,7 +29,7 @@ enum VecId : int { V_X = 0, V_R0 = 1, V_R1 = 2, V_S0 = 3, V_S1 = 4, V_Z = 5, V_Q
 // tables of one tile layout (device)
 struct TopoDev {
   const int* nbr;           // [4][T*len]: W (len nj), E (nj), S (ni), N (ni); compact source index or -1
-  const int* tg;            // [T][2nj+2ni][2]: halo slots a tile-edge point's value is pushed to (-1 = none)
+  const int* tg;            // push targets (pairs of halo slots, -1 = none): W, E [T][njp][2], S, N [T][nip][2]
   const int* map_src;       // full padded "T" map (src), for x_fortran halos and cg2d_exchange_scalar
   const int8_t* map_comp;
   int ni, nj, OLx, OLy, npx, npy, T;
@@ -80,7 +80,12 @@ struct KParams {
   unsigned* gs;             // [0] grid barrier arrivals, [1] error word
   unsigned long long timeout_ns;
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
+  unsigned long long* prof; // nullable: [1 + grid * 8] phase times (ns) per CTA
 };
+
+constexpr int kMaxCtas = 148 * 8;
+enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FIN = 4, PR_DIRECT = 5, PR_OTHER = 6,
+                       PR_TOTAL = 7 };
 
 // Shared-memory image of one chunk for a pipelined pass (offsets in bytes from the stage buffer).
 struct StageLay {
@@ -91,14 +96,15 @@ struct StageLay {
   int vpitch[2], vsize[2];
   unsigned hw[2][2], he[2][2];  // west / east cross-tile neighbours of the chunk's rows
   unsigned xo[2];               // P_S: own rows of x (double)
+  unsigned tw, te, ts, tn;      // push targets of the chunk's edge points (int2 per point)
   unsigned total;
 };
 
 __host__ __device__ inline unsigned al128(unsigned x) { return (x + 127u) & ~127u; }
 __host__ __device__ inline unsigned al16(unsigned x) { return (x + 15u) & ~15u; }
 
-__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int npx, int ldv, int ldx,
-                                                 int ldc) {
+__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int ni, int npx, int ldv,
+                                                 int ldx, int ldc) {
   StageLay L;
   unsigned o = 0;
   const bool coef64 = (pt == P_R) || !mixed;
@@ -127,6 +133,10 @@ __host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int 
     L.xo[s] = 0;
     if (pt == P_S && s < nrhs) { L.xo[s] = o; o += al128((unsigned)(ch * ldx * 8)); }
   }
+  L.tw = o; o += al128(al16((unsigned)(ch * 8)));
+  L.te = o; o += al128(al16((unsigned)(ch * 8)));
+  L.ts = o; o += al128(al16((unsigned)(ni * 8)));
+  L.tn = o; o += al128(al16((unsigned)(ni * 8)));
   L.total = al128(o);
   return L;
 }

@@ -83,11 +83,25 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned* p) {
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+// where a time limit ran out: gs[2] = 1 grid-wide wait, 2 bulk-copy wait, 3 unit-count wait; gs[3] = pass << 16 | CTA
+__device__ __forceinline__ void note_timeout(unsigned* gs, unsigned where, unsigned pass) {
+  if (atomicCAS(&gs[1], 0u, (unsigned)CG2D_BARRIER_TIMEOUT) == 0u) {
+    gs[2] = where;
+    gs[3] = (pass << 16) | (blockIdx.x & 0xffffu);
+  }
+}
 __device__ __forceinline__ unsigned long long globaltimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+
+// phase timers (thread 0, profiling only)
+#define PROF_T0(kp) (((kp).prof && threadIdx.x == 0) ? globaltimer() : 0ull)
+#define PROF_ADD(kp, sm, ph, t0)                                               \
+  do {                                                                         \
+    if ((kp).prof && threadIdx.x == 0) (sm).pacc[ph] += globaltimer() - (t0); \
+  } while (0)
 
 // ---- bulk asynchronous copies and mbarriers
 
@@ -145,6 +159,9 @@ struct Smem {
   double* tsum;      // [kMaxTiles]
   int* misc;         // [4]: barrier ok flag, last-arriver flag
   unsigned long long* bar;  // [2] stage mbarriers
+  unsigned long long* pacc; // [8] phase times of this CTA (thread 0; profiling)
+  unsigned* opn;            // [kMaxOps] passes with sums each operator has completed (its counter target)
+  double* uacc;             // [4] thread 0: the current unit's partial sums (slot, kind)
   double* prod;      // FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]
   unsigned char* stage;     // 2 x stage_bytes (128-aligned); also the direct-load staging area
 };
@@ -161,6 +178,9 @@ size_t fixed_smem_bytes(int max_ni, int serial) {
   s += a16(sizeof(double) * kMaxTiles);
   s += a16(sizeof(int) * 4);
   s += a16(sizeof(unsigned long long) * 2);
+  s += a16(sizeof(unsigned long long) * 8);
+  s += a16(sizeof(unsigned) * kMaxOps);
+  s += a16(sizeof(double) * 4);
   if (serial) s += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni);
   return (s + 127) & ~size_t(127);
 }
@@ -179,6 +199,9 @@ __device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
   m.tsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxTiles);
   m.misc = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * 4);
   m.bar = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 2);
+  m.pacc = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 8);
+  m.opn = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
+  m.uacc = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 4);
   m.prod = nullptr;
   if (serial) { m.prod = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni); }
   o = (o + 127) & ~size_t(127);
@@ -190,7 +213,9 @@ __device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
 // grid-wide wait with a time limit: every CTA arrives once; the wait ends when all have arrived,
 // when another CTA has flagged an error, or after timeout_ns (then this CTA flags the error).
 
-__device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag) {
+struct Smem;
+__device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag, unsigned long long* pacc) {
+  const unsigned long long tb = PROF_T0(kp);
   fence_proxy_async();        // this thread's stores before the next pass's bulk copies
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -204,7 +229,7 @@ __device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag) {
       if ((int)(v - target) >= 0) break;
       if (ld_relaxed(&kp.gs[1]) != 0u) { ok = 0; break; }
       if ((spins & 63u) == 63u && globaltimer() - t0 > kp.timeout_ns) {
-        atomicCAS(&kp.gs[1], 0u, (unsigned)CG2D_BARRIER_TIMEOUT);
+        note_timeout(kp.gs, 1u, 0u);
         ok = 0;
         break;
       }
@@ -212,6 +237,7 @@ __device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag) {
     __threadfence();
     fence_proxy_async();
     *flag = ok;
+    if (kp.prof) pacc[PR_BAR] += globaltimer() - tb;
   }
   __syncthreads();
   const int ok = *flag;
@@ -237,16 +263,32 @@ __device__ __forceinline__ T* halo_ptr(const GroupDev& g, int inst, int slot, in
 // store the value of point (t, j, i) into the halo slices of the tiles that read it across an edge
 template <class T>
 __device__ __forceinline__ void push(const TopoDev& tp, T* halo, int t, int j, int i, T v) {
-  int e;
-  if (i == 0) e = j;
-  else if (i == tp.ni - 1) e = tp.nj + j;
-  else if (j == 0) e = 2 * tp.nj + i;
-  else if (j == tp.nj - 1) e = 2 * tp.nj + tp.ni + i;
+  size_t e;
+  if (i == 0) e = (size_t)t * tp.njp + j;
+  else if (i == tp.ni - 1) e = (size_t)(tp.T + t) * tp.njp + j;
+  else if (j == 0) e = (size_t)2 * tp.T * tp.njp + (size_t)t * tp.nip + i;
+  else if (j == tp.nj - 1) e = (size_t)2 * tp.T * tp.njp + (size_t)(tp.T + t) * tp.nip + i;
   else return;
-  const int* tg = tp.tg + ((size_t)t * (2 * tp.nj + 2 * tp.ni) + e) * 2;
-  const int s0 = __ldg(tg), s1 = __ldg(tg + 1);
+  const int s0 = __ldg(tp.tg + 2 * e), s1 = __ldg(tp.tg + 2 * e + 1);
   if (s0 >= 0) stcg(halo + s0, v);
   if (s1 >= 0) stcg(halo + s1, v);
+}
+
+// the same with the chunk's target lists staged in shared memory (row w of the chunk = tile row j)
+struct PushTab {
+  const int2 *tw, *te, *ts, *tn;
+  int ni, nj;
+};
+template <class T>
+__device__ __forceinline__ void push_s(const PushTab& pt, T* halo, int j, int w, int i, T v) {
+  int2 e;
+  if (i == 0) e = pt.tw[w];
+  else if (i == pt.ni - 1) e = pt.te[w];
+  else if (j == 0) e = pt.ts[i];
+  else if (j == pt.nj - 1) e = pt.tn[i];
+  else return;
+  if (e.x >= 0) stcg(halo + e.x, v);
+  if (e.y >= 0) stcg(halo + e.y, v);
 }
 
 // compact index -> padded index of the same point
@@ -282,47 +324,57 @@ __device__ __forceinline__ int hist_kind(int pt, int kind) {
   }
 }
 
-// which solve slots of an instance take part, and their scalars
-struct SlotInfo {
-  int rid[2], act[2], has_alpha[2];
-  double c1[2], c2[2], rnorm[2], norm[2];
+// the solve slots of an instance and their scalars, read from shared memory by solve index
+struct Slots {
+  const Smem* sm;
+  int rid0, nrhs;
+  __device__ __forceinline__ int rid(int s) const { return rid0 + s; }
+  __device__ __forceinline__ int act(int s) const { return s < nrhs ? sm->act[rid0 + s] : (int)A_NONE; }
+  __device__ __forceinline__ double c1(int s) const { return sm->c1[rid0 + s]; }
+  __device__ __forceinline__ double c2(int s) const { return sm->c2[rid0 + s]; }
+  __device__ __forceinline__ double rnorm(int s) const { return sm->rnorm[rid0 + s]; }
+  __device__ __forceinline__ double norm(int s) const { return sm->norm[rid0 + s]; }
+  __device__ __forceinline__ int has_alpha(int s) const { return sm->has_alpha[rid0 + s]; }
 };
-__device__ __forceinline__ void slot_info(const GroupDev& g, int inst, const Smem& sm, SlotInfo& si) {
-#pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const bool on = s < g.nrhs;
-    const int r = g.rhs_base + inst * g.nrhs + s;
-    si.rid[s] = r;
-    si.act[s] = on ? sm.act[r] : A_NONE;
-    si.c1[s] = on ? sm.c1[r] : 0.0;
-    si.c2[s] = on ? sm.c2[r] : 0.0;
-    si.rnorm[s] = on ? sm.rnorm[r] : 1.0;
-    si.norm[s] = on ? sm.norm[r] : 1.0;
-    si.has_alpha[s] = on ? sm.has_alpha[r] : 0;
-  }
+__device__ __forceinline__ Slots slots_of(const GroupDev& g, int inst, const Smem& sm) {
+  Slots q;
+  q.sm = &sm;
+  q.rid0 = g.rhs_base + inst * g.nrhs;
+  q.nrhs = g.nrhs;
+  return q;
 }
 
 // ------------------------------------------------------------------------------------------------
 // row sums of one chunk into the unit partials, and the unit partials into the instance sums
 
 // warp w holds per-lane partials lp of row w: xor butterfly (every lane ends with the same value)
-__device__ __forceinline__ void row_sums(const GroupDev& g, const double (&lp)[2][2], const Smem& sm) {
+struct Lanes {
+  double v[4];   // (slot 0, kind 0), (0, 1), (1, 0), (1, 1): always indexed with constants
+};
+__device__ __forceinline__ double butterfly(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, const Smem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int s = 0; s < g.nrhs; ++s)
-    for (int q = 0; q < 2; ++q) {
-      double v = lp[s][q];
-      for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (lane == 0) sm.rowsum[(s * 2 + q) * kWarps + warp] = v;
-    }
+  const double r0 = butterfly(lp.v[0]), r1 = butterfly(lp.v[1]);
+  double r2 = 0.0, r3 = 0.0;
+  if (g.nrhs > 1) { r2 = butterfly(lp.v[2]); r3 = butterfly(lp.v[3]); }
+  if (lane == 0) {
+    sm.rowsum[0 * kWarps + warp] = r0;
+    sm.rowsum[1 * kWarps + warp] = r1;
+    sm.rowsum[2 * kWarps + warp] = r2;
+    sm.rowsum[3 * kWarps + warp] = r3;
+  }
 }
 
 // thread 0: add the chunk's rows (ROWBLOCK: row sums in order; FORTRAN: every product in j, i order)
-__device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupDev& g, int pt, const SlotInfo& si,
-                                                 int nr, double (&acc)[2][2], const Smem& sm) {
-  for (int s = 0; s < g.nrhs; ++s) {
-    const int ns = nsums(pt, si.act[s]);
+__device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupDev& g, int ns0, int ns1, int nr,
+                                                 const Smem& sm) {
+  for (int s = 0; s < 2; ++s) {
+    const int ns = s == 0 ? ns0 : ns1;
     for (int q = 0; q < ns; ++q) {
-      double a = acc[s][q];
+      double a = sm.uacc[s * 2 + q];
       if (kp.serial) {
         const double* pr = sm.prod + ((s * 2 + q) * kWarps) * kp.max_ni;
         for (int w = 0; w < nr; ++w)
@@ -330,52 +382,109 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
       } else {
         for (int w = 0; w < nr; ++w) a = add(a, sm.rowsum[(s * 2 + q) * kWarps + w]);
       }
-      acc[s][q] = a;
+      sm.uacc[s * 2 + q] = a;
     }
   }
 }
 
-// thread 0 writes the unit's partials; the CTA that completes an instance's last unit forms the
-// instance's sums in fixed order: blocks of a tile in order, then tiles in order from 0
-// (GLOBAL_SUM_TILE, global_sum.py:20-26)
-__device__ void finish_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int pt, int hidx,
-                            const SlotInfo& si, const double (&acc)[2][2], const Smem& sm) {
+// thread 0 writes the unit's partials and counts the unit done (release: the partials are visible to whoever
+// observes the count); no wait
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __noinline__ void finish_unit(const KParams& kp, int op, int lu, int rid0, int rid1, int ns0, int ns1,
+                                        double a00, double a01, double a10, double a11) {
+  if (ns0 + ns1 == 0) return;
+  if (ns0 > 0) stcg(kp.part + ((size_t)rid0 * 2 + 0) * kp.part_units + lu, a00);
+  if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, a01);
+  if (ns1 > 0) stcg(kp.part + ((size_t)rid1 * 2 + 0) * kp.part_units + lu, a10);
+  if (ns1 > 1) stcg(kp.part + ((size_t)rid1 * 2 + 1) * kp.part_units + lu, a11);
+  red_release_add(&kp.cnt[op], 1u);
+}
+__device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int ns0, int ns1,
+                                            const Smem& sm) {
+  if (threadIdx.x != 0) return;
+  const int rid0 = g.rhs_base + inst * g.nrhs;
+  finish_unit(kp, g.op_base + inst, lu, rid0, rid0 + 1, ns0, ns1, sm.uacc[0], sm.uacc[1], sm.uacc[2], sm.uacc[3]);
+}
+
+// End of a pass: the CTA that owns an instance's last unit waits until all of the instance's units are counted,
+// gathers their partials and forms the instance's sums in fixed order -- blocks of a tile in order, then tiles in
+// order from 0 (GLOBAL_SUM_TILE, global_sum.py:20-26). Then every CTA advances the operators' counter targets.
+__device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  int any = 0;
-  for (int s = 0; s < g.nrhs; ++s) any |= nsums(pt, si.act[s]);
-  if (!any) return;
-  if (tid == 0) {
-    for (int s = 0; s < g.nrhs; ++s) {
-      const int ns = nsums(pt, si.act[s]);
-      for (int q = 0; q < ns; ++q) stcg(kp.part + ((size_t)si.rid[s] * 2 + q) * kp.part_units + lu, acc[s][q]);
+  double* buf = reinterpret_cast<double*>(sm.stage);   // free at the end of a pass
+  bool ok = true;
+  for (int gi = 0; gi < kp.ngroups && ok; ++gi) {
+    const GroupDev& g = kp.g[gi];
+    for (int inst = 0; inst < g.count; ++inst) {
+      const int op = g.op_base + inst;
+      if (!sm.opp[op]) continue;
+      const int ulast = g.unit_base + inst * g.units + g.units - 1;
+      if (ulast % (int)gridDim.x != (int)blockIdx.x) continue;
+      const Slots si = slots_of(g, inst, sm);
+      // sums l = 0 .. nl-1: slot 0's ns0 kinds, then slot 1's
+      const int ns0 = nsums(pt, si.act(0)), ns1 = nsums(pt, si.act(1));
+      const int nl = ns0 + ns1;
+      if (!nl) continue;
+      if (tid == 0) {
+        const unsigned target = (sm.opn[op] + 1u) * (unsigned)g.units;
+        const unsigned long long t0 = globaltimer();
+        int good = 1;
+        for (unsigned spins = 0;; ++spins) {
+          if ((int)(ld_acquire(&kp.cnt[op]) - target) >= 0) break;
+          if ((spins & 63u) == 63u && (ld_relaxed(&kp.gs[1]) != 0u || globaltimer() - t0 > kp.timeout_ns)) {
+            note_timeout(kp.gs, 3u, (unsigned)pt);
+            good = 0;
+            break;
+          }
+        }
+        __threadfence();
+        sm.misc[2] = good;
+      }
+      __syncthreads();
+      if (!sm.misc[2]) { ok = false; break; }
+      const int U = g.units;
+      for (int idx = tid; idx < nl * U; idx += kThreads) {
+        const int l = idx / U, u = idx - (idx / U) * U;
+        const int sl = l < ns0 ? 0 : 1, ql = l < ns0 ? l : l - ns0;
+        buf[idx] = ldcg(kp.part + ((size_t)si.rid(sl) * 2 + ql) * kp.part_units + u);
+      }
+      __syncthreads();
+      if (warp == 0) {
+        for (int l = 0; l < nl; ++l) {
+          for (int tt = lane; tt < g.tp.T; tt += 32) {
+            double a = 0.0;
+            for (int b = 0; b < g.nblk; ++b) a = add(a, buf[l * U + tt * g.nblk + b]);
+            sm.tsum[tt] = a;
+          }
+          __syncwarp();
+          if (lane == 0) {
+            double a = 0.0;
+            for (int tt = 0; tt < g.tp.T; ++tt) a = add(a, sm.tsum[tt]);
+            const int sl = l < ns0 ? 0 : 1, ql = l < ns0 ? l : l - ns0;
+            stcg(hist_ptr(kp, si.rid(sl), hist_kind(pt, ql), hidx), a);
+          }
+          __syncwarp();
+        }
+      }
+      __syncthreads();
     }
-    __threadfence();
-    const unsigned old = atomicAdd(&kp.cnt[g.op_base + inst], 1u);
-    sm.misc[1] = ((old + 1u) % (unsigned)g.units) == 0u;
+  }
+  // every CTA: operators that produced sums in this pass expect one more round of unit counts
+  __syncthreads();
+  for (int op = tid; op < kp.total_ops; op += kThreads) {
+    if (!sm.opp[op]) continue;
+    int gi = 0;
+    while (gi + 1 < kp.ngroups && op >= kp.g[gi + 1].op_base) ++gi;
+    const GroupDev& g = kp.g[gi];
+    const int inst = op - g.op_base;
+    int any = 0;
+    for (int s = 0; s < g.nrhs; ++s) any |= nsums(pt, sm.act[g.rhs_base + inst * g.nrhs + s]);
+    if (any) sm.opn[op] += 1u;
   }
   __syncthreads();
-  if (sm.misc[1] && warp == 0) {
-    __threadfence();
-    const int T = g.tp.T;
-    for (int s = 0; s < g.nrhs; ++s) {
-      const int ns = nsums(pt, si.act[s]);
-      for (int q = 0; q < ns; ++q) {
-        const double* P = kp.part + ((size_t)si.rid[s] * 2 + q) * kp.part_units;
-        for (int tt = lane; tt < T; tt += 32) {
-          double a = 0.0;
-          for (int b = 0; b < g.nblk; ++b) a = add(a, ldcg(P + tt * g.nblk + b));
-          sm.tsum[tt] = a;
-        }
-        __syncwarp();
-        if (lane == 0) {
-          double a = 0.0;
-          for (int tt = 0; tt < T; ++tt) a = add(a, sm.tsum[tt]);
-          stcg(hist_ptr(kp, si.rid[s], hist_kind(pt, q), hidx), a);
-        }
-        __syncwarp();
-      }
-    }
-  }
+  return ok;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -395,14 +504,15 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
   const int W = ni + 2;
   const int SW = (kWarps + 2) * (kp.max_ni + 2);
   double* stage = reinterpret_cast<double*>(sm.stage);
-  SlotInfo si;
-  slot_info(g, inst, sm, si);
+  const Slots si = slots_of(g, inst, sm);
+  const int ns0 = nsums(pt, si.act(0));
+  const int ns1 = g.nrhs > 1 ? nsums(pt, si.act(1)) : 0;
   const double* aW = g.a64[0] + inst * pe;
   const double* aS = g.a64[1] + inst * pe;
   const double* aC = g.a64[2] + inst * pe;
 
-  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-  unsigned long long vmax[2] = {0ull, 0ull};
+  if (tid == 0) sm.uacc[0] = sm.uacc[1] = sm.uacc[2] = sm.uacc[3] = 0.0;
+  unsigned long long vmax0 = 0ull, vmax1 = 0ull;
 
   for (int jc = j0; jc < j1; jc += kWarps) {
     const int nr = min(kWarps, j1 - jc);
@@ -427,34 +537,35 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
           hp = ((long long)t * tp.npy + (j + tp.OLy)) * npx + (i + tp.OLx);
         }
         for (int s = 0; s < g.nrhs; ++s) {
-          if (si.act[s] != A_ACTIVE) continue;
+          if (si.act(s) != A_ACTIVE) continue;
           const double* x0 = g.x0[s] + inst * pe;
           stage[s * SW + rr * W + cc] =
-              (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), si.rnorm[s]) : __ldg(x0 + hp);
+              (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), si.rnorm(s)) : __ldg(x0 + hp);
         }
       }
       __syncthreads();
     }
-    double lp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
     if (warp < nr) {
       const int j = jc + warp;
       const long long prow = ((long long)t * tp.npy + (j + tp.OLy)) * npx + tp.OLx;
       for (int i = lane; i < ni; i += 32) {
         const long long po = prow + i;
         for (int s = 0; s < g.nrhs; ++s) {
-          if (si.act[s] != A_ACTIVE) continue;
+          if (si.act(s) != A_ACTIVE) continue;
           double p0 = 0.0, p1 = 0.0;
           if (pt == P_MAX) {
             const double bv = __ldg(g.b[s] + inst * pe + po);
             const unsigned long long m =
-                (unsigned long long)__double_as_longlong(fabs(mul(bv, si.norm[s])));   // cg2d.py:222-223
-            vmax[s] = m > vmax[s] ? m : vmax[s];
+                (unsigned long long)__double_as_longlong(fabs(mul(bv, si.norm(s))));   // cg2d.py:222-223
+            if (s == 0) vmax0 = m > vmax0 ? m : vmax0;
+            else vmax1 = m > vmax1 ? m : vmax1;
           } else {
             const double* st = stage + s * SW;
             const int sc = (warp + 1) * W + (i + 1);
             const double vc = st[sc], vw = st[sc - 1], ve = st[sc + 1], vs = st[sc - W], vn = st[sc + W];
             stcg(vec_ptr<double>(g, inst, s, V_X) + (t * nj + j) * g.ldx + i, vc);
-            const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), si.norm[s]), si.rnorm[s]);   // cg2d.py:221,226
+            const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), si.norm(s)), si.rnorm(s));   // cg2d.py:221,226
             const double ax = op_A<double>(__ldg(aW + po), __ldg(aW + po + 1), __ldg(aS + po), __ldg(aS + po + npx),
                                            __ldg(aC + po), vw, ve, vs, vn, vc);
             const V r0 = (V)sub(bn, ax);                                                   // cg2d.py:232
@@ -468,20 +579,21 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
             double* pr = sm.prod + ((s * 2 + 0) * kWarps + warp) * kp.max_ni;
             pr[i] = p0;
             pr[kWarps * kp.max_ni + i] = p1;
+          } else if (s == 0) {
+            lp.v[0] = add(lp.v[0], p0);
+            lp.v[1] = add(lp.v[1], p1);
           } else {
-            lp[s][0] = add(lp[s][0], p0);
-            lp[s][1] = add(lp[s][1], p1);
+            lp.v[2] = add(lp.v[2], p0);
+            lp.v[3] = add(lp.v[3], p1);
           }
         }
       }
       if (pt == P_MAX) {
-        for (int s = 0; s < g.nrhs; ++s) {
-          unsigned long long m = vmax[s];
-          for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
-            m = y > m ? y : m;
-          }
-          vmax[s] = m;
+        for (int o = 16; o > 0; o >>= 1) {
+          const unsigned long long y0 = __shfl_xor_sync(0xffffffffu, vmax0, o);
+          const unsigned long long y1 = __shfl_xor_sync(0xffffffffu, vmax1, o);
+          vmax0 = y0 > vmax0 ? y0 : vmax0;
+          vmax1 = y1 > vmax1 ? y1 : vmax1;
         }
       } else if (!kp.serial) {
         row_sums(g, lp, sm);
@@ -490,19 +602,21 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
     if (pt == P_MAX) {
       if (warp < nr && lane == 0)
         for (int s = 0; s < g.nrhs; ++s)
-          if (si.act[s] == A_ACTIVE) atomicMax(&kp.rmax[si.rid[s]], vmax[s]);
+          if (si.act(s) == A_ACTIVE) atomicMax(&kp.rmax[si.rid(s)], s == 0 ? vmax0 : vmax1);
       __syncthreads();
       continue;
     }
     __syncthreads();
-    if (tid == 0) accumulate_chunk(kp, g, pt, si, nr, acc, sm);
+    if (tid == 0) accumulate_chunk(kp, g, ns0, ns1, nr, sm);
   }
   if (pt == P_MAX) return;
-  finish_unit(kp, g, inst, lu, pt, 0, si, acc, sm);
+  finish_unit(kp, g, inst, lu, ns0, ns1, sm);
+  __syncthreads();   // the unit accumulators are reused by the next unit
 }
 
 template <bool MIXED>
-__device__ void run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
+__device__ bool run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
+  const unsigned long long t0 = PROF_T0(kp);
   for (int u = blockIdx.x; u < kp.total_units; u += gridDim.x) {
     int gi = 0;
     while (gi + 1 < kp.ngroups && u >= kp.g[gi + 1].unit_base) ++gi;
@@ -512,6 +626,9 @@ __device__ void run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
     if (!sm.opp[g.op_base + inst]) continue;
     process_unit_direct<MIXED>(kp, g, inst, rel - inst * g.units, pt, sm);
   }
+  const bool ok = reduce_pass(kp, pt, 0, sm);
+  PROF_ADD(kp, sm, PR_DIRECT, t0);
+  return ok;
 }
 
 // x halo slices at the start: the exchanged normalised first guess; unwritten points keep cg2d_x
@@ -603,7 +720,7 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
                             unsigned char* sb, unsigned long long* bar) {
   const GroupDev& g = kp.g[c.gi];
   const TopoDev& tp = g.tp;
-  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.npx, g.ldv, g.ldx, g.ldc);
+  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx, g.ldv, g.ldx, g.ldc);
   int act[2], hasal[2];
   bool any = false;
   for (int s = 0; s < 2; ++s) {
@@ -634,6 +751,15 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
                           tp.OLy) * g.ldc;
         cp(sb + L.coef + a * L.coef_stride, base, (unsigned)((c.nr + 1) * L.cpitch * L.csize));
       }
+      // push targets of the chunk's edge points
+      const unsigned tb = al16((unsigned)(c.nr * 8));
+      cp(sb + L.tw, tp.tg + 2 * ((long long)c.t * tp.njp + c.jc), tb);
+      cp(sb + L.te, tp.tg + 2 * ((long long)(tp.T + c.t) * tp.njp + c.jc), tb);
+      if (c.jc == 0)
+        cp(sb + L.ts, tp.tg + 2 * ((long long)2 * tp.T * tp.njp + (long long)c.t * tp.nip), al16((unsigned)(tp.ni * 8)));
+      if (c.jc + c.nr == tp.nj)
+        cp(sb + L.tn, tp.tg + 2 * ((long long)2 * tp.T * tp.njp + (long long)(tp.T + c.t) * tp.nip),
+           al16((unsigned)(tp.ni * 8)));
     }
     for (int s = 0; s < g.nrhs; ++s) {
       if (act[s] != A_ACTIVE) continue;
@@ -658,43 +784,51 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
         cp(sb + L.xo[s], xb + (long long)(c.t * tp.nj + c.jc) * g.ldx * 8, (unsigned)(c.nr * g.ldx * 8));
       }
     }
-    if (!go) {
-      fence_proxy_async();
-      mbar_arrive_expect_tx(bar, total);
-    }
+    if (!go) mbar_arrive_expect_tx(bar, total);
   }
 }
 
 // compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m
 template <bool MIXED>
-__device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const SlotInfo& si,
-                              const unsigned char* sb, double (&lp)[2][2], const Smem& sm) {
+__device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si,
+                               const unsigned char* sb, const Smem& sm) {
+  Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
   using V = typename Prec<MIXED>::V;
   using C = typename Prec<MIXED>::C;
   const GroupDev& g = kp.g[c.gi];
   const TopoDev& tp = g.tp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (warp >= c.nr) return;
-  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.npx, g.ldv, g.ldx, g.ldc);
+  if (warp >= c.nr) return lp;
+  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx, g.ldv, g.ldx, g.ldc);
   const int ni = tp.ni, nj = tp.nj, t = c.t, w = warp, j = c.jc + w;
   const int CP = L.cpitch, col0 = tp.OLx;
   const int crv = (t * nj + j) * g.ldv, crx = (t * nj + j) * g.ldx;
   const long long pe = g.pad_elems;
   const long long prow = (long long)c.inst * pe + ((long long)t * tp.npy + j + tp.OLy) * tp.npx + tp.OLx;
+  PushTab ptab;
+  ptab.tw = reinterpret_cast<const int2*>(sb + L.tw);
+  ptab.te = reinterpret_cast<const int2*>(sb + L.te);
+  ptab.ts = reinterpret_cast<const int2*>(sb + L.ts);
+  ptab.tn = reinterpret_cast<const int2*>(sb + L.tn);
+  ptab.ni = ni;
+  ptab.nj = nj;
 
   auto emit = [&](int s, int i, double p0, double p1) {
     if (kp.serial) {
       double* pr = sm.prod + ((s * 2) * kWarps + w) * kp.max_ni;
       pr[i] = p0;
       pr[kWarps * kp.max_ni + i] = p1;
+    } else if (s == 0) {
+      lp.v[0] = add(lp.v[0], p0);
+      lp.v[1] = add(lp.v[1], p1);
     } else {
-      lp[s][0] = add(lp[s][0], p0);
-      lp[s][1] = add(lp[s][1], p1);
+      lp.v[2] = add(lp.v[2], p0);
+      lp.v[3] = add(lp.v[3], p1);
     }
   };
 
   for (int s = 0; s < g.nrhs; ++s) {
-    const int a = si.act[s];
+    const int a = si.act(s);
     if (a == A_NONE) continue;
     if (a == A_FIN) {
       // pass S after convergence: the pending x update, un-normalised (cg2d.py:254, 266)
@@ -702,8 +836,8 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
       const double* x = vec_ptr<double>(g, c.inst, s, V_X);
       for (int i = lane; i < ni; i += 32) {
         double xv = ldcg(x + crx + i);
-        if (si.has_alpha[s]) xv = add(xv, mul(si.c2[s], (double)ldcg(so + crv + i)));
-        const double xf = __ddiv_rn(xv, si.rnorm[s]);
+        if (si.has_alpha(s)) xv = add(xv, mul(si.c2(s), (double)ldcg(so + crv + i)));
+        const double xf = __ddiv_rn(xv, si.rnorm(s));
         g.x_out[s][prow + i] = xf;
         if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
       }
@@ -722,8 +856,8 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
       const C* cs = reinterpret_cast<const C*>(cb + L.coef_stride);
       const C* cc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
       const int P = L.vpitch[0];
-      const double beta = si.c1[s], alpha_prev = si.c2[s];
-      const bool upd = si.has_alpha[s] != 0;
+      const double beta = si.c1(s), alpha_prev = si.c2(s);
+      const bool upd = si.has_alpha(s) != 0;
       V* s_out = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
       V* s_halo = halo_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
       V* q_out = vec_ptr<V>(g, c.inst, s, V_Q);
@@ -743,13 +877,13 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
         const V q = (V)op_A<C>(cw[cr], cw[cr + 1], cs[cr], cs[cr + CP], cc[cr], (C)vw, (C)ve, (C)vs, (C)vn,
                                (C)vc);                                                        // cg2d.py:251
         stcg(s_out + crv + i, vc);
-        push(tp, s_halo, t, j, i, vc);
+        push_s(ptab, s_halo, j, w, i, vc);
         stcg(q_out + crv + i, q);
-        push(tp, q_halo, t, j, i, q);
+        push_s(ptab, q_halo, j, w, i, q);
         if (upd) {
           const double xn = add(xo[w * g.ldx + i], mul(alpha_prev, (double)so[rc]));         // cg2d.py:254
           stcg(x_out + crx + i, xn);
-          push(tp, x_halo, t, j, i, xn);
+          push_s(ptab, x_halo, j, w, i, xn);
         }
         emit(s, i, mul((double)vc, (double)q), 0.0);                                          // cg2d.py:252
       }
@@ -764,7 +898,7 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
       const C* ps = reinterpret_cast<const C*>(cb + L.coef_stride);
       const C* pc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
       const int P = L.vpitch[0];
-      const double alpha = si.c1[s];
+      const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
@@ -782,9 +916,9 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
         const V z = (V)op_M<C>(pc[cr], pw[cr], pw[cr + 1], ps[cr], ps[cr + CP], (C)vc, (C)vw, (C)ve, (C)vs,
                                (C)vn);                                                        // cg2d.py:245
         stcg(r_out + crv + i, vc);
-        push(tp, r_halo, t, j, i, vc);
+        push_s(ptab, r_halo, j, w, i, vc);
         stcg(z_out + crv + i, z);
-        push(tp, z_halo, t, j, i, z);
+        push_s(ptab, z_halo, j, w, i, z);
         emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));                 // cg2d.py:256, 246
       }
     } else if (pt == P_Z) {
@@ -806,7 +940,7 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
         const V z = (V)op_M<C>(pc[cr], pw[cr], pw[cr + 1], ps[cr], ps[cr + CP], (C)vc, (C)vw, (C)ve,
                                (C)rr_[rc - P], (C)rr_[rc + P]);
         stcg(z_out + crv + i, z);
-        push(tp, z_halo, t, j, i, z);
+        push_s(ptab, z_halo, j, w, i, z);
         emit(s, i, mul((double)z, (double)vc), 0.0);
       }
     } else {  // P_R: the FP64 true residual b - A x_{k+1}
@@ -820,7 +954,7 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
       const double* as = reinterpret_cast<const double*>(cb + L.coef_stride);
       const double* ac = reinterpret_cast<const double*>(cb + 2 * L.coef_stride);
       const int PX = L.vpitch[0], PS = L.vpitch[1];
-      const double alpha = si.c1[s];
+      const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       auto x1 = [&](double xx, V ss) -> double { return add(xx, mul(alpha, (double)ss)); };
@@ -832,61 +966,72 @@ __device__ void compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, 
         const double vs = x1(xr[rx - PX], sk[rs - PS]);
         const double vn = x1(xr[rx + PX], sk[rs + PS]);
         const int cr = w * CP + col0 + i;
-        const double bn = mul(mul(__ldg(g.b[s] + prow + i), si.norm[s]), si.rnorm[s]);
+        const double bn = mul(mul(__ldg(g.b[s] + prow + i), si.norm(s)), si.rnorm(s));
         const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + CP], ac[cr], vw, ve, vs, vn, vc));
         stcg(r_out + crv + i, r);
-        push(tp, r_halo, t, j, i, r);
+        push_s(ptab, r_halo, j, w, i, r);
         emit(s, i, mul((double)r, (double)r), 0.0);
       }
     }
   }
+  return lp;
 }
 
 template <bool MIXED>
 __device__ bool run_pass_tma(const KParams& kp, int pt, int k, int hidx, const Smem& sm, unsigned& phase) {
   const int tid = threadIdx.x;
   Chunk cur;
-  if (!chunk_unit(kp, sm, blockIdx.x, cur)) return true;
+  if (!chunk_unit(kp, sm, blockIdx.x, cur)) return reduce_pass(kp, pt, hidx, sm);
   const int ns = kp.nstage[pt];
   int st = 0;
+  unsigned long long t0 = PROF_T0(kp);
   if (tid == 0) issue_chunk<MIXED>(kp, cur, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
+  PROF_ADD(kp, sm, PR_ISSUE, t0);
   Chunk nxt = cur;
   bool have_next = chunk_next(kp, sm, nxt);
   bool have = true;
-  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
   while (have) {
+    t0 = PROF_T0(kp);
     if (ns == 2 && have_next && tid == 0)
       issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage + (st ^ 1) * kp.stage_bytes, &sm.bar[st ^ 1]);
+    PROF_ADD(kp, sm, PR_ISSUE, t0);
+    t0 = PROF_T0(kp);
     const bool ok = mbar_wait(&sm.bar[st], (phase >> st) & 1u, kp.timeout_ns);
     phase ^= 1u << st;
+    PROF_ADD(kp, sm, PR_MBAR, t0);
     if (__syncthreads_or(!ok)) {
       // a copy did not complete in time: flag the error, give the copies in flight a bounded time to land
-      if (tid == 0) atomicCAS(&kp.gs[1], 0u, (unsigned)CG2D_BARRIER_TIMEOUT);
+      if (tid == 0) note_timeout(kp.gs, 2u, (unsigned)pt);
       mbar_wait(&sm.bar[st], ((phase >> st) & 1u) ^ 1u, kp.timeout_ns);
       if (ns == 2 && have_next) mbar_wait(&sm.bar[st ^ 1], (phase >> (st ^ 1)) & 1u, kp.timeout_ns);
       __syncthreads();
       return false;
     }
     const GroupDev& g = kp.g[cur.gi];
-    SlotInfo si;
-    slot_info(g, cur.inst, sm, si);
-    if (tid == 0 && cur.jc == cur.j0u) acc[0][0] = acc[0][1] = acc[1][0] = acc[1][1] = 0.0;
-    double lp[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
-    compute_chunk<MIXED>(kp, cur, pt, k, si, sm.stage + st * kp.stage_bytes, lp, sm);
+    const Slots si = slots_of(g, cur.inst, sm);
+    const int ns0 = nsums(pt, si.act(0));
+    const int ns1 = g.nrhs > 1 ? nsums(pt, si.act(1)) : 0;
+    if (tid == 0 && cur.jc == cur.j0u) sm.uacc[0] = sm.uacc[1] = sm.uacc[2] = sm.uacc[3] = 0.0;
+    t0 = PROF_T0(kp);
+    const Lanes lp = compute_chunk<MIXED>(kp, cur, pt, k, si, sm.stage + st * kp.stage_bytes, sm);
     if ((tid >> 5) < cur.nr && !kp.serial) row_sums(g, lp, sm);
     __syncthreads();
-    if (tid == 0) accumulate_chunk(kp, g, pt, si, cur.nr, acc, sm);
-    if (cur.jc + cur.nr >= cur.j1u) finish_unit(kp, g, cur.inst, cur.lu, pt, hidx, si, acc, sm);
-    if (ns == 1 && have_next) {
-      __syncthreads();
-      if (tid == 0) issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
-    }
+    if (tid == 0) accumulate_chunk(kp, g, ns0, ns1, cur.nr, sm);
+    PROF_ADD(kp, sm, PR_COMP, t0);
+    if (cur.jc + cur.nr >= cur.j1u) finish_unit(kp, g, cur.inst, cur.lu, ns0, ns1, sm);
+    // row sums and stage buffers are rewritten by the next chunk
+    __syncthreads();
+    if (ns == 1 && have_next && tid == 0) issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
     cur = nxt;
     have = have_next;
     if (have) have_next = chunk_next(kp, sm, nxt);
     if (ns == 2) st ^= 1;
   }
-  return true;
+  __syncthreads();
+  t0 = PROF_T0(kp);
+  const bool ok = reduce_pass(kp, pt, hidx, sm);
+  PROF_ADD(kp, sm, PR_FIN, t0);
+  return ok;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -919,12 +1064,15 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_constant__ KParams kp) {
+__global__ void __launch_bounds__(kThreads, 1) cg2d_persistent(const __grid_constant__ KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const Smem sm = carve(smem_raw, kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
   unsigned target = (unsigned)kp.test_missing;
   unsigned phase = 0;
+  const unsigned long long t_start = PROF_T0(kp);
+  if (tid < 8) sm.pacc[tid] = 0ull;
+  for (int i = tid; i < kMaxOps; i += kThreads) sm.opn[i] = 0u;
   if (tid == 0) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);
@@ -952,8 +1100,8 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
 
   // ---- rhsMax = max |b cg2dNorm| (cg2d.py:221-225)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  run_pass_direct<MIXED>(kp, P_MAX, sm);
-  ok = grid_barrier(kp, target, sm.misc);
+  ok = run_pass_direct<MIXED>(kp, P_MAX, sm);
+  ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
   if (!ok) goto epilogue;
   if (own) {
     rhsMax = __longlong_as_double((long long)__ldcg(&kp.rmax[tid]));
@@ -962,15 +1110,15 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
   }
   // ---- x = x0 rhsNorm, r = b - A x, s = 0, err^2, sumRHS (cg2d.py:226-236)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  run_pass_direct<MIXED>(kp, P_INIT, sm);
   init_x_halo(kp, sm);
-  ok = grid_barrier(kp, target, sm.misc);
+  ok = run_pass_direct<MIXED>(kp, P_INIT, sm);
+  ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
   if (!ok) goto epilogue;
   if (own) rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   ok = run_pass_tma<MIXED>(kp, P_Z, 0, 0, sm, phase);
-  ok = grid_barrier(kp, target, sm.misc) && ok;
+  ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
   if (!ok) goto epilogue;
   if (own) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
 
@@ -994,7 +1142,7 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
     ok = run_pass_tma<MIXED>(kp, P_S, k, k, sm, phase);
-    ok = grid_barrier(kp, target, sm.misc) && ok;
+    ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
     if (a == A_ACTIVE) {
@@ -1012,7 +1160,7 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, alpha, 0.0);
       ok = run_pass_tma<MIXED>(kp, P_X, k, k + 1, sm, phase);
-      ok = grid_barrier(kp, target, sm.misc) && ok;
+      ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
         rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
@@ -1022,7 +1170,7 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, alpha, 0.0);
       ok = run_pass_tma<MIXED>(kp, P_R, k, k + 1, sm, phase);
-      ok = grid_barrier(kp, target, sm.misc) && ok;
+      ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
         rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
@@ -1030,7 +1178,7 @@ __global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_cons
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
       ok = run_pass_tma<MIXED>(kp, P_Z, k, k + 1, sm, phase);
-      ok = grid_barrier(kp, target, sm.misc) && ok;
+      ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
     }
@@ -1090,6 +1238,15 @@ epilogue:
     else d.status = CG2D_OK;
     if (!ok) { d.firstResidual = d.lastResidual = d.sumRHS = __longlong_as_double(0x7ff8000000000000LL); }
     g.diag[slot][inst] = d;
+  }
+  if (kp.prof && tid == 0 && blockIdx.x < kMaxCtas) {
+    unsigned long long* o = kp.prof + 1 + (size_t)blockIdx.x * 8;
+    const unsigned long long tot = globaltimer() - t_start;
+    unsigned long long acc = 0;
+    for (int i = 0; i < PR_OTHER; ++i) { o[i] = sm.pacc[i]; acc += sm.pacc[i]; }
+    o[PR_OTHER] = tot > acc ? tot - acc : 0ull;
+    o[PR_TOTAL] = tot;
+    if (blockIdx.x == 0) kp.prof[0] = gridDim.x;
   }
 }
 

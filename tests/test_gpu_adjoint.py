@@ -68,11 +68,11 @@ def test_gradients_match_central_differences(prob):
     grads = [aW_t.grad.cpu().numpy(), aC_t.grad.cpu().numpy(), b_t.grad.cpu().numpy()]
     base = [ops[0], ops[2], syn.rhs()]
     # a 3x3 window whose west faces are all wet (first one found scanning tile 4, then the others)
-    J, I = L.interior
+    Jw, Iw = L.interior
     found = None
     for t in (4, 3, 5, 1, 7, 8):
-        for j in range(J.start, J.stop - 2):
-            for i in range(I.start, I.stop - 2):
+        for j in range(Jw.start, Jw.stop - 2):
+            for i in range(Iw.start, Iw.stop - 2):
                 if np.all(ops[0][t, j:j + 3, i:i + 3] != 0):
                     found = (t, j, i)
                     break
