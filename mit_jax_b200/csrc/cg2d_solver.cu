@@ -41,6 +41,7 @@ __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, 
 __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
 
 // apply_operator (cg2d.py:181-188): aW(i)x(i-1) + aW(i+1)x(i+1) + aS(j)x(j-1) + aS(j+1)x(j+1) + aC x
 template <class T>
@@ -162,6 +163,7 @@ struct Smem {
   unsigned long long* pacc; // [8] phase times of this CTA (thread 0; profiling)
   unsigned* opn;            // [kMaxOps] passes with sums each operator has completed (its counter target)
   double* uacc;             // [4] thread 0: the current unit's partial sums (slot, kind)
+  unsigned* ucnt;           // [kMaxOps] units this CTA completed in the current pass, per operator
   double* prod;      // FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]
   unsigned char* stage;     // 2 x stage_bytes (128-aligned); also the direct-load staging area
 };
@@ -181,6 +183,7 @@ size_t fixed_smem_bytes(int max_ni, int serial) {
   s += a16(sizeof(unsigned long long) * 8);
   s += a16(sizeof(unsigned) * kMaxOps);
   s += a16(sizeof(double) * 4);
+  s += a16(sizeof(unsigned) * kMaxOps);
   if (serial) s += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni);
   return (s + 127) & ~size_t(127);
 }
@@ -202,6 +205,7 @@ __device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
   m.pacc = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 8);
   m.opn = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
   m.uacc = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 4);
+  m.ucnt = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
   m.prod = nullptr;
   if (serial) { m.prod = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni); }
   o = (o + 127) & ~size_t(127);
@@ -227,6 +231,7 @@ __device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag, uns
     for (unsigned spins = 0;; ++spins) {
       const unsigned v = ld_acquire(&kp.gs[0]);
       if ((int)(v - target) >= 0) break;
+      if (spins > 8) __nanosleep(64);
       if (ld_relaxed(&kp.gs[1]) != 0u) { ok = 0; break; }
       if ((spins & 63u) == 63u && globaltimer() - t0 > kp.timeout_ns) {
         note_timeout(kp.gs, 1u, 0u);
@@ -387,25 +392,34 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
   }
 }
 
-// thread 0 writes the unit's partials and counts the unit done (release: the partials are visible to whoever
-// observes the count); no wait
+// thread 0 writes the unit's partials (no wait) and counts the unit in shared memory; the counts are published
+// once per pass (publish_counts)
 __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-__device__ __noinline__ void finish_unit(const KParams& kp, int op, int lu, int rid0, int rid1, int ns0, int ns1,
-                                        double a00, double a01, double a10, double a11) {
-  if (ns0 + ns1 == 0) return;
-  if (ns0 > 0) stcg(kp.part + ((size_t)rid0 * 2 + 0) * kp.part_units + lu, a00);
-  if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, a01);
-  if (ns1 > 0) stcg(kp.part + ((size_t)rid1 * 2 + 0) * kp.part_units + lu, a10);
-  if (ns1 > 1) stcg(kp.part + ((size_t)rid1 * 2 + 1) * kp.part_units + lu, a11);
-  red_release_add(&kp.cnt[op], 1u);
-}
 __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int ns0, int ns1,
                                             const Smem& sm) {
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x != 0 || ns0 + ns1 == 0) return;
   const int rid0 = g.rhs_base + inst * g.nrhs;
-  finish_unit(kp, g.op_base + inst, lu, rid0, rid0 + 1, ns0, ns1, sm.uacc[0], sm.uacc[1], sm.uacc[2], sm.uacc[3]);
+  if (ns0 > 0) stcg(kp.part + ((size_t)rid0 * 2 + 0) * kp.part_units + lu, sm.uacc[0]);
+  if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, sm.uacc[1]);
+  if (ns1 > 0) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 0) * kp.part_units + lu, sm.uacc[2]);
+  if (ns1 > 1) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 1) * kp.part_units + lu, sm.uacc[3]);
+  sm.ucnt[g.op_base + inst] += 1u;
+}
+// every CTA, end of its units: add its unit counts to the operators' counters (release: the partials written
+// before are visible to whoever observes the count)
+__device__ __forceinline__ void publish_counts(const KParams& kp, const Smem& sm) {
+  if (threadIdx.x == 0) __threadfence();
+  __syncthreads();
+  for (int op = threadIdx.x; op < kp.total_ops; op += kThreads) {
+    const unsigned c = sm.ucnt[op];
+    if (c) {
+      red_release_add(&kp.cnt[op], c);
+      sm.ucnt[op] = 0u;
+    }
+  }
+  __syncthreads();
 }
 
 // End of a pass: the CTA that owns an instance's last unit waits until all of the instance's units are counted,
@@ -413,6 +427,7 @@ __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g
 // order from 0 (GLOBAL_SUM_TILE, global_sum.py:20-26). Then every CTA advances the operators' counter targets.
 __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  publish_counts(kp, sm);
   double* buf = reinterpret_cast<double*>(sm.stage);   // free at the end of a pass
   bool ok = true;
   for (int gi = 0; gi < kp.ngroups && ok; ++gi) {
@@ -433,6 +448,7 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
         int good = 1;
         for (unsigned spins = 0;; ++spins) {
           if ((int)(ld_acquire(&kp.cnt[op]) - target) >= 0) break;
+          if (spins > 8) __nanosleep(64);
           if ((spins & 63u) == 63u && (ld_relaxed(&kp.gs[1]) != 0u || globaltimer() - t0 > kp.timeout_ns)) {
             note_timeout(kp.gs, 3u, (unsigned)pt);
             good = 0;
@@ -714,78 +730,87 @@ __device__ __forceinline__ void pass_vectors(int pt, int k, int hidx, int (&ids)
   else { ids[0] = (hidx & 1) ? V_R1 : V_R0; ids[1] = -1; }
 }
 
-// thread 0: bulk copies of chunk c into the stage buffer sb, completion on bar
+// warp 0: bulk copies of chunk c into the stage buffer sb, completion on bar. Each lane owns one fixed copy
+// (a lane whose copy is not needed moves 0 bytes): lanes 0-2 the coefficient rows, 3-6 the push targets
+// (W, E, S, N), 7 + 5 (2 s + v) + piece the vector pieces of slot s, vector v (rows, west and east neighbours,
+// south and north halo rows), 27 + s the own rows of x (pass S).
 template <bool MIXED>
 __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, int hidx, const Smem& sm,
                             unsigned char* sb, unsigned long long* bar) {
   const GroupDev& g = kp.g[c.gi];
   const TopoDev& tp = g.tp;
+  const int lane = threadIdx.x & 31;
   const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx, g.ldv, g.ldx, g.ldc);
-  int act[2], hasal[2];
-  bool any = false;
-  for (int s = 0; s < 2; ++s) {
-    const int r = g.rhs_base + c.inst * g.nrhs + s;
-    act[s] = s < g.nrhs ? sm.act[r] : A_NONE;
-    hasal[s] = s < g.nrhs ? sm.has_alpha[r] : 0;
-    any |= act[s] == A_ACTIVE;
-  }
-  // two passes over the same plan: count the bytes and arm the mbarrier, then issue the copies
-  const int first = (pt == P_X || pt == P_Z) ? 3 : 0;   // M = (pW, pS, pC) or A = (aW2d, aS2d, aC2d)
-  int ids[2];
-  pass_vectors(pt, k, hidx, ids);
-  const int jlo = max(c.jc - 1, 0), jhi = min(c.jc + c.nr, tp.nj - 1);
-  unsigned total = 0;
-  for (int go = 0; go < 2; ++go) {
-    auto cp = [&](void* d, const void* s_, unsigned bytes) {
-      if (go) bulk_g2s(d, s_, bytes, bar);
-      else total += bytes;
-    };
+  const int rid0 = g.rhs_base + c.inst * g.nrhs;
+  const bool act0 = sm.act[rid0] == A_ACTIVE;
+  const bool act1 = g.nrhs > 1 && sm.act[rid0 + 1] == A_ACTIVE;
+  const bool any = act0 || act1;
+  const int T = tp.T, nj = tp.nj, ni = tp.ni, njp = tp.njp, nip = tp.nip;
+  const bool bottom = c.jc == 0, top = c.jc + c.nr == nj;
+  void* dst = nullptr;
+  const void* src = nullptr;
+  unsigned bytes = 0;
+  if (lane < 3) {
     if (any) {
-      for (int a = 0; a < 3; ++a) {
-        const void* base;
-        if (L.csize == 8)
-          base = g.a64[first + a] + (long long)c.inst * g.pad_elems +
-                 ((long long)c.t * tp.npy + c.jc + tp.OLy) * tp.npx;
-        else
-          base = g.c32 + (((long long)c.inst * 6 + first + a) * tp.T * tp.npy + (long long)c.t * tp.npy + c.jc +
-                          tp.OLy) * g.ldc;
-        cp(sb + L.coef + a * L.coef_stride, base, (unsigned)((c.nr + 1) * L.cpitch * L.csize));
-      }
-      // push targets of the chunk's edge points
-      const unsigned tb = al16((unsigned)(c.nr * 8));
-      cp(sb + L.tw, tp.tg + 2 * ((long long)c.t * tp.njp + c.jc), tb);
-      cp(sb + L.te, tp.tg + 2 * ((long long)(tp.T + c.t) * tp.njp + c.jc), tb);
-      if (c.jc == 0)
-        cp(sb + L.ts, tp.tg + 2 * ((long long)2 * tp.T * tp.njp + (long long)c.t * tp.nip), al16((unsigned)(tp.ni * 8)));
-      if (c.jc + c.nr == tp.nj)
-        cp(sb + L.tn, tp.tg + 2 * ((long long)2 * tp.T * tp.njp + (long long)(tp.T + c.t) * tp.nip),
-           al16((unsigned)(tp.ni * 8)));
+      const int first = (pt == P_X || pt == P_Z) ? 3 : 0;   // M = (pW, pS, pC) or A = (aW2d, aS2d, aC2d)
+      if (L.csize == 8)
+        src = g.a64[first + lane] + (long long)c.inst * g.pad_elems + ((long long)c.t * tp.npy + c.jc + tp.OLy) * tp.npx;
+      else
+        src = g.c32 + (((long long)c.inst * 6 + first + lane) * T * tp.npy + (long long)c.t * tp.npy + c.jc + tp.OLy) *
+                          g.ldc;
+      dst = sb + L.coef + lane * L.coef_stride;
+      bytes = (unsigned)((c.nr + 1) * L.cpitch * L.csize);
     }
-    for (int s = 0; s < g.nrhs; ++s) {
-      if (act[s] != A_ACTIVE) continue;
-      for (int v = 0; v < L.nvec; ++v) {
-        const int sz = L.vsize[v], P = L.vpitch[v];
-        const char* vb = vec_ptr<const char>(g, c.inst, s, ids[v]);
-        const char* hb = halo_ptr<const char>(g, c.inst, s, ids[v]);
-        cp(sb + L.vec[s][v] + (jlo - c.jc + 1) * P * sz, vb + (long long)(c.t * tp.nj + jlo) * P * sz,
-           (unsigned)((jhi - jlo + 1) * P * sz));
-        const unsigned hbytes = al16((unsigned)(c.nr * sz));
-        cp(sb + L.hw[s][v], hb + ((long long)c.t * tp.njp + c.jc) * sz, hbytes);
-        cp(sb + L.he[s][v], hb + ((long long)(tp.T + c.t) * tp.njp + c.jc) * sz, hbytes);
-        if (c.jc == 0)
-          cp(sb + L.vec[s][v], hb + ((long long)2 * tp.T * tp.njp + (long long)c.t * tp.nip) * sz,
-             al16((unsigned)(tp.ni * sz)));
-        if (c.jc + c.nr == tp.nj)
-          cp(sb + L.vec[s][v] + (c.nr + 1) * P * sz,
-             hb + ((long long)2 * tp.T * tp.njp + (long long)(tp.T + c.t) * tp.nip) * sz, al16((unsigned)(tp.ni * sz)));
-      }
-      if (pt == P_S && hasal[s]) {
-        const char* xb = vec_ptr<const char>(g, c.inst, s, V_X);
-        cp(sb + L.xo[s], xb + (long long)(c.t * tp.nj + c.jc) * g.ldx * 8, (unsigned)(c.nr * g.ldx * 8));
+  } else if (lane < 7) {
+    const int side = lane - 3;   // W, E, S, N push-target slices
+    if (any && (side < 2 || (side == 2 && bottom) || (side == 3 && top))) {
+      long long e;
+      if (side < 2) e = (long long)(side * T + c.t) * njp + c.jc;
+      else e = (long long)2 * T * njp + (long long)((side - 2) * T + c.t) * nip;
+      src = tp.tg + 2 * e;
+      dst = sb + (side == 0 ? L.tw : side == 1 ? L.te : side == 2 ? L.ts : L.tn);
+      bytes = side < 2 ? al16((unsigned)(c.nr * 8)) : al16((unsigned)(ni * 8));
+    }
+  } else if (lane < 27) {
+    const int q = lane - 7, sv = q / 5, piece = q - sv * 5;
+    const int s = sv >> 1, v = sv & 1;
+    if (s < g.nrhs && (s == 0 ? act0 : act1) && v < L.nvec) {
+      int id;
+      if (pt == P_S) id = v == 0 ? V_Z : (((k + 1) & 1) ? V_S1 : V_S0);
+      else if (pt == P_X) id = v == 0 ? ((k & 1) ? V_R1 : V_R0) : V_Q;
+      else if (pt == P_R) id = v == 0 ? V_X : ((k & 1) ? V_S1 : V_S0);
+      else id = (hidx & 1) ? V_R1 : V_R0;
+      const int sz = L.vsize[v], P = L.vpitch[v];
+      const char* vb = vec_ptr<const char>(g, c.inst, s, id);
+      const char* hb = halo_ptr<const char>(g, c.inst, s, id);
+      const unsigned char* vd = sb + L.vec[s][v];
+      if (piece == 0) {
+        const int jlo = max(c.jc - 1, 0), jhi = min(c.jc + c.nr, nj - 1);
+        src = vb + (long long)(c.t * nj + jlo) * P * sz;
+        dst = const_cast<unsigned char*>(vd) + (jlo - c.jc + 1) * P * sz;
+        bytes = (unsigned)((jhi - jlo + 1) * P * sz);
+      } else if (piece <= 2) {
+        src = hb + ((long long)((piece - 1) * T + c.t) * njp + c.jc) * sz;
+        dst = sb + (piece == 1 ? L.hw[s][v] : L.he[s][v]);
+        bytes = al16((unsigned)(c.nr * sz));
+      } else if ((piece == 3 && bottom) || (piece == 4 && top)) {
+        src = hb + ((long long)2 * T * njp + (long long)((piece - 3) * T + c.t) * nip) * sz;
+        dst = const_cast<unsigned char*>(vd) + (piece == 3 ? 0 : (c.nr + 1) * P * sz);
+        bytes = al16((unsigned)(ni * sz));
       }
     }
-    if (!go) mbar_arrive_expect_tx(bar, total);
+  } else if (lane < 29) {
+    const int s = lane - 27;
+    if (pt == P_S && s < g.nrhs && (s == 0 ? act0 : act1) && sm.has_alpha[rid0 + s]) {
+      src = vec_ptr<const char>(g, c.inst, s, V_X) + (long long)(c.t * nj + c.jc) * g.ldx * 8;
+      dst = sb + L.xo[s];
+      bytes = (unsigned)(c.nr * g.ldx * 8);
+    }
   }
+  const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
+  if (lane == 0) mbar_arrive_expect_tx(bar, total);
+  __syncwarp();
+  if (bytes) bulk_g2s(dst, src, bytes, bar);
 }
 
 // compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m
@@ -864,8 +889,9 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       V* q_halo = halo_ptr<V>(g, c.inst, s, V_Q);
       double* x_out = vec_ptr<double>(g, c.inst, s, V_X);
       double* x_halo = halo_ptr<double>(g, c.inst, s, V_X);
-      // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike
-      auto sn = [&](V zz, V ss) -> V { return (V)add((double)zz, mul(beta, (double)ss)); };
+      // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike (MIXED: in FP32)
+      const V betav = (V)beta;
+      auto sn = [&](V zz, V ss) -> V { return add(zz, mul(betav, ss)); };
       for (int i = lane; i < ni; i += 32) {
         const int rc = (w + 1) * P + i;
         const V vc = sn(zr[rc], so[rc]);
@@ -903,8 +929,9 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
       V* z_halo = halo_ptr<V>(g, c.inst, s, V_Z);
-      // r_{k+1} = r_k - alpha_k q_k (cg2d.py:255)
-      auto rn = [&](V rr, V qq) -> V { return (V)sub((double)rr, mul(alpha, (double)qq)); };
+      // r_{k+1} = r_k - alpha_k q_k (cg2d.py:255) (MIXED: in FP32)
+      const V alphav = (V)alpha;
+      auto rn = [&](V rr, V qq) -> V { return sub(rr, mul(alphav, qq)); };
       for (int i = lane; i < ni; i += 32) {
         const int rc = (w + 1) * P + i;
         const V vc = rn(ro[rc], qv[rc]);
@@ -985,14 +1012,14 @@ __device__ bool run_pass_tma(const KParams& kp, int pt, int k, int hidx, const S
   const int ns = kp.nstage[pt];
   int st = 0;
   unsigned long long t0 = PROF_T0(kp);
-  if (tid == 0) issue_chunk<MIXED>(kp, cur, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
+  if ((tid >> 5) == 0) issue_chunk<MIXED>(kp, cur, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
   PROF_ADD(kp, sm, PR_ISSUE, t0);
   Chunk nxt = cur;
   bool have_next = chunk_next(kp, sm, nxt);
   bool have = true;
   while (have) {
     t0 = PROF_T0(kp);
-    if (ns == 2 && have_next && tid == 0)
+    if (ns == 2 && have_next && (tid >> 5) == 0)
       issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage + (st ^ 1) * kp.stage_bytes, &sm.bar[st ^ 1]);
     PROF_ADD(kp, sm, PR_ISSUE, t0);
     t0 = PROF_T0(kp);
@@ -1021,7 +1048,7 @@ __device__ bool run_pass_tma(const KParams& kp, int pt, int k, int hidx, const S
     if (cur.jc + cur.nr >= cur.j1u) finish_unit(kp, g, cur.inst, cur.lu, ns0, ns1, sm);
     // row sums and stage buffers are rewritten by the next chunk
     __syncthreads();
-    if (ns == 1 && have_next && tid == 0) issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
+    if (ns == 1 && have_next && (tid >> 5) == 0) issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
     cur = nxt;
     have = have_next;
     if (have) have_next = chunk_next(kp, sm, nxt);
@@ -1064,7 +1091,7 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads, 1) cg2d_persistent(const __grid_constant__ KParams kp) {
+__global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_constant__ KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const Smem sm = carve(smem_raw, kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
@@ -1072,7 +1099,7 @@ __global__ void __launch_bounds__(kThreads, 1) cg2d_persistent(const __grid_cons
   unsigned phase = 0;
   const unsigned long long t_start = PROF_T0(kp);
   if (tid < 8) sm.pacc[tid] = 0ull;
-  for (int i = tid; i < kMaxOps; i += kThreads) sm.opn[i] = 0u;
+  for (int i = tid; i < kMaxOps; i += kThreads) { sm.opn[i] = 0u; sm.ucnt[i] = 0u; }
   if (tid == 0) {
     mbar_init(&sm.bar[0], 1);
     mbar_init(&sm.bar[1], 1);

@@ -165,8 +165,8 @@ def cg2d_fortran(L, tmap, ops, cg2d_b, cg2d_x, *, cg2dNorm, tolerance, max_iters
 def cg2d_mixed(L, tmap, ops, cg2d_b, cg2d_x, *, cg2dNorm, tolerance, max_iters, replace_every=25,
                replace_above=100.0, rows_per_block=8):
     """The GPU solver's MIXED iteration, operation for operation: r, s, z, q and the stencil coefficients in
-    float32 (float32 stencil arithmetic), x and every dot product in float64 (products of float32 values are exact
-    in float64), the s and r updates formed in float64 and rounded to float32. At iteration k (0-based) with
+    float32 (float32 stencil arithmetic and float32 updates s = z + float32(beta) s, r = r - float32(alpha) q), x and
+    every dot product in float64 (products of float32 values are exact in float64). At iteration k (0-based) with
     (k+1) % replace_every == 0, while the residual entering the iteration is above replace_above * tolerance, the
     updated r is instead the float64 true residual b - A x (float64 operator), and z = M r, eta follow from it.
     The stop rule is the reference's, on the residual the iteration carries (cg2d.py:238-241).
@@ -216,7 +216,7 @@ def cg2d_mixed(L, tmap, ops, cg2d_b, cg2d_x, *, cg2dNorm, tolerance, max_iters, 
     while it < max_iters and not (err_sq < tol2):
         beta = eta / eta_prev
         eta_prev = eta
-        s = (z.astype(np.float64) + beta * s.astype(np.float64)).astype(np.float32)
+        s = z + np.float32(beta) * s
         q = apply_operator(L, aW32, aS32, aC32, ex32(s))
         alpha = eta / S(s.astype(np.float64) * q.astype(np.float64))
         x = x + alpha * s.astype(np.float64)
@@ -224,7 +224,7 @@ def cg2d_mixed(L, tmap, ops, cg2d_b, cg2d_x, *, cg2dNorm, tolerance, max_iters, 
             r = true_residual(x)
             nrep += 1
         else:
-            r = (r.astype(np.float64) - alpha * q.astype(np.float64)).astype(np.float32)
+            r = r - np.float32(alpha) * q
         err_sq = S(r.astype(np.float64) ** 2)
         z, eta = precond(r)
         it += 1
