@@ -1091,7 +1091,7 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kThreads, 2) cg2d_persistent(const __grid_constant__ KParams kp) {
+__global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const __grid_constant__ KParams kp) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const Smem sm = carve(smem_raw, kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
