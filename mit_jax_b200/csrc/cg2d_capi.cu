@@ -12,9 +12,9 @@
 
 struct cg2d_topology {
   int sNx, sNy, OLx, OLy, nTiles;
-  int njp, nip;      // halo slice pitches (multiples of 4)
+  int nip;           // column pitch of the S/N push-target lists (even)
   int* d_nbr;        // [4][...] W, E (T*sNy each), S, N (T*sNx each)
-  int* d_tg;         // push targets: W, E [T][njp][2], S, N [T][nip][2] (halo slots, -1 = none)
+  int* d_tg;         // push targets (ring cells of the vectors, -1 = none): WE [T][sNy][4], S, N [T][nip][2]
   int* d_src;        // full padded map
   int8_t* d_comp;
   int device;
@@ -31,8 +31,8 @@ TopoDev topo_dev(const cg2d_topology* tp) {
   TopoDev d;
   d.nbr = tp->d_nbr;
   d.tg = tp->d_tg;
-  d.njp = tp->njp;
   d.nip = tp->nip;
+  d.P = vec_pitch(tp->sNx);
   d.map_src = tp->d_src;
   d.map_comp = tp->d_comp;
   d.ni = tp->sNx;
@@ -46,11 +46,10 @@ TopoDev topo_dev(const cg2d_topology* tp) {
 }
 
 struct WsLayout {
-  size_t gs, rmax, cnt, prof, halo_begin, zero_end, hist, part, total;
-  size_t vec[kMaxGroups], c32[kMaxGroups], halo[kMaxGroups];
-  long long vec_stride[kMaxGroups], halo_stride[kMaxGroups];
-  long long vec_off[kMaxGroups][V_NVEC], halo_off[kMaxGroups][V_NVEC];
-  int ldv[kMaxGroups], ldx[kMaxGroups], ldc[kMaxGroups];
+  size_t gs, rmax, cnt, prof, zero_end, hist, part, total;
+  size_t vec[kMaxGroups], cpk[kMaxGroups];
+  long long vec_stride[kMaxGroups];
+  long long vec_off[kMaxGroups][V_NVEC];
   int hist_len, part_units, total_rhs, total_ops, total_units, max_ni;
   int nblk[kMaxGroups], units[kMaxGroups];
   int ch, nstage[P_NPASS];
@@ -81,11 +80,11 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
       const cg2d_topology* tp = gr[g].topo;
       const int npx = tp->sNx + 2 * tp->OLx;
       for (int pt : {P_S, P_X, P_Z}) {
-        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, tp->sNx, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
+        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, tp->sNx, npx);
         if (S.total > hot) hot = S.total;
       }
       if (mixed) {
-        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, tp->sNx, npx, L->ldv[g], L->ldx[g], L->ldc[g]);
+        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, tp->sNx, npx);
         if (S.total > rep) rep = S.total;
       }
     }
@@ -132,9 +131,6 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     L->units[g] = L->nblk[g] * tp->nTiles;
     if (L->units[g] > L->part_units) L->part_units = L->units[g];
     if (tp->sNx > L->max_ni) L->max_ni = tp->sNx;
-    L->ldv[g] = round_up(tp->sNx, (int)(16 / vsz));
-    L->ldx[g] = round_up(tp->sNx, 2);
-    L->ldc[g] = round_up(tp->sNx + 2 * tp->OLx, 4);
     L->total_rhs += G.count * G.nrhs;
     L->total_ops += G.count;
     const long long tu = (long long)L->total_units + (long long)G.count * L->units[g];
@@ -151,33 +147,21 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
   L->cnt = o; o += al(sizeof(unsigned) * L->total_ops);
   L->prof = o;
   if (p->profile) o += al(sizeof(unsigned long long) * (1 + (size_t)kMaxCtas * 8));
-  L->halo_begin = o;
-  for (int g = 0; g < ng; ++g) {
-    const cg2d_topology* tp = gr[g].topo;
-    const long long hn = (long long)tp->nTiles * (2 * tp->njp + 2 * tp->nip);
-    long long off = 0;
-    for (int v = 0; v < V_NVEC; ++v) {
-      L->halo_off[g][v] = off;
-      off += (long long)al((v == V_X ? sizeof(double) : vsz) * hn);
-    }
-    L->halo_stride[g] = off;
-    L->halo[g] = o;
-    o += al((size_t)off * gr[g].count * gr[g].nrhs);
-  }
   L->zero_end = o;
   L->hist = o; o += al(sizeof(double) * (size_t)L->total_rhs * H_NKIND * L->hist_len);
   L->part = o; o += al(sizeof(double) * (size_t)L->total_rhs * 2 * L->part_units);
   for (int g = 0; g < ng; ++g) {
     const cg2d_topology* tp = gr[g].topo;
-    const long long rows = (long long)tp->nTiles * tp->sNy;
-    const long long npy = tp->sNy + 2 * tp->OLy;
+    // ringed vector tiles [T][sNy+2][P]
+    const long long elems = (long long)tp->nTiles * (tp->sNy + 2) * vec_pitch(tp->sNx);
     long long off = 0;
-    L->vec_off[g][V_X] = off; off += (long long)al(sizeof(double) * rows * L->ldx[g]);
-    for (int v = 1; v < V_NVEC; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * rows * L->ldv[g]); }
+    L->vec_off[g][V_X] = off; off += (long long)al(sizeof(double) * elems);
+    for (int v = 1; v < V_NVEC; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * elems); }
     L->vec_stride[g] = off;
     L->vec[g] = o; o += al((size_t)off * gr[g].count * gr[g].nrhs);
-    L->c32[g] = o;
-    if (mixed) o += al(sizeof(float) * 6 * (size_t)tp->nTiles * npy * L->ldc[g] * gr[g].count);
+    // packed coefficients [count][2][T][sNy+1][3][ldc] (the solver's precision)
+    L->cpk[g] = o;
+    o += al(vsz * 2 * (size_t)tp->nTiles * (tp->sNy + 1) * 3 * coef_pitch(tp->sNx) * gr[g].count);
   }
   L->total = o;
   return CG2D_OK;
@@ -254,40 +238,43 @@ cg2d_status_t cg2d_topology_create(int sNx, int sNy, int OLx, int OLy, int nTile
       if (comp[pn] == 1 && !to_cmp(src[pn], &N[t * sNx + i])) return CG2D_BAD_ARG;
     }
   }
-  // push targets: every halo slot (side, tile, position) with a source point is filled by that point's
-  // owner; a source must lie on its own tile's edge, with at most two slots per edge point
-  const int njp = round_up(sNy, 4), nip = round_up(sNx, 4);
-  // target lists by side: a point with i == 0 uses the W list (row j), i == sNx-1 the E list, otherwise
-  // j == 0 the S list (column i) and j == sNy-1 the N list
-  std::vector<int> tg((size_t)nTiles * (2 * njp + 2 * nip) * 2, -1);
-  auto add_target = [&](int c, int slot) -> bool {
+  // push targets: every ring cell (side, tile, position) of the vectors that has a source is filled by that
+  // point's owner whenever it writes the value. A source must lie on its own tile's edge, with at most two
+  // target cells per edge point. A target is the cell's element in a ringed vector [T][sNy+2][P].
+  const int P = vec_pitch(sNx);
+  const int nip = round_up(sNx, 2);
+  if ((long long)nTiles * (sNy + 2) * P > (1ll << 31) - 1) return CG2D_UNSUPPORTED;
+  auto cell = [&](int t, int j, int i) { return (int)(((long long)t * (sNy + 2) + j + 1) * P + i + 1); };
+  // lists by the source point's position: i == 0 -> WE row j (first pair), i == sNx-1 -> WE row j (second
+  // pair), otherwise j == 0 -> S column i, j == sNy-1 -> N column i
+  const size_t n_we = (size_t)nTiles * sNy * 4;
+  std::vector<int> tg(n_we + (size_t)nTiles * nip * 4, -1);
+  auto add_target = [&](int c, int target) -> bool {
     const int t = c / (sNy * sNx), rem = c - t * sNy * sNx, j = rem / sNx, i = rem - j * sNx;
-    size_t e;
-    if (i == 0) e = (size_t)t * njp + j;
-    else if (i == sNx - 1) e = (size_t)(nTiles + t) * njp + j;
-    else if (j == 0) e = (size_t)2 * nTiles * njp + (size_t)t * nip + i;
-    else if (j == sNy - 1) e = (size_t)2 * nTiles * njp + (size_t)(nTiles + t) * nip + i;
+    int* q;
+    if (i == 0) q = &tg[((size_t)t * sNy + j) * 4];
+    else if (i == sNx - 1) q = &tg[((size_t)t * sNy + j) * 4 + 2];
+    else if (j == 0) q = &tg[n_we + ((size_t)t * nip + i) * 2];
+    else if (j == sNy - 1) q = &tg[n_we + ((size_t)(nTiles + t) * nip + i) * 2];
     else return false;
-    int* q = &tg[e * 2];
-    if (q[0] < 0) q[0] = slot;
-    else if (q[1] < 0) q[1] = slot;
+    if (q[0] < 0) q[0] = target;
+    else if (q[1] < 0) q[1] = target;
     else return false;
     return true;
   };
   for (int t = 0; t < nTiles; ++t) {
     for (int k = 0; k < sNy; ++k) {
-      if (W[t * sNy + k] >= 0 && !add_target(W[t * sNy + k], t * njp + k)) return CG2D_BAD_ARG;
-      if (E[t * sNy + k] >= 0 && !add_target(E[t * sNy + k], (nTiles + t) * njp + k)) return CG2D_BAD_ARG;
+      if (W[t * sNy + k] >= 0 && !add_target(W[t * sNy + k], cell(t, k, -1))) return CG2D_BAD_ARG;
+      if (E[t * sNy + k] >= 0 && !add_target(E[t * sNy + k], cell(t, k, sNx))) return CG2D_BAD_ARG;
     }
     for (int k = 0; k < sNx; ++k) {
-      if (S[t * sNx + k] >= 0 && !add_target(S[t * sNx + k], 2 * nTiles * njp + t * nip + k)) return CG2D_BAD_ARG;
-      if (N[t * sNx + k] >= 0 && !add_target(N[t * sNx + k], 2 * nTiles * njp + (nTiles + t) * nip + k))
-        return CG2D_BAD_ARG;
+      if (S[t * sNx + k] >= 0 && !add_target(S[t * sNx + k], cell(t, -1, k))) return CG2D_BAD_ARG;
+      if (N[t * sNx + k] >= 0 && !add_target(N[t * sNx + k], cell(t, sNy, k))) return CG2D_BAD_ARG;
     }
   }
   cg2d_topology* tp = new cg2d_topology();
   tp->sNx = sNx; tp->sNy = sNy; tp->OLx = OLx; tp->OLy = OLy; tp->nTiles = nTiles;
-  tp->njp = njp; tp->nip = nip;
+  tp->nip = nip;
   tp->d_nbr = nullptr; tp->d_tg = nullptr; tp->d_src = nullptr; tp->d_comp = nullptr;
   cudaGetDevice(&tp->device);
   bool ok = cudaMalloc(&tp->d_nbr, nbr.size() * sizeof(int)) == cudaSuccess &&
@@ -386,12 +373,10 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
     d.op_base = op_base;
     d.rhs_base = rhs_base;
     d.pad_elems = (long long)d.tp.T * d.tp.npy * d.tp.npx;
-    d.ldv = L.ldv[g];
-    d.ldx = L.ldx[g];
-    d.ldc = L.ldc[g];
+    d.ldc = coef_pitch(d.tp.ni);
     d.a64[0] = G.aW2d; d.a64[1] = G.aS2d; d.a64[2] = G.aC2d;
     d.a64[3] = G.pW; d.a64[4] = G.pS; d.a64[5] = G.pC;
-    d.c32 = kp.mixed ? reinterpret_cast<float*>(ws + L.c32[g]) : nullptr;
+    d.cpk = ws + L.cpk[g];
     d.norm = G.cg2dNorm;
     d.norm_arr = G.cg2dNorm_per_instance;
     for (int s = 0; s < 2; ++s) {
@@ -407,18 +392,14 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
     d.vec = ws + L.vec[g];
     d.vec_stride = L.vec_stride[g];
     for (int v = 0; v < V_NVEC; ++v) d.vec_off[v] = L.vec_off[g][v];
-    d.halo = ws + L.halo[g];
-    d.halo_stride = L.halo_stride[g];
-    for (int v = 0; v < V_NVEC; ++v) d.halo_off[v] = L.halo_off[g][v];
     unit_base += G.count * d.units;
     op_base += G.count;
     rhs_base += G.count * G.nrhs;
   }
 
   if (cudaMemsetAsync(ws, 0, L.zero_end, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
-  if (kp.mixed)
-    for (int g = 0; g < ngroups; ++g)
-      if (launch_pack32(kp.g[g], stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  for (int g = 0; g < ngroups; ++g)
+    if (launch_pack_coef(kp.g[g], kp.mixed, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
 
   const size_t smem = L.smem;
   int bps = 0;

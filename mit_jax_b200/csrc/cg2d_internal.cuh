@@ -23,17 +23,30 @@ enum Pass : int { P_MAX = 0, P_INIT = 1, P_Z = 2, P_S = 3, P_X = 4, P_R = 5, P_N
 enum Act : int { A_NONE = 0, A_ACTIVE = 1, A_FIN = 2 };
 // per-solve scalar history: one slot per (kind, iteration), each written at most once
 enum Hist : int { H_RRX = 0, H_ETAX = 1, H_SQ = 2, H_RRR = 3, H_ETAZ = 4, H_SUM = 5, H_NKIND = 6 };
-// per-solve vectors (compact [T][nj][pitch]) and their halo slices
+// per-solve vectors, each [T][nj+2][P]: every tile row with its west and east neighbour cell, plus the south
+// and north neighbour rows (the tile's halo ring); see vec_pitch
 enum VecId : int { V_X = 0, V_R0 = 1, V_R1 = 2, V_S0 = 3, V_S1 = 4, V_Z = 5, V_Q = 6, V_NVEC = 7 };
+
+// Row pitch (elements) of every per-solve vector: the tile row plus its two neighbour cells, rounded up to 4
+// elements so that rows start 16-byte aligned for the bulk copies in FP32 and FP64 alike. One pitch for all
+// vectors lets one table of push targets serve every vector. Point (t, j, i), -1 <= j, i <= n, is element
+// (t (nj + 2) + j + 1) P + i + 1.
+__host__ __device__ inline int vec_pitch(int ni) { return (ni + 2 + 3) & ~3; }
+// Row pitch of the packed coefficient rows: columns i = 0 .. ni (the east face of the last point included).
+__host__ __device__ inline int coef_pitch(int ni) { return (ni + 1 + 3) & ~3; }
 
 // tables of one tile layout (device)
 struct TopoDev {
   const int* nbr;           // [4][T*len]: W (len nj), E (nj), S (ni), N (ni); compact source index or -1
-  const int* tg;            // push targets (pairs of halo slots, -1 = none): W, E [T][njp][2], S, N [T][nip][2]
+  // push targets: vector elements (halo-ring cells of other tiles) that take the value of a tile-edge point,
+  // -1 = none. WE [T][nj][4] (west-edge point of row j: 2 targets, east-edge point: 2 targets), then
+  // S [T][nip][2] and N [T][nip][2] by column. A point on two edges uses the W/E entry.
+  const int* tg;
   const int* map_src;       // full padded "T" map (src), for x_fortran halos and cg2d_exchange_scalar
   const int8_t* map_comp;
   int ni, nj, OLx, OLy, npx, npy, T;
-  int njp, nip;             // halo slice pitches: W/E slices [T][njp], S/N slices [T][nip]
+  int nip;                  // column pitch of the S/N target lists (even: 16-byte aligned per tile)
+  int P;                    // vec_pitch(ni)
 };
 
 struct GroupDev {
@@ -42,9 +55,11 @@ struct GroupDev {
   int nblk, units;          // work units (row blocks) per tile / per instance
   int unit_base, op_base, rhs_base;
   long long pad_elems;      // T*npy*npx
-  int ldv, ldx, ldc;        // row pitches (elements): V vectors, x (double), FP32 coefficient copies
+  int ldc;                  // coef_pitch(ni)
   const double* a64[6];     // aW2d, aS2d, aC2d, pW, pS, pC: [count][pad_elems]
-  float* c32;               // MIXED: [count][6][T][npy][ldc] float copies of a64
+  // packed coefficients [count][2 (A, M)][T][nj+1][3][ldc], FP32 in MIXED, FP64 otherwise: the rows a
+  // chunk needs are one contiguous block. A: aW2d, aS2d, aC2d; M: pW, pS, pC; row j, column i = point (j, i).
+  void* cpk;
   double norm;
   const double* norm_arr;   // nullable [count]
   const double* b[2];
@@ -57,9 +72,6 @@ struct GroupDev {
   char* vec;                // [count][nrhs] vector blocks
   long long vec_stride;     // bytes per vector block
   long long vec_off[V_NVEC];
-  char* halo;               // [count][nrhs] halo blocks (zeroed before the launch)
-  long long halo_stride;    // bytes per halo block
-  long long halo_off[V_NVEC];
 };
 
 struct KParams {
@@ -77,7 +89,7 @@ struct KParams {
   int part_units;
   unsigned* cnt;            // [total_ops] monotonic per-operator unit counters
   unsigned long long* rmax; // [total_rhs] max|b*cg2dNorm| as ordered bits
-  unsigned* gs;             // [0] grid barrier arrivals, [1] error word
+  unsigned* gs;             // [0] grid barrier arrivals, [1] error word, [2] where, [3] pass << 16 | CTA
   unsigned long long timeout_ns;
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
   unsigned long long* prof; // nullable: [1 + grid * 8] phase times (ns) per CTA
@@ -89,52 +101,48 @@ enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FI
 
 // Shared-memory image of one chunk for a pipelined pass (offsets in bytes from the stage buffer).
 struct StageLay {
-  unsigned coef, coef_stride;   // 3 coefficient arrays, (ch+1) padded rows each
-  int cpitch, csize;
+  int packed;                   // coefficients: 1 packed block (S, X, Z) or 3 FP64 arrays (R)
+  unsigned coef, coef_stride;   // R: the 3 arrays, (ch+1) padded rows each
+  int csize;
   int nvec;                     // stencil vectors per solve
-  unsigned vec[2][2], vstride[2];
-  int vpitch[2], vsize[2];
-  unsigned hw[2][2], he[2][2];  // west / east cross-tile neighbours of the chunk's rows
-  unsigned xo[2];               // P_S: own rows of x (double)
-  unsigned tw, te, ts, tn;      // push targets of the chunk's edge points (int2 per point)
+  unsigned vec[2][2];           // rows jc-1 .. jc+nr of each vector, pitch P
+  int vsize[2];
+  unsigned xo[2];               // P_S: own rows of x (double, pitch P)
+  unsigned twe, ts, tn;         // push targets of the chunk's edge points
   unsigned total;
 };
 
 __host__ __device__ inline unsigned al128(unsigned x) { return (x + 127u) & ~127u; }
 __host__ __device__ inline unsigned al16(unsigned x) { return (x + 15u) & ~15u; }
 
-__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int ni, int npx, int ldv,
-                                                 int ldx, int ldc) {
+__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int ni, int npx) {
   StageLay L;
+  const int P = vec_pitch(ni), ldc = coef_pitch(ni);
   unsigned o = 0;
-  const bool coef64 = (pt == P_R) || !mixed;
-  L.csize = coef64 ? 8 : 4;
-  L.cpitch = coef64 ? npx : ldc;
+  L.packed = pt != P_R;
   L.coef = o;
-  L.coef_stride = al128((unsigned)((ch + 1) * L.cpitch * L.csize));
-  o += 3 * L.coef_stride;
+  if (L.packed) {
+    L.csize = mixed ? 4 : 8;
+    L.coef_stride = al128((unsigned)((ch + 1) * 3 * ldc * L.csize));
+    o += L.coef_stride;
+  } else {
+    L.csize = 8;
+    L.coef_stride = al128((unsigned)((ch + 1) * npx * 8));
+    o += 3 * L.coef_stride;
+  }
   L.nvec = (pt == P_Z) ? 1 : 2;
   const int vs = mixed ? 4 : 8;
-  for (int v = 0; v < 2; ++v) {
-    L.vsize[v] = (pt == P_R && v == 0) ? 8 : vs;
-    L.vpitch[v] = (L.vsize[v] == 8) ? ldx : ldv;
-    L.vstride[v] = al128((unsigned)((ch + 2) * L.vpitch[v] * L.vsize[v]));
-  }
+  for (int v = 0; v < 2; ++v) L.vsize[v] = (pt == P_R && v == 0) ? 8 : vs;
   for (int s = 0; s < 2; ++s)
     for (int v = 0; v < 2; ++v) {
-      L.vec[s][v] = L.hw[s][v] = L.he[s][v] = 0;
-      if (s < nrhs && v < L.nvec) {
-        L.vec[s][v] = o; o += L.vstride[v];
-        L.hw[s][v] = o; o += al128(al16((unsigned)(ch * L.vsize[v])));
-        L.he[s][v] = o; o += al128(al16((unsigned)(ch * L.vsize[v])));
-      }
+      L.vec[s][v] = 0;
+      if (s < nrhs && v < L.nvec) { L.vec[s][v] = o; o += al128((unsigned)((ch + 2) * P * L.vsize[v])); }
     }
   for (int s = 0; s < 2; ++s) {
     L.xo[s] = 0;
-    if (pt == P_S && s < nrhs) { L.xo[s] = o; o += al128((unsigned)(ch * ldx * 8)); }
+    if (pt == P_S && s < nrhs) { L.xo[s] = o; o += al128((unsigned)(ch * P * 8)); }
   }
-  L.tw = o; o += al128(al16((unsigned)(ch * 8)));
-  L.te = o; o += al128(al16((unsigned)(ch * 8)));
+  L.twe = o; o += al128((unsigned)(ch * 16));
   L.ts = o; o += al128(al16((unsigned)(ni * 8)));
   L.tn = o; o += al128(al16((unsigned)(ni * 8)));
   L.total = al128(o);
@@ -145,7 +153,7 @@ __host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int 
 size_t fixed_smem_bytes(int max_ni, int serial);
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream);
 cudaError_t solver_occupancy(int mixed, size_t smem, int* blocks_per_sm);
-cudaError_t launch_pack32(const GroupDev& g, cudaStream_t stream);
+cudaError_t launch_pack_coef(const GroupDev& g, int mixed, cudaStream_t stream);
 cudaError_t launch_apply_operator(const TopoDev& tp, int batch, double norm, const double* aW, const double* aS,
                                   const double* aC, const double* v, double* out, cudaStream_t stream);
 cudaError_t launch_edge_products(const TopoDev& tp, int batch, double norm, const double* norm_arr,

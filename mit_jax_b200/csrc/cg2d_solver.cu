@@ -9,17 +9,18 @@
 // Data movement per iteration k (per solve), two grid-wide waits:
 //   pass S_k : s_k = z_k + beta_k s_{k-1};  q_k = A s_k;  x_k = x_{k-1} + alpha_{k-1} s_{k-1};  sum s_k.q_k
 //   pass X_k : r_{k+1} = r_k - alpha_k q_k;  z_{k+1} = M r_{k+1};  sums r.r and z.r
-// Work is cut into chunks of up to 8 rows of one tile. For every chunk one thread issues bulk
-// asynchronous copies (cp.async.bulk, completion counted on an mbarrier) of the coefficient rows,
-// the vector rows j-1 .. j+8 and the chunk's cross-tile neighbours into shared memory; the next
-// chunk's copies are in flight while the current one is computed (two stage buffers). Values at the
-// four neighbours of a point are formed in shared memory exactly as their owner forms them (a
-// neighbour's s_k from its z_k and s_{k-1}, its r_{k+1} from r_k and q_k), so no exchange step and no
-// extra wait is needed. Cross-tile neighbours -- the exch2 halo of cg2d.py:228,235,250,260 -- are
-// pushed by the owner of each tile-edge point into per-tile halo slices whenever it writes the
-// value, so a chunk's halo is as contiguous as its rows. The x update is deferred by one pass (it
-// needs s_{k-1}, which pass S_k reads anyway); its arithmetic is the reference's x + alpha * s
-// (cg2d.py:254).
+// Work is cut into chunks of up to 8 rows of one tile. For every chunk the lanes of warp 0 issue
+// bulk asynchronous copies (cp.async.bulk, completion counted on an mbarrier) into shared memory:
+// one for the packed coefficient rows, one per vector (rows j-1 .. j+8 with their neighbour cells)
+// and the push targets of the chunk's edge points; the next chunk's copies are in flight while the
+// current one is computed (two stage buffers). Values at the four neighbours of a point are formed
+// in shared memory exactly as their owner forms them (a neighbour's s_k from its z_k and s_{k-1},
+// its r_{k+1} from r_k and q_k), so no exchange step and no extra wait is needed. Every vector tile
+// is stored with its halo ring (one cell on each side); cross-tile neighbours -- the exch2 halo of
+// cg2d.py:228,235,250,260 -- are pushed by the owner of each tile-edge point into the rings of the
+// tiles that read it whenever it writes the value, so the stencil needs no edge cases. The x update
+// is deferred by one pass (it needs s_{k-1}, which pass S_k reads anyway); its arithmetic is the
+// reference's x + alpha * s (cg2d.py:254).
 //
 // MIXED precision keeps r, s, z, q and the operator copies in FP32 (FP32 stencils), x and all dot
 // products in FP64, and replaces r by the FP64 true residual b - A x every replace_every iterations
@@ -256,44 +257,46 @@ __device__ __forceinline__ double* hist_ptr(const KParams& kp, int rid, int kind
   return kp.hist + ((size_t)rid * H_NKIND + kind) * (size_t)kp.hist_len + idx;
 }
 
+// a solve's vector (ringed tiles, [T][nj+2][P])
 template <class T>
 __device__ __forceinline__ T* vec_ptr(const GroupDev& g, int inst, int slot, int which) {
   return reinterpret_cast<T*>(g.vec + (long long)(inst * g.nrhs + slot) * g.vec_stride + g.vec_off[which]);
 }
-template <class T>
-__device__ __forceinline__ T* halo_ptr(const GroupDev& g, int inst, int slot, int which) {
-  return reinterpret_cast<T*>(g.halo + (long long)(inst * g.nrhs + slot) * g.halo_stride + g.halo_off[which]);
+// element of point (t, j, i) in a ringed vector; -1 <= j <= nj, -1 <= i <= ni
+__device__ __forceinline__ long long vidx(const TopoDev& tp, int t, int j, int i) {
+  return ((long long)t * (tp.nj + 2) + j + 1) * tp.P + i + 1;
 }
 
-// store the value of point (t, j, i) into the halo slices of the tiles that read it across an edge
+// store the value of point (t, j, i) into the ring cells of the tiles that read it across an edge
 template <class T>
-__device__ __forceinline__ void push(const TopoDev& tp, T* halo, int t, int j, int i, T v) {
-  size_t e;
-  if (i == 0) e = (size_t)t * tp.njp + j;
-  else if (i == tp.ni - 1) e = (size_t)(tp.T + t) * tp.njp + j;
-  else if (j == 0) e = (size_t)2 * tp.T * tp.njp + (size_t)t * tp.nip + i;
-  else if (j == tp.nj - 1) e = (size_t)2 * tp.T * tp.njp + (size_t)(tp.T + t) * tp.nip + i;
+__device__ __forceinline__ void push(const TopoDev& tp, T* vec, int t, int j, int i, T v) {
+  const int* e;
+  if (i == 0) e = tp.tg + ((size_t)t * tp.nj + j) * 4;
+  else if (i == tp.ni - 1) e = tp.tg + ((size_t)t * tp.nj + j) * 4 + 2;
+  else if (j == 0) e = tp.tg + (size_t)tp.T * tp.nj * 4 + ((size_t)t * tp.nip + i) * 2;
+  else if (j == tp.nj - 1) e = tp.tg + (size_t)tp.T * tp.nj * 4 + ((size_t)(tp.T + t) * tp.nip + i) * 2;
   else return;
-  const int s0 = __ldg(tp.tg + 2 * e), s1 = __ldg(tp.tg + 2 * e + 1);
-  if (s0 >= 0) stcg(halo + s0, v);
-  if (s1 >= 0) stcg(halo + s1, v);
+  const int s0 = __ldg(e), s1 = __ldg(e + 1);
+  if (s0 >= 0) stcg(vec + s0, v);
+  if (s1 >= 0) stcg(vec + s1, v);
 }
 
 // the same with the chunk's target lists staged in shared memory (row w of the chunk = tile row j)
 struct PushTab {
-  const int2 *tw, *te, *ts, *tn;
+  const int4* twe;
+  const int2 *ts, *tn;
   int ni, nj;
 };
 template <class T>
-__device__ __forceinline__ void push_s(const PushTab& pt, T* halo, int j, int w, int i, T v) {
-  int2 e;
-  if (i == 0) e = pt.tw[w];
-  else if (i == pt.ni - 1) e = pt.te[w];
-  else if (j == 0) e = pt.ts[i];
-  else if (j == pt.nj - 1) e = pt.tn[i];
+__device__ __forceinline__ void push_s(const PushTab& pt, T* vec, int j, int w, int i, T v) {
+  int a, b;
+  if (i == 0) { const int4 e = pt.twe[w]; a = e.x; b = e.y; }
+  else if (i == pt.ni - 1) { const int4 e = pt.twe[w]; a = e.z; b = e.w; }
+  else if (j == 0) { const int2 e = pt.ts[i]; a = e.x; b = e.y; }
+  else if (j == pt.nj - 1) { const int2 e = pt.tn[i]; a = e.x; b = e.y; }
   else return;
-  if (e.x >= 0) stcg(halo + e.x, v);
-  if (e.y >= 0) stcg(halo + e.y, v);
+  if (a >= 0) stcg(vec + a, v);
+  if (b >= 0) stcg(vec + b, v);
 }
 
 // compact index -> padded index of the same point
@@ -373,23 +376,31 @@ __device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, con
   }
 }
 
-// thread 0: add the chunk's rows (ROWBLOCK: row sums in order; FORTRAN: every product in j, i order)
+// warp 0: add the chunk's rows into the unit's partial sums, lane l < 4 owning sum (slot l >> 1, kind l & 1)
+// (ROWBLOCK: row sums in row order; FORTRAN: every product in j, i order). Ends with the warp converged, so
+// thread 0 may read the partials.
 __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupDev& g, int ns0, int ns1, int nr,
                                                  const Smem& sm) {
-  for (int s = 0; s < 2; ++s) {
-    const int ns = s == 0 ? ns0 : ns1;
-    for (int q = 0; q < ns; ++q) {
-      double a = sm.uacc[s * 2 + q];
-      if (kp.serial) {
-        const double* pr = sm.prod + ((s * 2 + q) * kWarps) * kp.max_ni;
-        for (int w = 0; w < nr; ++w)
-          for (int i = 0; i < g.tp.ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
-      } else {
-        for (int w = 0; w < nr; ++w) a = add(a, sm.rowsum[(s * 2 + q) * kWarps + w]);
-      }
-      sm.uacc[s * 2 + q] = a;
+  const int lane = threadIdx.x & 31;
+  const int s = lane >> 1, q = lane & 1;
+  if (lane < 4 && q < (s == 0 ? ns0 : ns1)) {
+    double a = sm.uacc[lane];
+    if (kp.serial) {
+      const double* pr = sm.prod + (lane * kWarps) * kp.max_ni;
+      for (int w = 0; w < nr; ++w)
+        for (int i = 0; i < g.tp.ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
+    } else {
+      const double* rs = sm.rowsum + lane * kWarps;
+      double v[kWarps];
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) v[w] = rs[w];
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w)
+        if (w < nr) a = add(a, v[w]);
     }
+    sm.uacc[lane] = a;
   }
+  __syncwarp();
 }
 
 // thread 0 writes the unit's partials (no wait) and counts the unit in shared memory; the counts are published
@@ -530,6 +541,27 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
   if (tid == 0) sm.uacc[0] = sm.uacc[1] = sm.uacc[2] = sm.uacc[3] = 0.0;
   unsigned long long vmax0 = 0ull, vmax1 = 0ull;
 
+  if (pt == P_MAX) {
+    // ring cells of r, s, z and q read 0 unless a neighbour pushes a value into them (the exchange leaves
+    // unwritten halo points as they are, and the reference's r, s, z, q start with zero halos): zero the
+    // west and east cells of the unit's rows, and the south / north rows at the tile's edges. Pushes come
+    // after the next grid-wide wait.
+    const int P = tp.P;
+    const int nrow = j1 - j0;
+    const int n_we = 2 * nrow, n_s = (j0 == 0) ? P : 0, n_n = (j1 == nj) ? P : 0;
+    const int per = n_we + n_s + n_n;
+    for (int idx = tid; idx < per * g.nrhs * (V_NVEC - 1); idx += kThreads) {
+      const int sv = idx / per, e = idx - (idx / per) * per;
+      const int s = sv / (V_NVEC - 1), v = 1 + sv - (sv / (V_NVEC - 1)) * (V_NVEC - 1);
+      V* vb = vec_ptr<V>(g, inst, s, v);
+      long long o;
+      if (e < n_we) o = vidx(tp, t, j0 + (e >> 1), (e & 1) ? ni : -1);
+      else if (e < n_we + n_s) o = ((long long)t * (nj + 2)) * P + (e - n_we);
+      else o = ((long long)t * (nj + 2) + nj + 1) * P + (e - n_we - n_s);
+      vb[o] = (V)0;
+    }
+  }
+
   for (int jc = j0; jc < j1; jc += kWarps) {
     const int nr = min(kWarps, j1 - jc);
     if (pt == P_INIT) {
@@ -580,14 +612,16 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
             const double* st = stage + s * SW;
             const int sc = (warp + 1) * W + (i + 1);
             const double vc = st[sc], vw = st[sc - 1], ve = st[sc + 1], vs = st[sc - W], vn = st[sc + W];
-            stcg(vec_ptr<double>(g, inst, s, V_X) + (t * nj + j) * g.ldx + i, vc);
+            const long long vo = vidx(tp, t, j, i);
+            stcg(vec_ptr<double>(g, inst, s, V_X) + vo, vc);
             const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), si.norm(s)), si.rnorm(s));   // cg2d.py:221,226
             const double ax = op_A<double>(__ldg(aW + po), __ldg(aW + po + 1), __ldg(aS + po), __ldg(aS + po + npx),
                                            __ldg(aC + po), vw, ve, vs, vn, vc);
             const V r0 = (V)sub(bn, ax);                                                   // cg2d.py:232
-            stcg(vec_ptr<V>(g, inst, s, V_R0) + (t * nj + j) * g.ldv + i, r0);
-            push(tp, halo_ptr<V>(g, inst, s, V_R0), t, j, i, r0);
-            stcg(vec_ptr<V>(g, inst, s, V_S1) + (t * nj + j) * g.ldv + i, (V)0);         // s = 0 (cg2d.py:231)
+            V* rv = vec_ptr<V>(g, inst, s, V_R0);
+            stcg(rv + vo, r0);
+            push(tp, rv, t, j, i, r0);
+            stcg(vec_ptr<V>(g, inst, s, V_S1) + vo, (V)0);                               // s = 0 (cg2d.py:231)
             p0 = mul((double)r0, (double)r0);
             p1 = bn;
           }
@@ -623,7 +657,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
       continue;
     }
     __syncthreads();
-    if (tid == 0) accumulate_chunk(kp, g, ns0, ns1, nr, sm);
+    if (tid < 32) accumulate_chunk(kp, g, ns0, ns1, nr, sm);
   }
   if (pt == P_MAX) return;
   finish_unit(kp, g, inst, lu, ns0, ns1, sm);
@@ -647,41 +681,40 @@ __device__ bool run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
   return ok;
 }
 
-// x halo slices at the start: the exchanged normalised first guess; unwritten points keep cg2d_x
+// x ring cells at the start: the exchanged normalised first guess; unwritten points keep cg2d_x
 // (cg2d.py:227-228). Later values are pushed by the owners as x is updated.
-__device__ void init_x_halo(const KParams& kp, const Smem& sm) {
+__device__ void init_x_ring(const KParams& kp, const Smem& sm) {
   const long long gstride = (long long)gridDim.x * kThreads;
   for (int gg = 0; gg < kp.ngroups; ++gg) {
     const GroupDev& g = kp.g[gg];
     const TopoDev& tp = g.tp;
-    const long long per = (long long)tp.T * (2 * tp.njp + 2 * tp.nip);
+    const int T = tp.T, nj = tp.nj, ni = tp.ni;
+    const long long per = (long long)T * (2 * nj + 2 * ni);   // W, E [T][nj], S, N [T][ni]
     const long long tot = per * g.count * g.nrhs;
     for (long long idx = (long long)blockIdx.x * kThreads + threadIdx.x; idx < tot; idx += gstride) {
       const long long ins_slot = idx / per;
       const int h = (int)(idx - ins_slot * per);
       const int inst = (int)(ins_slot / g.nrhs), s = (int)(ins_slot - (long long)inst * g.nrhs);
-      int t, kk, j, i, src;
-      if (h < 2 * tp.T * tp.njp) {
-        const int side = h / (tp.T * tp.njp);
-        const int r = h - side * tp.T * tp.njp;
-        t = r / tp.njp; kk = r - t * tp.njp;
-        if (kk >= tp.nj) continue;
-        j = kk; i = side == 0 ? -1 : tp.ni;
-        src = tp.nbr[side * tp.T * tp.nj + t * tp.nj + kk];
+      int t, j, i, src;
+      if (h < 2 * T * nj) {
+        const int side = h / (T * nj);
+        const int r = h - side * T * nj;
+        t = r / nj; j = r - t * nj;
+        i = side == 0 ? -1 : ni;
+        src = tp.nbr[side * T * nj + r];
       } else {
-        const int h2 = h - 2 * tp.T * tp.njp;
-        const int side = h2 / (tp.T * tp.nip);
-        const int r = h2 - side * tp.T * tp.nip;
-        t = r / tp.nip; kk = r - t * tp.nip;
-        if (kk >= tp.ni) continue;
-        i = kk; j = side == 0 ? -1 : tp.nj;
-        src = tp.nbr[2 * tp.T * tp.nj + side * tp.T * tp.ni + t * tp.ni + kk];
+        const int h2 = h - 2 * T * nj;
+        const int side = h2 / (T * ni);
+        const int r = h2 - side * T * ni;
+        t = r / ni; i = r - t * ni;
+        j = side == 0 ? -1 : nj;
+        src = tp.nbr[2 * T * nj + side * T * ni + r];
       }
       const double* x0 = g.x0[s] + inst * g.pad_elems;
       const double rn = sm.rnorm[g.rhs_base + inst * g.nrhs + s];
       const double v = (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), rn)
                                   : __ldg(x0 + ((long long)t * tp.npy + (j + tp.OLy)) * tp.npx + (i + tp.OLx));
-      halo_ptr<double>(g, inst, s, V_X)[h] = v;
+      vec_ptr<double>(g, inst, s, V_X)[vidx(tp, t, j, i)] = v;
     }
   }
 }
@@ -722,89 +755,74 @@ __device__ bool chunk_next(const KParams& kp, const Smem& sm, Chunk& c) {
   return chunk_unit(kp, sm, c.u + gridDim.x, c);
 }
 
-// the vectors a pass stages (with their neighbours) for an active solve
-__device__ __forceinline__ void pass_vectors(int pt, int k, int hidx, int (&ids)[2]) {
-  if (pt == P_S) { ids[0] = V_Z; ids[1] = ((k + 1) & 1) ? V_S1 : V_S0; }
-  else if (pt == P_X) { ids[0] = (k & 1) ? V_R1 : V_R0; ids[1] = V_Q; }
-  else if (pt == P_R) { ids[0] = V_X; ids[1] = (k & 1) ? V_S1 : V_S0; }
-  else { ids[0] = (hidx & 1) ? V_R1 : V_R0; ids[1] = -1; }
+// the vector a pass stages as stencil input v (0, 1) of a solve
+__device__ __forceinline__ int pass_vector(int pt, int k, int hidx, int v) {
+  if (pt == P_S) return v == 0 ? V_Z : (((k + 1) & 1) ? V_S1 : V_S0);
+  if (pt == P_X) return v == 0 ? ((k & 1) ? V_R1 : V_R0) : V_Q;
+  if (pt == P_R) return v == 0 ? V_X : ((k & 1) ? V_S1 : V_S0);
+  return (hidx & 1) ? V_R1 : V_R0;
 }
 
 // warp 0: bulk copies of chunk c into the stage buffer sb, completion on bar. Each lane owns one fixed copy
-// (a lane whose copy is not needed moves 0 bytes): lanes 0-2 the coefficient rows, 3-6 the push targets
-// (W, E, S, N), 7 + 5 (2 s + v) + piece the vector pieces of slot s, vector v (rows, west and east neighbours,
-// south and north halo rows), 27 + s the own rows of x (pass S).
+// (a lane whose copy is not needed moves 0 bytes): lane 0 the packed coefficient rows (pass R: lanes 0-2
+// the three FP64 operator arrays), 3 the west/east push targets of the chunk's rows, 4 and 5 the south /
+// north push targets (first / last chunk of a tile), 6 + 2 s + v vector v of slot s (rows jc-1 .. jc+nr,
+// ring cells included), 10 + s the own rows of x (pass S).
 template <bool MIXED>
 __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, int hidx, const Smem& sm,
                             unsigned char* sb, unsigned long long* bar) {
   const GroupDev& g = kp.g[c.gi];
   const TopoDev& tp = g.tp;
   const int lane = threadIdx.x & 31;
-  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx, g.ldv, g.ldx, g.ldc);
+  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx);
   const int rid0 = g.rhs_base + c.inst * g.nrhs;
   const bool act0 = sm.act[rid0] == A_ACTIVE;
   const bool act1 = g.nrhs > 1 && sm.act[rid0 + 1] == A_ACTIVE;
   const bool any = act0 || act1;
-  const int T = tp.T, nj = tp.nj, ni = tp.ni, njp = tp.njp, nip = tp.nip;
+  const int T = tp.T, nj = tp.nj, ni = tp.ni, P = tp.P;
   const bool bottom = c.jc == 0, top = c.jc + c.nr == nj;
   void* dst = nullptr;
   const void* src = nullptr;
   unsigned bytes = 0;
   if (lane < 3) {
-    if (any) {
-      const int first = (pt == P_X || pt == P_Z) ? 3 : 0;   // M = (pW, pS, pC) or A = (aW2d, aS2d, aC2d)
-      if (L.csize == 8)
-        src = g.a64[first + lane] + (long long)c.inst * g.pad_elems + ((long long)c.t * tp.npy + c.jc + tp.OLy) * tp.npx;
-      else
-        src = g.c32 + (((long long)c.inst * 6 + first + lane) * T * tp.npy + (long long)c.t * tp.npy + c.jc + tp.OLy) *
-                          g.ldc;
+    if (any && L.packed && lane == 0) {
+      const int op = (pt == P_X || pt == P_Z) ? 1 : 0;   // M = (pW, pS, pC) or A = (aW2d, aS2d, aC2d)
+      const long long row = ((long long)(c.inst * 2 + op) * T + c.t) * (nj + 1) + c.jc;
+      src = static_cast<const char*>(g.cpk) + row * 3 * g.ldc * L.csize;
+      dst = sb + L.coef;
+      bytes = (unsigned)((c.nr + 1) * 3 * g.ldc * L.csize);
+    } else if (any && !L.packed) {
+      src = g.a64[lane] + (long long)c.inst * g.pad_elems + ((long long)c.t * tp.npy + c.jc + tp.OLy) * tp.npx;
       dst = sb + L.coef + lane * L.coef_stride;
-      bytes = (unsigned)((c.nr + 1) * L.cpitch * L.csize);
+      bytes = (unsigned)((c.nr + 1) * tp.npx * 8);
     }
-  } else if (lane < 7) {
-    const int side = lane - 3;   // W, E, S, N push-target slices
-    if (any && (side < 2 || (side == 2 && bottom) || (side == 3 && top))) {
-      long long e;
-      if (side < 2) e = (long long)(side * T + c.t) * njp + c.jc;
-      else e = (long long)2 * T * njp + (long long)((side - 2) * T + c.t) * nip;
-      src = tp.tg + 2 * e;
-      dst = sb + (side == 0 ? L.tw : side == 1 ? L.te : side == 2 ? L.ts : L.tn);
-      bytes = side < 2 ? al16((unsigned)(c.nr * 8)) : al16((unsigned)(ni * 8));
-    }
-  } else if (lane < 27) {
-    const int q = lane - 7, sv = q / 5, piece = q - sv * 5;
-    const int s = sv >> 1, v = sv & 1;
-    if (s < g.nrhs && (s == 0 ? act0 : act1) && v < L.nvec) {
-      int id;
-      if (pt == P_S) id = v == 0 ? V_Z : (((k + 1) & 1) ? V_S1 : V_S0);
-      else if (pt == P_X) id = v == 0 ? ((k & 1) ? V_R1 : V_R0) : V_Q;
-      else if (pt == P_R) id = v == 0 ? V_X : ((k & 1) ? V_S1 : V_S0);
-      else id = (hidx & 1) ? V_R1 : V_R0;
-      const int sz = L.vsize[v], P = L.vpitch[v];
-      const char* vb = vec_ptr<const char>(g, c.inst, s, id);
-      const char* hb = halo_ptr<const char>(g, c.inst, s, id);
-      const unsigned char* vd = sb + L.vec[s][v];
-      if (piece == 0) {
-        const int jlo = max(c.jc - 1, 0), jhi = min(c.jc + c.nr, nj - 1);
-        src = vb + (long long)(c.t * nj + jlo) * P * sz;
-        dst = const_cast<unsigned char*>(vd) + (jlo - c.jc + 1) * P * sz;
-        bytes = (unsigned)((jhi - jlo + 1) * P * sz);
-      } else if (piece <= 2) {
-        src = hb + ((long long)((piece - 1) * T + c.t) * njp + c.jc) * sz;
-        dst = sb + (piece == 1 ? L.hw[s][v] : L.he[s][v]);
-        bytes = al16((unsigned)(c.nr * sz));
-      } else if ((piece == 3 && bottom) || (piece == 4 && top)) {
-        src = hb + ((long long)2 * T * njp + (long long)((piece - 3) * T + c.t) * nip) * sz;
-        dst = const_cast<unsigned char*>(vd) + (piece == 3 ? 0 : (c.nr + 1) * P * sz);
-        bytes = al16((unsigned)(ni * sz));
+  } else if (lane < 6) {
+    if (any) {
+      if (lane == 3) {
+        src = tp.tg + ((long long)c.t * nj + c.jc) * 4;
+        dst = sb + L.twe;
+        bytes = (unsigned)(c.nr * 16);
+      } else if ((lane == 4 && bottom) || (lane == 5 && top)) {
+        src = tp.tg + (long long)T * nj * 4 + ((long long)((lane - 4) * T + c.t) * tp.nip) * 2;
+        dst = sb + (lane == 4 ? L.ts : L.tn);
+        bytes = al16((unsigned)(ni * 8));
       }
     }
-  } else if (lane < 29) {
-    const int s = lane - 27;
+  } else if (lane < 10) {
+    const int s = (lane - 6) >> 1, v = (lane - 6) & 1;
+    if (s < g.nrhs && (s == 0 ? act0 : act1) && v < L.nvec) {
+      const int sz = L.vsize[v];
+      src = vec_ptr<const char>(g, c.inst, s, pass_vector(pt, k, hidx, v)) +
+            ((long long)c.t * (nj + 2) + c.jc) * P * sz;
+      dst = sb + L.vec[s][v];
+      bytes = (unsigned)((c.nr + 2) * P * sz);
+    }
+  } else if (lane < 12) {
+    const int s = lane - 10;
     if (pt == P_S && s < g.nrhs && (s == 0 ? act0 : act1) && sm.has_alpha[rid0 + s]) {
-      src = vec_ptr<const char>(g, c.inst, s, V_X) + (long long)(c.t * nj + c.jc) * g.ldx * 8;
+      src = vec_ptr<const char>(g, c.inst, s, V_X) + ((long long)c.t * (nj + 2) + c.jc + 1) * P * 8;
       dst = sb + L.xo[s];
-      bytes = (unsigned)(c.nr * g.ldx * 8);
+      bytes = (unsigned)(c.nr * P * 8);
     }
   }
   const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
@@ -813,7 +831,9 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
   if (bytes) bulk_g2s(dst, src, bytes, bar);
 }
 
-// compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m
+// compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m. In shared memory
+// point (w, i) of a vector is element (w + 1) P + i + 1 (its neighbours at -1, +1, -P, +P) and of the packed
+// coefficients element w 3 ldc + i (columns: W/pW, +ldc S/pS, +2 ldc C/pC; east face +1, north face +3 ldc).
 template <bool MIXED>
 __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si,
                                const unsigned char* sb, const Smem& sm) {
@@ -824,15 +844,14 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   const TopoDev& tp = g.tp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp >= c.nr) return lp;
-  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx, g.ldv, g.ldx, g.ldc);
+  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx);
   const int ni = tp.ni, nj = tp.nj, t = c.t, w = warp, j = c.jc + w;
-  const int CP = L.cpitch, col0 = tp.OLx;
-  const int crv = (t * nj + j) * g.ldv, crx = (t * nj + j) * g.ldx;
+  const int P = tp.P, CL = g.ldc, CR = 3 * g.ldc;
+  const long long grow = ((long long)t * (nj + 2) + j + 1) * P + 1;   // element of (t, j, 0)
   const long long pe = g.pad_elems;
   const long long prow = (long long)c.inst * pe + ((long long)t * tp.npy + j + tp.OLy) * tp.npx + tp.OLx;
   PushTab ptab;
-  ptab.tw = reinterpret_cast<const int2*>(sb + L.tw);
-  ptab.te = reinterpret_cast<const int2*>(sb + L.te);
+  ptab.twe = reinterpret_cast<const int4*>(sb + L.twe);
   ptab.ts = reinterpret_cast<const int2*>(sb + L.ts);
   ptab.tn = reinterpret_cast<const int2*>(sb + L.tn);
   ptab.ni = ni;
@@ -860,143 +879,111 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
       const double* x = vec_ptr<double>(g, c.inst, s, V_X);
       for (int i = lane; i < ni; i += 32) {
-        double xv = ldcg(x + crx + i);
-        if (si.has_alpha(s)) xv = add(xv, mul(si.c2(s), (double)ldcg(so + crv + i)));
+        double xv = ldcg(x + grow + i);
+        if (si.has_alpha(s)) xv = add(xv, mul(si.c2(s), (double)ldcg(so + grow + i)));
         const double xf = __ddiv_rn(xv, si.rnorm(s));
         g.x_out[s][prow + i] = xf;
         if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
       }
       continue;
     }
-    const unsigned char* cb = sb + L.coef;
+    const int cb0 = w * CR;
     if (pt == P_S) {
       const V* zr = reinterpret_cast<const V*>(sb + L.vec[s][0]);
       const V* so = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      const V* hwz = reinterpret_cast<const V*>(sb + L.hw[s][0]);
-      const V* hws = reinterpret_cast<const V*>(sb + L.hw[s][1]);
-      const V* hez = reinterpret_cast<const V*>(sb + L.he[s][0]);
-      const V* hes = reinterpret_cast<const V*>(sb + L.he[s][1]);
       const double* xo = reinterpret_cast<const double*>(sb + L.xo[s]);
-      const C* cw = reinterpret_cast<const C*>(cb);
-      const C* cs = reinterpret_cast<const C*>(cb + L.coef_stride);
-      const C* cc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
-      const int P = L.vpitch[0];
+      const C* cp = reinterpret_cast<const C*>(sb + L.coef);
       const double beta = si.c1(s), alpha_prev = si.c2(s);
       const bool upd = si.has_alpha(s) != 0;
       V* s_out = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
-      V* s_halo = halo_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
       V* q_out = vec_ptr<V>(g, c.inst, s, V_Q);
-      V* q_halo = halo_ptr<V>(g, c.inst, s, V_Q);
       double* x_out = vec_ptr<double>(g, c.inst, s, V_X);
-      double* x_halo = halo_ptr<double>(g, c.inst, s, V_X);
       // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike (MIXED: in FP32)
       const V betav = (V)beta;
       auto sn = [&](V zz, V ss) -> V { return add(zz, mul(betav, ss)); };
       for (int i = lane; i < ni; i += 32) {
-        const int rc = (w + 1) * P + i;
+        const int rc = (w + 1) * P + i + 1;
         const V vc = sn(zr[rc], so[rc]);
-        const V vw = (i > 0) ? sn(zr[rc - 1], so[rc - 1]) : sn(hwz[w], hws[w]);
-        const V ve = (i < ni - 1) ? sn(zr[rc + 1], so[rc + 1]) : sn(hez[w], hes[w]);
+        const V vw = sn(zr[rc - 1], so[rc - 1]);
+        const V ve = sn(zr[rc + 1], so[rc + 1]);
         const V vs = sn(zr[rc - P], so[rc - P]);
         const V vn = sn(zr[rc + P], so[rc + P]);
-        const int cr = w * CP + col0 + i;
-        const V q = (V)op_A<C>(cw[cr], cw[cr + 1], cs[cr], cs[cr + CP], cc[cr], (C)vw, (C)ve, (C)vs, (C)vn,
-                               (C)vc);                                                        // cg2d.py:251
-        stcg(s_out + crv + i, vc);
-        push_s(ptab, s_halo, j, w, i, vc);
-        stcg(q_out + crv + i, q);
-        push_s(ptab, q_halo, j, w, i, q);
+        const int cr = cb0 + i;
+        const V q = (V)op_A<C>(cp[cr], cp[cr + 1], cp[cr + CL], cp[cr + CL + CR], cp[cr + 2 * CL], (C)vw, (C)ve,
+                               (C)vs, (C)vn, (C)vc);                                          // cg2d.py:251
+        stcg(s_out + grow + i, vc);
+        push_s(ptab, s_out, j, w, i, vc);
+        stcg(q_out + grow + i, q);
+        push_s(ptab, q_out, j, w, i, q);
         if (upd) {
-          const double xn = add(xo[w * g.ldx + i], mul(alpha_prev, (double)so[rc]));         // cg2d.py:254
-          stcg(x_out + crx + i, xn);
-          push_s(ptab, x_halo, j, w, i, xn);
+          const double xn = add(xo[w * P + i + 1], mul(alpha_prev, (double)so[rc]));          // cg2d.py:254
+          stcg(x_out + grow + i, xn);
+          if (MIXED) push_s(ptab, x_out, j, w, i, xn);   // x's neighbours are read by the replacement pass only
         }
         emit(s, i, mul((double)vc, (double)q), 0.0);                                          // cg2d.py:252
       }
     } else if (pt == P_X) {
       const V* ro = reinterpret_cast<const V*>(sb + L.vec[s][0]);
       const V* qv = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      const V* hwr = reinterpret_cast<const V*>(sb + L.hw[s][0]);
-      const V* hwq = reinterpret_cast<const V*>(sb + L.hw[s][1]);
-      const V* her = reinterpret_cast<const V*>(sb + L.he[s][0]);
-      const V* heq = reinterpret_cast<const V*>(sb + L.he[s][1]);
-      const C* pw = reinterpret_cast<const C*>(cb);
-      const C* ps = reinterpret_cast<const C*>(cb + L.coef_stride);
-      const C* pc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
-      const int P = L.vpitch[0];
+      const C* cp = reinterpret_cast<const C*>(sb + L.coef);
       const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
-      V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
-      V* z_halo = halo_ptr<V>(g, c.inst, s, V_Z);
       // r_{k+1} = r_k - alpha_k q_k (cg2d.py:255) (MIXED: in FP32)
       const V alphav = (V)alpha;
       auto rn = [&](V rr, V qq) -> V { return sub(rr, mul(alphav, qq)); };
       for (int i = lane; i < ni; i += 32) {
-        const int rc = (w + 1) * P + i;
+        const int rc = (w + 1) * P + i + 1;
         const V vc = rn(ro[rc], qv[rc]);
-        const V vw = (i > 0) ? rn(ro[rc - 1], qv[rc - 1]) : rn(hwr[w], hwq[w]);
-        const V ve = (i < ni - 1) ? rn(ro[rc + 1], qv[rc + 1]) : rn(her[w], heq[w]);
+        const V vw = rn(ro[rc - 1], qv[rc - 1]);
+        const V ve = rn(ro[rc + 1], qv[rc + 1]);
         const V vs = rn(ro[rc - P], qv[rc - P]);
         const V vn = rn(ro[rc + P], qv[rc + P]);
-        const int cr = w * CP + col0 + i;
-        const V z = (V)op_M<C>(pc[cr], pw[cr], pw[cr + 1], ps[cr], ps[cr + CP], (C)vc, (C)vw, (C)ve, (C)vs,
-                               (C)vn);                                                        // cg2d.py:245
-        stcg(r_out + crv + i, vc);
-        push_s(ptab, r_halo, j, w, i, vc);
-        stcg(z_out + crv + i, z);
-        push_s(ptab, z_halo, j, w, i, z);
+        const int cr = cb0 + i;
+        const V z = (V)op_M<C>(cp[cr + 2 * CL], cp[cr], cp[cr + 1], cp[cr + CL], cp[cr + CL + CR], (C)vc, (C)vw,
+                               (C)ve, (C)vs, (C)vn);                                          // cg2d.py:245
+        stcg(r_out + grow + i, vc);
+        push_s(ptab, r_out, j, w, i, vc);
+        stcg(z_out + grow + i, z);
+        push_s(ptab, z_out, j, w, i, z);
         emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));                 // cg2d.py:256, 246
       }
     } else if (pt == P_Z) {
       const V* rr_ = reinterpret_cast<const V*>(sb + L.vec[s][0]);
-      const V* hw = reinterpret_cast<const V*>(sb + L.hw[s][0]);
-      const V* he = reinterpret_cast<const V*>(sb + L.he[s][0]);
-      const C* pw = reinterpret_cast<const C*>(cb);
-      const C* ps = reinterpret_cast<const C*>(cb + L.coef_stride);
-      const C* pc = reinterpret_cast<const C*>(cb + 2 * L.coef_stride);
-      const int P = L.vpitch[0];
+      const C* cp = reinterpret_cast<const C*>(sb + L.coef);
       V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
-      V* z_halo = halo_ptr<V>(g, c.inst, s, V_Z);
       for (int i = lane; i < ni; i += 32) {
-        const int rc = (w + 1) * P + i;
+        const int rc = (w + 1) * P + i + 1;
         const V vc = rr_[rc];
-        const V vw = (i > 0) ? rr_[rc - 1] : hw[w];
-        const V ve = (i < ni - 1) ? rr_[rc + 1] : he[w];
-        const int cr = w * CP + col0 + i;
-        const V z = (V)op_M<C>(pc[cr], pw[cr], pw[cr + 1], ps[cr], ps[cr + CP], (C)vc, (C)vw, (C)ve,
-                               (C)rr_[rc - P], (C)rr_[rc + P]);
-        stcg(z_out + crv + i, z);
-        push_s(ptab, z_halo, j, w, i, z);
+        const int cr = cb0 + i;
+        const V z = (V)op_M<C>(cp[cr + 2 * CL], cp[cr], cp[cr + 1], cp[cr + CL], cp[cr + CL + CR], (C)vc,
+                               (C)rr_[rc - 1], (C)rr_[rc + 1], (C)rr_[rc - P], (C)rr_[rc + P]);
+        stcg(z_out + grow + i, z);
+        push_s(ptab, z_out, j, w, i, z);
         emit(s, i, mul((double)z, (double)vc), 0.0);
       }
     } else {  // P_R: the FP64 true residual b - A x_{k+1}
       const double* xr = reinterpret_cast<const double*>(sb + L.vec[s][0]);
       const V* sk = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      const double* hwx = reinterpret_cast<const double*>(sb + L.hw[s][0]);
-      const V* hws = reinterpret_cast<const V*>(sb + L.hw[s][1]);
-      const double* hex = reinterpret_cast<const double*>(sb + L.he[s][0]);
-      const V* hes = reinterpret_cast<const V*>(sb + L.he[s][1]);
-      const double* aw = reinterpret_cast<const double*>(cb);
-      const double* as = reinterpret_cast<const double*>(cb + L.coef_stride);
-      const double* ac = reinterpret_cast<const double*>(cb + 2 * L.coef_stride);
-      const int PX = L.vpitch[0], PS = L.vpitch[1];
+      const double* aw = reinterpret_cast<const double*>(sb + L.coef);
+      const double* as = reinterpret_cast<const double*>(sb + L.coef + L.coef_stride);
+      const double* ac = reinterpret_cast<const double*>(sb + L.coef + 2 * L.coef_stride);
+      const int NP = tp.npx, col0 = tp.OLx;
       const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
-      V* r_halo = halo_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       auto x1 = [&](double xx, V ss) -> double { return add(xx, mul(alpha, (double)ss)); };
       for (int i = lane; i < ni; i += 32) {
-        const int rx = (w + 1) * PX + i, rs = (w + 1) * PS + i;
-        const double vc = x1(xr[rx], sk[rs]);
-        const double vw = (i > 0) ? x1(xr[rx - 1], sk[rs - 1]) : x1(hwx[w], hws[w]);
-        const double ve = (i < ni - 1) ? x1(xr[rx + 1], sk[rs + 1]) : x1(hex[w], hes[w]);
-        const double vs = x1(xr[rx - PX], sk[rs - PS]);
-        const double vn = x1(xr[rx + PX], sk[rs + PS]);
-        const int cr = w * CP + col0 + i;
+        const int rc = (w + 1) * P + i + 1;
+        const double vc = x1(xr[rc], sk[rc]);
+        const double vw = x1(xr[rc - 1], sk[rc - 1]);
+        const double ve = x1(xr[rc + 1], sk[rc + 1]);
+        const double vs = x1(xr[rc - P], sk[rc - P]);
+        const double vn = x1(xr[rc + P], sk[rc + P]);
+        const int cr = w * NP + col0 + i;
         const double bn = mul(mul(__ldg(g.b[s] + prow + i), si.norm(s)), si.rnorm(s));
-        const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + CP], ac[cr], vw, ve, vs, vn, vc));
-        stcg(r_out + crv + i, r);
-        push_s(ptab, r_halo, j, w, i, r);
+        const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + NP], ac[cr], vw, ve, vs, vn, vc));
+        stcg(r_out + grow + i, r);
+        push_s(ptab, r_out, j, w, i, r);
         emit(s, i, mul((double)r, (double)r), 0.0);
       }
     }
@@ -1043,7 +1030,7 @@ __device__ bool run_pass_tma(const KParams& kp, int pt, int k, int hidx, const S
     const Lanes lp = compute_chunk<MIXED>(kp, cur, pt, k, si, sm.stage + st * kp.stage_bytes, sm);
     if ((tid >> 5) < cur.nr && !kp.serial) row_sums(g, lp, sm);
     __syncthreads();
-    if (tid == 0) accumulate_chunk(kp, g, ns0, ns1, cur.nr, sm);
+    if (tid < 32) accumulate_chunk(kp, g, ns0, ns1, cur.nr, sm);
     PROF_ADD(kp, sm, PR_COMP, t0);
     if (cur.jc + cur.nr >= cur.j1u) finish_unit(kp, g, cur.inst, cur.lu, ns0, ns1, sm);
     // row sums and stage buffers are rewritten by the next chunk
@@ -1137,7 +1124,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   }
   // ---- x = x0 rhsNorm, r = b - A x, s = 0, err^2, sumRHS (cg2d.py:226-236)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  init_x_halo(kp, sm);
+  init_x_ring(kp, sm);
   ok = run_pass_direct<MIXED>(kp, P_INIT, sm);
   ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
   if (!ok) goto epilogue;
@@ -1278,21 +1265,31 @@ epilogue:
 }
 
 // ------------------------------------------------------------------------------------------------
-// MIXED: FP32 copies of the six coefficient arrays, [inst][6][T][npy][ldc] (row pitch ldc)
+// packed coefficients: [inst][A, M][T][nj+1][3][ldc] in the solver's precision, rows j = 0 .. nj and
+// columns i = 0 .. ni of (aW2d, aS2d, aC2d) and (pW, pS, pC); columns past ni are 0
 
-__global__ void pack32_kernel(GroupDev g) {
+template <class C>
+__global__ void pack_coef_kernel(GroupDev g) {
   const TopoDev& tp = g.tp;
-  const long long rows = (long long)tp.T * tp.npy;
-  const long long tot = rows * g.ldc * 6 * g.count;
+  const int ldc = g.ldc, rows = tp.nj + 1;
+  const long long tot = (long long)g.count * 2 * tp.T * rows * 3 * ldc;
+  C* out = static_cast<C*>(g.cpk);
   for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < tot;
        idx += (long long)gridDim.x * blockDim.x) {
-    const long long row = idx / g.ldc;
-    const int col = (int)(idx - row * g.ldc);
-    const long long ia = row / rows;             // inst * 6 + which
-    const long long r = row - ia * rows;
-    const int which = (int)(ia % 6);
-    const long long in = ia / 6;
-    g.c32[idx] = col < tp.npx ? __double2float_rn(g.a64[which][in * g.pad_elems + r * tp.npx + col]) : 0.0f;
+    long long r = idx / ldc;
+    const int i = (int)(idx - r * ldc);
+    const int w = (int)(r % 3); r /= 3;
+    const int j = (int)(r % rows); r /= rows;
+    const int t = (int)(r % tp.T); r /= tp.T;
+    const int op = (int)(r % 2);
+    const long long in = r / 2;
+    C v = (C)0;
+    if (i <= tp.ni) {
+      const double a = g.a64[op * 3 + w][in * g.pad_elems + ((long long)t * tp.npy + j + tp.OLy) * tp.npx + i + tp.OLx];
+      if constexpr (sizeof(C) == 4) v = __double2float_rn(a);
+      else v = a;
+    }
+    out[idx] = v;
   }
 }
 
@@ -1411,9 +1408,10 @@ cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream);
 }
 
-cudaError_t launch_pack32(const GroupDev& g, cudaStream_t stream) {
-  const long long tot = (long long)g.tp.T * g.tp.npy * g.ldc * 6 * g.count;
-  pack32_kernel<<<grid_for(tot), 256, 0, stream>>>(g);
+cudaError_t launch_pack_coef(const GroupDev& g, int mixed, cudaStream_t stream) {
+  const long long tot = (long long)g.count * 2 * g.tp.T * (g.tp.nj + 1) * 3 * g.ldc;
+  if (mixed) pack_coef_kernel<float><<<grid_for(tot), 256, 0, stream>>>(g);
+  else pack_coef_kernel<double><<<grid_for(tot), 256, 0, stream>>>(g);
   return cudaGetLastError();
 }
 
