@@ -101,8 +101,9 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
       L->ch = ch;
       L->stage_bytes = sb;
       L->smem = smem;
-      for (int i = 0; i < P_NPASS; ++i) L->nstage[i] = 2;
-      L->nstage[P_R] = (rep <= sb) ? 2 : 1;
+      // FORTRAN order keeps every element product of a chunk in one buffer: one stage
+      for (int i = 0; i < P_NPASS; ++i) L->nstage[i] = serial ? 1 : 2;
+      L->nstage[P_R] = (!serial && rep <= sb) ? 2 : 1;
       return CG2D_OK;
     }
   }
@@ -120,7 +121,7 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     const cg2d_group_t& G = gr[g];
     if (!G.topo || G.count < 1 || G.nrhs < 1 || G.nrhs > 2) return CG2D_BAD_ARG;
     const cg2d_topology* tp = G.topo;
-    if (tp->nTiles > kMaxTiles || tp->sNx > kMaxNi) return CG2D_UNSUPPORTED;
+    if (tp->nTiles > kMaxTiles || tp->sNx > kMaxNi || tp->sNy > kMaxNi) return CG2D_UNSUPPORTED;
     // bulk copies move whole padded coefficient rows: 16-byte multiples
     if (((tp->sNx + 2 * tp->OLx) * 8) % 16 != 0) return CG2D_UNSUPPORTED;
     for (int s = 0; s < G.nrhs; ++s) {
@@ -360,6 +361,11 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   kp.timeout_ns = (unsigned long long)(params->timeout_s * 1e9);
   kp.test_missing = params->test_missing_arrivals;
   kp.prof = params->profile ? reinterpret_cast<unsigned long long*>(ws + L.prof) : nullptr;
+  for (int g = 0; g < ngroups; ++g) {
+    const cg2d_topology* tp = groups[g].topo;
+    for (int pt = 0; pt < P_NPASS; ++pt)
+      kp.lay[g][pt] = stage_layout(pt, kp.mixed, L.ch, groups[g].nrhs, tp->sNx, tp->sNx + 2 * tp->OLx);
+  }
   int unit_base = 0, op_base = 0, rhs_base = 0;
   for (int g = 0; g < ngroups; ++g) {
     const cg2d_group_t& G = groups[g];
@@ -397,10 +403,6 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
     rhs_base += G.count * G.nrhs;
   }
 
-  if (cudaMemsetAsync(ws, 0, L.zero_end, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
-  for (int g = 0; g < ngroups; ++g)
-    if (launch_pack_coef(kp.g[g], kp.mixed, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
-
   const size_t smem = L.smem;
   int bps = 0;
   if (solver_occupancy(kp.mixed, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
@@ -413,6 +415,11 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   if (grid > kp.total_units) grid = kp.total_units;
   if (grid > kMaxCtas) grid = kMaxCtas;
   if (grid < 1) grid = 1;
+  if ((kp.total_units + grid - 1) / grid > kMaxUnitsPerCta) return CG2D_UNSUPPORTED;   // unit table of a CTA
+  if (cudaMemsetAsync(ws, 0, L.zero_end, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  for (int g = 0; g < ngroups; ++g)
+    if (launch_pack_coef(kp.g[g], kp.mixed, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+
   if (launch_solver(kp, (int)grid, smem, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return CG2D_OK;
 }

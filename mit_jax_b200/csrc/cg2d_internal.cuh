@@ -8,8 +8,11 @@
 
 namespace cg2d {
 
-constexpr int kWarps = 8;                  // warps per CTA; a chunk has at most kWarps rows (one warp per row)
-constexpr int kThreads = kWarps * 32;
+constexpr int kWarps = 8;                  // compute warps per CTA; a chunk has at most kWarps rows (one warp per row)
+constexpr int kProducer = kWarps;          // index of the warp that issues the bulk copies and folds the row sums
+constexpr int kThreads = (kWarps + 1) * 32;
+constexpr int kMaxStages = 2;              // stage buffers of the copy pipeline
+constexpr int kMaxUnitsPerCta = 512;       // work units one CTA owns in a launch (its unit table)
 constexpr int kMaxGroups = CG2D_MAX_GROUPS;
 constexpr int kMaxSolves = CG2D_MAX_SOLVES; // right-hand sides per launch (one thread owns each)
 constexpr int kMaxOps = 256;               // operators (instances) per launch
@@ -74,31 +77,6 @@ struct GroupDev {
   long long vec_off[V_NVEC];
 };
 
-struct KParams {
-  GroupDev g[kMaxGroups];
-  int ngroups, total_units, total_rhs, total_ops;
-  int mixed, serial, rows_per_block, replace_every;
-  double replace_above;
-  int max_ni;
-  int ch;                   // rows per chunk (<= kWarps)
-  int nstage[P_NPASS];      // pipeline depth of each pass kind (1 or 2)
-  unsigned stage_bytes;     // bytes of one stage buffer
-  double* hist;             // [total_rhs][H_NKIND][hist_len]
-  int hist_len;
-  double* part;             // [total_rhs][2][part_units]
-  int part_units;
-  unsigned* cnt;            // [total_ops] monotonic per-operator unit counters
-  unsigned long long* rmax; // [total_rhs] max|b*cg2dNorm| as ordered bits
-  unsigned* gs;             // [0] grid barrier arrivals, [1] error word, [2] where, [3] pass << 16 | CTA
-  unsigned long long timeout_ns;
-  int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
-  unsigned long long* prof; // nullable: [1 + grid * 8] phase times (ns) per CTA
-};
-
-constexpr int kMaxCtas = 148 * 8;
-enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FIN = 4, PR_DIRECT = 5, PR_OTHER = 6,
-                       PR_TOTAL = 7 };
-
 // Shared-memory image of one chunk for a pipelined pass (offsets in bytes from the stage buffer).
 struct StageLay {
   int packed;                   // coefficients: 1 packed block (S, X, Z) or 3 FP64 arrays (R)
@@ -148,6 +126,32 @@ __host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int 
   L.total = al128(o);
   return L;
 }
+
+struct KParams {
+  GroupDev g[kMaxGroups];
+  int ngroups, total_units, total_rhs, total_ops;
+  int mixed, serial, rows_per_block, replace_every;
+  double replace_above;
+  int max_ni;
+  int ch;                   // rows per chunk (<= kWarps)
+  int nstage[P_NPASS];      // pipeline depth of each pass kind (1 or 2)
+  unsigned stage_bytes;     // bytes of one stage buffer
+  double* hist;             // [total_rhs][H_NKIND][hist_len]
+  int hist_len;
+  double* part;             // [total_rhs][2][part_units]
+  int part_units;
+  unsigned* cnt;            // [total_ops] monotonic per-operator unit counters
+  unsigned long long* rmax; // [total_rhs] max|b*cg2dNorm| as ordered bits
+  unsigned* gs;             // [0] grid barrier arrivals, [1] error word, [2] where, [3] pass << 16 | CTA
+  unsigned long long timeout_ns;
+  int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
+  unsigned long long* prof; // nullable: [1 + grid * 8] phase times (ns) per CTA
+  StageLay lay[kMaxGroups][P_NPASS];  // shared-memory image of a chunk, per group and pipelined pass
+};
+
+constexpr int kMaxCtas = 148 * 8;
+enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FIN = 4, PR_DIRECT = 5, PR_OTHER = 6,
+                       PR_TOTAL = 7 };
 
 // launchers (cg2d_solver.cu)
 size_t fixed_smem_bytes(int max_ni, int serial);

@@ -149,6 +149,10 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // ------------------------------------------------------------------------------------------------
 // shared memory carve
 
+// the dynamic shared memory of the persistent kernel; pointers derived from this symbol are known to the
+// compiler to address shared memory (shared loads, no aliasing with global stores)
+extern __shared__ __align__(128) unsigned char smem_raw[];
+
 struct Smem {
   int* act;          // [kMaxSolves] action of each solve in the current pass
   double* c1;        // [kMaxSolves] pass coefficient (beta in S, alpha in X and R)
@@ -157,16 +161,20 @@ struct Smem {
   double* norm;      // [kMaxSolves] cg2dNorm
   int* has_alpha;    // [kMaxSolves]
   int* opp;          // [kMaxOps] operator takes part in the pass
-  double* rowsum;    // [2 slots][2 kinds][kWarps]
+  double* rowsum;    // [kMaxStages][4 sums][kWarps] row sums of the chunk in each stage
   double* tsum;      // [kMaxTiles]
-  int* misc;         // [4]: barrier ok flag, last-arriver flag
-  unsigned long long* bar;  // [2] stage mbarriers
-  unsigned long long* pacc; // [8] phase times of this CTA (thread 0; profiling)
+  int* misc;         // [4]: barrier ok flag, -, reducer ok flag, number of units in the unit table
+  unsigned long long* full;   // [kMaxStages] stage mbarriers: the chunk's copies have landed
+  unsigned long long* empty;  // [kMaxStages] stage mbarriers: the compute warps are done with the stage
+  unsigned long long* pacc;   // [8] phase times of this CTA (profiling)
   unsigned* opn;            // [kMaxOps] passes with sums each operator has completed (its counter target)
-  double* uacc;             // [4] thread 0: the current unit's partial sums (slot, kind)
+  double* uacc;             // [4] the current unit's partial sums (slot, kind)
   unsigned* ucnt;           // [kMaxOps] units this CTA completed in the current pass, per operator
+  int2* utab;               // [kMaxUnitsPerCta] this CTA's work units (unit_pack)
+  int4* pend;               // [kMaxStages] chunk in each stage awaiting its row sums: unit, jc, nr
   double* prod;      // FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]
-  unsigned char* stage;     // 2 x stage_bytes (128-aligned); also the direct-load staging area
+  unsigned stage;    // offset of the stage buffers (kMaxStages x stage_bytes, 128-aligned) in smem_raw; also
+                     // the direct-pass staging area and the reducer's gather buffer
 };
 
 __host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
@@ -177,19 +185,22 @@ size_t fixed_smem_bytes(int max_ni, int serial) {
   s += 4 * a16(sizeof(double) * kMaxSolves);
   s += a16(sizeof(int) * kMaxSolves);
   s += a16(sizeof(int) * kMaxOps);
-  s += a16(sizeof(double) * 2 * 2 * kWarps);
+  s += a16(sizeof(double) * kMaxStages * 4 * kWarps);
   s += a16(sizeof(double) * kMaxTiles);
   s += a16(sizeof(int) * 4);
-  s += a16(sizeof(unsigned long long) * 2);
+  s += 2 * a16(sizeof(unsigned long long) * kMaxStages);
   s += a16(sizeof(unsigned long long) * 8);
   s += a16(sizeof(unsigned) * kMaxOps);
   s += a16(sizeof(double) * 4);
   s += a16(sizeof(unsigned) * kMaxOps);
+  s += a16(sizeof(int2) * kMaxUnitsPerCta);
+  s += a16(sizeof(int4) * kMaxStages);
   if (serial) s += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni);
   return (s + 127) & ~size_t(127);
 }
 
-__device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
+__device__ inline Smem carve(int max_ni, int serial) {
+  unsigned char* base = smem_raw;
   Smem m;
   size_t o = 0;
   m.act = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxSolves);
@@ -199,18 +210,21 @@ __device__ inline Smem carve(unsigned char* base, int max_ni, int serial) {
   m.norm = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
   m.has_alpha = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxSolves);
   m.opp = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxOps);
-  m.rowsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps);
+  m.rowsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxStages * 4 * kWarps);
   m.tsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxTiles);
   m.misc = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * 4);
-  m.bar = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 2);
+  m.full = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * kMaxStages);
+  m.empty = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * kMaxStages);
   m.pacc = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 8);
   m.opn = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
   m.uacc = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 4);
   m.ucnt = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
+  m.utab = reinterpret_cast<int2*>(base + o); o += a16(sizeof(int2) * kMaxUnitsPerCta);
+  m.pend = reinterpret_cast<int4*>(base + o); o += a16(sizeof(int4) * kMaxStages);
   m.prod = nullptr;
   if (serial) { m.prod = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni); }
   o = (o + 127) & ~size_t(127);
-  m.stage = base + o;
+  m.stage = (unsigned)o;
   return m;
 }
 
@@ -363,34 +377,35 @@ __device__ __forceinline__ double butterfly(double v) {
   for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-__device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, const Smem& sm) {
+__device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, const Smem& sm, int st) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double r0 = butterfly(lp.v[0]), r1 = butterfly(lp.v[1]);
   double r2 = 0.0, r3 = 0.0;
   if (g.nrhs > 1) { r2 = butterfly(lp.v[2]); r3 = butterfly(lp.v[3]); }
   if (lane == 0) {
-    sm.rowsum[0 * kWarps + warp] = r0;
-    sm.rowsum[1 * kWarps + warp] = r1;
-    sm.rowsum[2 * kWarps + warp] = r2;
-    sm.rowsum[3 * kWarps + warp] = r3;
+    double* rs = sm.rowsum + st * 4 * kWarps;
+    rs[0 * kWarps + warp] = r0;
+    rs[1 * kWarps + warp] = r1;
+    rs[2 * kWarps + warp] = r2;
+    rs[3 * kWarps + warp] = r3;
   }
 }
 
-// warp 0: add the chunk's rows into the unit's partial sums, lane l < 4 owning sum (slot l >> 1, kind l & 1)
-// (ROWBLOCK: row sums in row order; FORTRAN: every product in j, i order). Ends with the warp converged, so
-// thread 0 may read the partials.
+// one warp: add the chunk's rows (row sums of stage st) into the unit's partial sums, lane l < 4 owning sum
+// (slot l >> 1, kind l & 1); `first` starts the unit from 0 (ROWBLOCK: row sums in row order; FORTRAN: every
+// product in j, i order). Ends with the warp converged, so its lane 0 may read the partials.
 __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupDev& g, int ns0, int ns1, int nr,
-                                                 const Smem& sm) {
+                                                 int st, bool first, const Smem& sm) {
   const int lane = threadIdx.x & 31;
   const int s = lane >> 1, q = lane & 1;
   if (lane < 4 && q < (s == 0 ? ns0 : ns1)) {
-    double a = sm.uacc[lane];
+    double a = first ? 0.0 : sm.uacc[lane];
     if (kp.serial) {
       const double* pr = sm.prod + (lane * kWarps) * kp.max_ni;
       for (int w = 0; w < nr; ++w)
         for (int i = 0; i < g.tp.ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
     } else {
-      const double* rs = sm.rowsum + lane * kWarps;
+      const double* rs = sm.rowsum + (st * 4 + lane) * kWarps;
       double v[kWarps];
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) v[w] = rs[w];
@@ -403,14 +418,14 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
   __syncwarp();
 }
 
-// thread 0 writes the unit's partials (no wait) and counts the unit in shared memory; the counts are published
-// once per pass (publish_counts)
+// lane 0 of the accumulating warp writes the unit's partials (no wait) and counts the unit in shared memory; the
+// counts are published once per pass (publish_counts)
 __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int ns0, int ns1,
                                             const Smem& sm) {
-  if (threadIdx.x != 0 || ns0 + ns1 == 0) return;
+  if ((threadIdx.x & 31) != 0 || ns0 + ns1 == 0) return;
   const int rid0 = g.rhs_base + inst * g.nrhs;
   if (ns0 > 0) stcg(kp.part + ((size_t)rid0 * 2 + 0) * kp.part_units + lu, sm.uacc[0]);
   if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, sm.uacc[1]);
@@ -421,7 +436,7 @@ __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g
 // every CTA, end of its units: add its unit counts to the operators' counters (release: the partials written
 // before are visible to whoever observes the count)
 __device__ __forceinline__ void publish_counts(const KParams& kp, const Smem& sm) {
-  if (threadIdx.x == 0) __threadfence();
+  if (threadIdx.x == 0 || threadIdx.x == kProducer * 32) __threadfence();   // the writers of the unit partials
   __syncthreads();
   for (int op = threadIdx.x; op < kp.total_ops; op += kThreads) {
     const unsigned c = sm.ucnt[op];
@@ -439,7 +454,7 @@ __device__ __forceinline__ void publish_counts(const KParams& kp, const Smem& sm
 __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   publish_counts(kp, sm);
-  double* buf = reinterpret_cast<double*>(sm.stage);   // free at the end of a pass
+  double* buf = reinterpret_cast<double*>(smem_raw + sm.stage);   // free at the end of a pass
   bool ok = true;
   for (int gi = 0; gi < kp.ngroups && ok; ++gi) {
     const GroupDev& g = kp.g[gi];
@@ -530,7 +545,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
   const long long pe = g.pad_elems;
   const int W = ni + 2;
   const int SW = (kWarps + 2) * (kp.max_ni + 2);
-  double* stage = reinterpret_cast<double*>(sm.stage);
+  double* stage = reinterpret_cast<double*>(smem_raw + sm.stage);
   const Slots si = slots_of(g, inst, sm);
   const int ns0 = nsums(pt, si.act(0));
   const int ns1 = g.nrhs > 1 ? nsums(pt, si.act(1)) : 0;
@@ -538,7 +553,6 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
   const double* aS = g.a64[1] + inst * pe;
   const double* aC = g.a64[2] + inst * pe;
 
-  if (tid == 0) sm.uacc[0] = sm.uacc[1] = sm.uacc[2] = sm.uacc[3] = 0.0;
   unsigned long long vmax0 = 0ull, vmax1 = 0ull;
 
   if (pt == P_MAX) {
@@ -646,7 +660,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
           vmax1 = y1 > vmax1 ? y1 : vmax1;
         }
       } else if (!kp.serial) {
-        row_sums(g, lp, sm);
+        row_sums(g, lp, sm, 0);
       }
     }
     if (pt == P_MAX) {
@@ -657,10 +671,10 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
       continue;
     }
     __syncthreads();
-    if (tid < 32) accumulate_chunk(kp, g, ns0, ns1, nr, sm);
+    if (tid < 32) accumulate_chunk(kp, g, ns0, ns1, nr, 0, jc == j0, sm);
   }
   if (pt == P_MAX) return;
-  finish_unit(kp, g, inst, lu, ns0, ns1, sm);
+  if (tid < 32) finish_unit(kp, g, inst, lu, ns0, ns1, sm);
   __syncthreads();   // the unit accumulators are reused by the next unit
 }
 
@@ -722,37 +736,76 @@ __device__ void init_x_ring(const KParams& kp, const Smem& sm) {
 // ------------------------------------------------------------------------------------------------
 // pipelined passes: chunks of this CTA in order, bulk copies into two stage buffers
 
-struct Chunk {
-  int u, gi, inst, lu, t, j0u, j1u, jc, nr;
+// this CTA's work units: u = blockIdx.x + n gridDim.x, packed once at the start of the launch
+//   x = gi | inst << 2 | lu << 10,   y = t | j0 << 8 | j1 << 19
+struct Unit {
+  int gi, inst, lu, t, j0, j1;
 };
-
-__device__ bool chunk_unit(const KParams& kp, const Smem& sm, int u, Chunk& c) {
-  for (; u < kp.total_units; u += gridDim.x) {
+__device__ __forceinline__ Unit unit_at(const Smem& sm, int ui) {
+  const int2 e = sm.utab[ui];
+  Unit u;
+  u.gi = e.x & 3; u.inst = (e.x >> 2) & 255; u.lu = (unsigned)e.x >> 10;
+  u.t = e.y & 255; u.j0 = (e.y >> 8) & 2047; u.j1 = (unsigned)e.y >> 19;
+  return u;
+}
+__device__ void build_unit_table(const KParams& kp, const Smem& sm) {
+  const int n = (kp.total_units - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  for (int q = threadIdx.x; q < n; q += kThreads) {
+    const int u = (int)blockIdx.x + q * (int)gridDim.x;
     int gi = 0;
     while (gi + 1 < kp.ngroups && u >= kp.g[gi + 1].unit_base) ++gi;
     const GroupDev& g = kp.g[gi];
     const int rel = u - g.unit_base;
     const int inst = rel / g.units;
-    if (!sm.opp[g.op_base + inst]) continue;
     const int lu = rel - inst * g.units;
     const int t = lu / g.nblk, blk = lu - t * g.nblk;
     const int R = kp.serial ? g.tp.nj : kp.rows_per_block;
-    c.u = u; c.gi = gi; c.inst = inst; c.lu = lu; c.t = t;
-    c.j0u = blk * R;
-    c.j1u = min(g.tp.nj, c.j0u + R);
-    c.jc = c.j0u;
-    c.nr = min(kp.ch, c.j1u - c.jc);
-    return true;
+    const int j0 = blk * R, j1 = min(g.tp.nj, j0 + R);
+    sm.utab[q] = make_int2(gi | (inst << 2) | (lu << 10), t | (j0 << 8) | (j1 << 19));
+  }
+  if (threadIdx.x == 0) sm.misc[3] = n > 0 ? n : 0;
+}
+
+// position in this CTA's chunk sequence of a pass: unit ui of the table, first row jc; units of operators that
+// take no part in the pass are skipped
+struct Cursor {
+  int ui, jc;
+};
+__device__ __forceinline__ bool cursor_unit(const KParams& kp, const Smem& sm, Cursor& c) {
+  const int n = sm.misc[3];
+  for (++c.ui; c.ui < n; ++c.ui) {
+    const Unit u = unit_at(sm, c.ui);
+    if (sm.opp[kp.g[u.gi].op_base + u.inst]) {
+      c.jc = u.j0;
+      return true;
+    }
   }
   return false;
 }
-__device__ bool chunk_next(const KParams& kp, const Smem& sm, Chunk& c) {
-  if (c.jc + kp.ch < c.j1u) {
+__device__ __forceinline__ bool cursor_first(const KParams& kp, const Smem& sm, Cursor& c) {
+  c.ui = -1;
+  c.jc = 0;
+  return cursor_unit(kp, sm, c);
+}
+__device__ __forceinline__ bool cursor_next(const KParams& kp, const Smem& sm, Cursor& c) {
+  const Unit u = unit_at(sm, c.ui);
+  if (c.jc + kp.ch < u.j1) {
     c.jc += kp.ch;
-    c.nr = min(kp.ch, c.j1u - c.jc);
     return true;
   }
-  return chunk_unit(kp, sm, c.u + gridDim.x, c);
+  return cursor_unit(kp, sm, c);
+}
+
+struct Chunk {
+  int gi, inst, lu, t, j0u, j1u, jc, nr;
+};
+__device__ __forceinline__ Chunk chunk_at(const KParams& kp, const Smem& sm, int ui, int jc) {
+  const Unit u = unit_at(sm, ui);
+  Chunk c;
+  c.gi = u.gi; c.inst = u.inst; c.lu = u.lu; c.t = u.t; c.j0u = u.j0; c.j1u = u.j1;
+  c.jc = jc;
+  c.nr = min(kp.ch, u.j1 - jc);
+  return c;
 }
 
 // the vector a pass stages as stencil input v (0, 1) of a solve
@@ -768,13 +821,13 @@ __device__ __forceinline__ int pass_vector(int pt, int k, int hidx, int v) {
 // the three FP64 operator arrays), 3 the west/east push targets of the chunk's rows, 4 and 5 the south /
 // north push targets (first / last chunk of a tile), 6 + 2 s + v vector v of slot s (rows jc-1 .. jc+nr,
 // ring cells included), 10 + s the own rows of x (pass S).
-template <bool MIXED>
-__device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, int hidx, const Smem& sm,
-                            unsigned char* sb, unsigned long long* bar) {
+__device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, int hidx, const Smem& sm, int st) {
   const GroupDev& g = kp.g[c.gi];
   const TopoDev& tp = g.tp;
   const int lane = threadIdx.x & 31;
-  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx);
+  const StageLay& L = kp.lay[c.gi][pt];
+  unsigned char* sb = smem_raw + sm.stage + st * kp.stage_bytes;
+  unsigned long long* bar = &sm.full[st];
   const int rid0 = g.rhs_base + c.inst * g.nrhs;
   const bool act0 = sm.act[rid0] == A_ACTIVE;
   const bool act1 = g.nrhs > 1 && sm.act[rid0 + 1] == A_ACTIVE;
@@ -835,8 +888,8 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
 // point (w, i) of a vector is element (w + 1) P + i + 1 (its neighbours at -1, +1, -P, +P) and of the packed
 // coefficients element w 3 ldc + i (columns: W/pW, +ldc S/pS, +2 ldc C/pC; east face +1, north face +3 ldc).
 template <bool MIXED>
-__device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si,
-                               const unsigned char* sb, const Smem& sm) {
+__device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si, int st,
+                               const Smem& sm) {
   Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
   using V = typename Prec<MIXED>::V;
   using C = typename Prec<MIXED>::C;
@@ -844,7 +897,8 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   const TopoDev& tp = g.tp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp >= c.nr) return lp;
-  const StageLay L = stage_layout(pt, MIXED, kp.ch, g.nrhs, tp.ni, tp.npx);
+  const StageLay& L = kp.lay[c.gi][pt];
+  const unsigned char* sb = smem_raw + sm.stage + st * kp.stage_bytes;
   const int ni = tp.ni, nj = tp.nj, t = c.t, w = warp, j = c.jc + w;
   const int P = tp.P, CL = g.ldc, CR = 3 * g.ldc;
   const long long grow = ((long long)t * (nj + 2) + j + 1) * P + 1;   // element of (t, j, 0)
@@ -991,59 +1045,117 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   return lp;
 }
 
+// Copy pipeline of a pass. The producer warp walks this CTA's chunks, issues each chunk's bulk copies into the
+// next stage buffer (full barrier) and, before it reuses a stage, waits until the compute warps are done with it
+// (empty barrier) and folds that chunk's row sums into its unit's partial sums, in chunk order. The compute
+// warps walk the same chunks: wait for the stage, compute, write their row sums, release the stage. Each thread
+// keeps the parity bits of its role: the next wait on each stage's full (compute warps) and empty barrier
+// (producer), the parity of each stage's latest copy and the stages whose chunk awaits its row sums (producer).
+struct Pipe {
+  unsigned fph, eph, cph, pend;
+};
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// producer: wait until the compute warps release stage st, then add its chunk's rows to the unit partials
+__device__ bool release_stage(const KParams& kp, int pt, const Smem& sm, int st, Pipe& pp,
+                              unsigned long long& t_wait) {
+  const unsigned long long t0 = kp.prof ? globaltimer() : 0ull;
+  const bool ok = mbar_wait(&sm.empty[st], (pp.eph >> st) & 1u, kp.timeout_ns);
+  pp.eph ^= 1u << st;
+  if (kp.prof) t_wait += globaltimer() - t0;
+  if (!__all_sync(0xffffffffu, ok)) return false;
+  pp.pend &= ~(1u << st);
+  const int4 e = sm.pend[st];
+  const Chunk c = chunk_at(kp, sm, e.x, e.y);
+  const GroupDev& g = kp.g[c.gi];
+  const Slots si = slots_of(g, c.inst, sm);
+  const int ns0 = nsums(pt, si.act(0));
+  const int ns1 = g.nrhs > 1 ? nsums(pt, si.act(1)) : 0;
+  accumulate_chunk(kp, g, ns0, ns1, c.nr, st, c.jc == c.j0u, sm);
+  if (c.jc + c.nr >= c.j1u) finish_unit(kp, g, c.inst, c.lu, ns0, ns1, sm);
+  return true;
+}
+
+__device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const Smem& sm, Pipe& pp) {
+  const int lane = threadIdx.x & 31;
+  const int ns = kp.nstage[pt];
+  const unsigned long long t_start = kp.prof ? globaltimer() : 0ull;
+  unsigned long long t_wait = 0ull;
+  int st = 0;
+  bool ok = true;
+  Cursor cur;
+  bool have = cursor_first(kp, sm, cur);
+  while (have) {
+    if ((pp.pend >> st) & 1u) {
+      if (!release_stage(kp, pt, sm, st, pp, t_wait)) { ok = false; break; }
+    }
+    const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
+    issue_chunk(kp, c, pt, k, hidx, sm, st);
+    pp.cph ^= 1u << st;
+    if (lane == 0) sm.pend[st] = make_int4(cur.ui, cur.jc, 0, 0);
+    __syncwarp();
+    pp.pend |= 1u << st;
+    st = (st + 1 == ns) ? 0 : st + 1;
+    have = cursor_next(kp, sm, cur);
+  }
+  // the last chunks, oldest first
+  for (int q = 0; q < ns && ok; ++q) {
+    if ((pp.pend >> st) & 1u) ok = release_stage(kp, pt, sm, st, pp, t_wait);
+    st = (st + 1 == ns) ? 0 : st + 1;
+  }
+  if (!ok) {
+    if (lane == 0) note_timeout(kp.gs, 2u, (unsigned)pt);
+    // a bounded wait for copies still in flight into this CTA's shared memory
+    for (int s2 = 0; s2 < kMaxStages; ++s2)
+      if ((pp.pend >> s2) & 1u) mbar_wait(&sm.full[s2], ((pp.cph >> s2) & 1u) ^ 1u, kp.timeout_ns);
+    pp.pend = 0u;
+  }
+  if (kp.prof && lane == 0) sm.pacc[PR_ISSUE] += (globaltimer() - t_start) - t_wait;
+  return ok;
+}
+
 template <bool MIXED>
-__device__ bool run_pass_tma(const KParams& kp, int pt, int k, int hidx, const Smem& sm, unsigned& phase) {
-  const int tid = threadIdx.x;
-  Chunk cur;
-  if (!chunk_unit(kp, sm, blockIdx.x, cur)) return reduce_pass(kp, pt, hidx, sm);
+__device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, Pipe& pp) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ns = kp.nstage[pt];
   int st = 0;
-  unsigned long long t0 = PROF_T0(kp);
-  if ((tid >> 5) == 0) issue_chunk<MIXED>(kp, cur, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
-  PROF_ADD(kp, sm, PR_ISSUE, t0);
-  Chunk nxt = cur;
-  bool have_next = chunk_next(kp, sm, nxt);
-  bool have = true;
+  Cursor cur;
+  bool have = cursor_first(kp, sm, cur);
   while (have) {
-    t0 = PROF_T0(kp);
-    if (ns == 2 && have_next && (tid >> 5) == 0)
-      issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage + (st ^ 1) * kp.stage_bytes, &sm.bar[st ^ 1]);
-    PROF_ADD(kp, sm, PR_ISSUE, t0);
-    t0 = PROF_T0(kp);
-    const bool ok = mbar_wait(&sm.bar[st], (phase >> st) & 1u, kp.timeout_ns);
-    phase ^= 1u << st;
+    unsigned long long t0 = PROF_T0(kp);
+    const bool ok = mbar_wait(&sm.full[st], (pp.fph >> st) & 1u, kp.timeout_ns);
+    pp.fph ^= 1u << st;
     PROF_ADD(kp, sm, PR_MBAR, t0);
-    if (__syncthreads_or(!ok)) {
-      // a copy did not complete in time: flag the error, give the copies in flight a bounded time to land
-      if (tid == 0) note_timeout(kp.gs, 2u, (unsigned)pt);
-      mbar_wait(&sm.bar[st], ((phase >> st) & 1u) ^ 1u, kp.timeout_ns);
-      if (ns == 2 && have_next) mbar_wait(&sm.bar[st ^ 1], (phase >> (st ^ 1)) & 1u, kp.timeout_ns);
-      __syncthreads();
+    if (!__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) note_timeout(kp.gs, 2u, (unsigned)pt);
       return false;
     }
-    const GroupDev& g = kp.g[cur.gi];
-    const Slots si = slots_of(g, cur.inst, sm);
-    const int ns0 = nsums(pt, si.act(0));
-    const int ns1 = g.nrhs > 1 ? nsums(pt, si.act(1)) : 0;
-    if (tid == 0 && cur.jc == cur.j0u) sm.uacc[0] = sm.uacc[1] = sm.uacc[2] = sm.uacc[3] = 0.0;
     t0 = PROF_T0(kp);
-    const Lanes lp = compute_chunk<MIXED>(kp, cur, pt, k, si, sm.stage + st * kp.stage_bytes, sm);
-    if ((tid >> 5) < cur.nr && !kp.serial) row_sums(g, lp, sm);
-    __syncthreads();
-    if (tid < 32) accumulate_chunk(kp, g, ns0, ns1, cur.nr, sm);
+    const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
+    const GroupDev& g = kp.g[c.gi];
+    const Slots si = slots_of(g, c.inst, sm);
+    const Lanes lp = compute_chunk<MIXED>(kp, c, pt, k, si, st, sm);
+    if (warp < c.nr && !kp.serial) row_sums(g, lp, sm, st);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);
     PROF_ADD(kp, sm, PR_COMP, t0);
-    if (cur.jc + cur.nr >= cur.j1u) finish_unit(kp, g, cur.inst, cur.lu, ns0, ns1, sm);
-    // row sums and stage buffers are rewritten by the next chunk
-    __syncthreads();
-    if (ns == 1 && have_next && (tid >> 5) == 0) issue_chunk<MIXED>(kp, nxt, pt, k, hidx, sm, sm.stage, &sm.bar[0]);
-    cur = nxt;
-    have = have_next;
-    if (have) have_next = chunk_next(kp, sm, nxt);
-    if (ns == 2) st ^= 1;
+    st = (st + 1 == ns) ? 0 : st + 1;
+    have = cursor_next(kp, sm, cur);
   }
-  __syncthreads();
-  t0 = PROF_T0(kp);
-  const bool ok = reduce_pass(kp, pt, hidx, sm);
+  return true;
+}
+
+template <bool MIXED>
+__device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const Smem& sm, Pipe& pp) {
+  bool ok;
+  if ((threadIdx.x >> 5) == kProducer) ok = produce_pass(kp, pt, k, hidx, sm, pp);
+  else ok = consume_pass<MIXED>(kp, pt, k, sm, pp);
+  if (__syncthreads_or(!ok)) return false;
+  const unsigned long long t0 = PROF_T0(kp);
+  ok = reduce_pass(kp, pt, hidx, sm);
   PROF_ADD(kp, sm, PR_FIN, t0);
   return ok;
 }
@@ -1079,19 +1191,21 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const __grid_constant__ KParams kp) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  const Smem sm = carve(smem_raw, kp.max_ni, kp.serial);
+  const Smem sm = carve(kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
   unsigned target = (unsigned)kp.test_missing;
-  unsigned phase = 0;
+  Pipe pp = {0u, 0u, 0u, 0u};
   const unsigned long long t_start = PROF_T0(kp);
   if (tid < 8) sm.pacc[tid] = 0ull;
   for (int i = tid; i < kMaxOps; i += kThreads) { sm.opn[i] = 0u; sm.ucnt[i] = 0u; }
   if (tid == 0) {
-    mbar_init(&sm.bar[0], 1);
-    mbar_init(&sm.bar[1], 1);
+    for (int s = 0; s < kMaxStages; ++s) {
+      mbar_init(&sm.full[s], 1);          // the producer's arrive (with the copies' byte count)
+      mbar_init(&sm.empty[s], kWarps);    // one arrive per compute warp
+    }
     fence_mbar_init();
   }
+  build_unit_table(kp, sm);
   __syncthreads();
 
   // state of solve `tid` (identical in every CTA: computed from the same write-once sums)
@@ -1131,7 +1245,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   if (own) rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  ok = run_pass_tma<MIXED>(kp, P_Z, 0, 0, sm, phase);
+  ok = run_pass_pipe<MIXED>(kp, P_Z, 0, 0, sm, pp);
   ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
   if (!ok) goto epilogue;
   if (own) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
@@ -1155,7 +1269,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
-    ok = run_pass_tma<MIXED>(kp, P_S, k, k, sm, phase);
+    ok = run_pass_pipe<MIXED>(kp, P_S, k, k, sm, pp);
     ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
@@ -1173,7 +1287,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     }
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, alpha, 0.0);
-      ok = run_pass_tma<MIXED>(kp, P_X, k, k + 1, sm, phase);
+      ok = run_pass_pipe<MIXED>(kp, P_X, k, k + 1, sm, pp);
       ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
@@ -1183,7 +1297,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     }
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, alpha, 0.0);
-      ok = run_pass_tma<MIXED>(kp, P_R, k, k + 1, sm, phase);
+      ok = run_pass_pipe<MIXED>(kp, P_R, k, k + 1, sm, pp);
       ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
@@ -1191,7 +1305,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
         ++nrep;
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
-      ok = run_pass_tma<MIXED>(kp, P_Z, k, k + 1, sm, phase);
+      ok = run_pass_pipe<MIXED>(kp, P_Z, k, k + 1, sm, pp);
       ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
@@ -1253,11 +1367,12 @@ epilogue:
     if (!ok) { d.firstResidual = d.lastResidual = d.sumRHS = __longlong_as_double(0x7ff8000000000000LL); }
     g.diag[slot][inst] = d;
   }
+  if (kp.prof) __syncthreads();   // the producer warp's copy-issue time
   if (kp.prof && tid == 0 && blockIdx.x < kMaxCtas) {
     unsigned long long* o = kp.prof + 1 + (size_t)blockIdx.x * 8;
     const unsigned long long tot = globaltimer() - t_start;
-    unsigned long long acc = 0;
-    for (int i = 0; i < PR_OTHER; ++i) { o[i] = sm.pacc[i]; acc += sm.pacc[i]; }
+    unsigned long long acc = 0;   // thread 0's phases (the copy issue runs on the producer warp, beside them)
+    for (int i = 0; i < PR_OTHER; ++i) { o[i] = sm.pacc[i]; if (i != PR_ISSUE) acc += sm.pacc[i]; }
     o[PR_OTHER] = tot > acc ? tot - acc : 0ull;
     o[PR_TOTAL] = tot;
     if (blockIdx.x == 0) kp.prof[0] = gridDim.x;
