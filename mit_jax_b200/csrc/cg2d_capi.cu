@@ -405,7 +405,7 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
 
   const size_t smem = L.smem;
   int bps = 0;
-  if (solver_occupancy(kp.mixed, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  if (solver_occupancy(kp.mixed, kp.max_ni, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   if (params->ctas_per_sm > 0 && params->ctas_per_sm < bps) bps = params->ctas_per_sm;
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);

@@ -156,7 +156,7 @@ enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FI
 // launchers (cg2d_solver.cu)
 size_t fixed_smem_bytes(int max_ni, int serial);
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream);
-cudaError_t solver_occupancy(int mixed, size_t smem, int* blocks_per_sm);
+cudaError_t solver_occupancy(int mixed, int max_ni, size_t smem, int* blocks_per_sm);
 cudaError_t launch_pack_coef(const GroupDev& g, int mixed, cudaStream_t stream);
 cudaError_t launch_apply_operator(const TopoDev& tp, int batch, double norm, const double* aW, const double* aS,
                                   const double* aC, const double* v, double* out, cudaStream_t stream);

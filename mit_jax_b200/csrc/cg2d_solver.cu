@@ -102,7 +102,7 @@ __device__ __forceinline__ unsigned long long globaltimer() {
 #define PROF_T0(kp) (((kp).prof && threadIdx.x == 0) ? globaltimer() : 0ull)
 #define PROF_ADD(kp, sm, ph, t0)                                               \
   do {                                                                         \
-    if ((kp).prof && threadIdx.x == 0) (sm).pacc[ph] += globaltimer() - (t0); \
+    if ((kp).prof && threadIdx.x == 0) (sm).pacc()[ph] += globaltimer() - (t0); \
   } while (0)
 
 // ---- bulk asynchronous copies and mbarriers
@@ -136,13 +136,27 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// the same, letting the thread sleep up to hint_ns while the phase is incomplete (it wakes when the phase
+// completes), so that waiting warps leave the issue slots to the computing ones
+__device__ __forceinline__ bool mbar_try_wait_sleep(unsigned long long* bar, unsigned parity, unsigned hint_ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
 // bounded wait for an mbarrier phase
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, unsigned long long limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = globaltimer();
   for (unsigned it = 1;; ++it) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 0u && globaltimer() - t0 > limit_ns) return false;
+    if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
+    if ((it & 15u) == 0u && globaltimer() - t0 > limit_ns) return false;
   }
 }
 
@@ -153,78 +167,76 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // compiler to address shared memory (shared loads, no aliasing with global stores)
 extern __shared__ __align__(128) unsigned char smem_raw[];
 
+// Fixed part of the shared-memory layout: compile-time offsets, so that no registers hold its addresses.
+__host__ __device__ constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+namespace smo {
+constexpr size_t act = 0;                                                    // int [kMaxSolves] action of each solve
+constexpr size_t c1 = act + a16(sizeof(int) * kMaxSolves);                  // double [kMaxSolves] beta (S) / alpha (X, R)
+constexpr size_t c2 = c1 + a16(sizeof(double) * kMaxSolves);                // double [kMaxSolves] alpha_{k-1} (x update)
+constexpr size_t rnorm = c2 + a16(sizeof(double) * kMaxSolves);             // double [kMaxSolves] rhsNorm
+constexpr size_t norm = rnorm + a16(sizeof(double) * kMaxSolves);           // double [kMaxSolves] cg2dNorm
+constexpr size_t has_alpha = norm + a16(sizeof(double) * kMaxSolves);       // int [kMaxSolves]
+constexpr size_t opp = has_alpha + a16(sizeof(int) * kMaxSolves);           // int [kMaxOps] operator in the pass
+constexpr size_t rowsum = opp + a16(sizeof(int) * kMaxOps);                 // double [kMaxStages][4][kWarps]
+constexpr size_t tsum = rowsum + a16(sizeof(double) * kMaxStages * 4 * kWarps);   // double [kMaxTiles]
+constexpr size_t misc = tsum + a16(sizeof(double) * kMaxTiles);             // int [4]
+constexpr size_t full = misc + a16(sizeof(int) * 4);                        // mbarrier [kMaxStages]
+constexpr size_t empty = full + a16(8 * kMaxStages);                        // mbarrier [kMaxStages]
+constexpr size_t pacc = empty + a16(8 * kMaxStages);                        // u64 [8]
+constexpr size_t opn = pacc + a16(8 * 8);                                   // unsigned [kMaxOps]
+constexpr size_t uacc = opn + a16(sizeof(unsigned) * kMaxOps);              // double [4]
+constexpr size_t ucnt = uacc + a16(sizeof(double) * 4);                     // unsigned [kMaxOps]
+constexpr size_t utab = ucnt + a16(sizeof(unsigned) * kMaxOps);             // int2 [kMaxUnitsPerCta]
+constexpr size_t pend = utab + a16(sizeof(int2) * kMaxUnitsPerCta);         // int4 [kMaxStages]
+constexpr size_t end = pend + a16(sizeof(int4) * kMaxStages);               // then prod (FORTRAN order)
+}  // namespace smo
+
+// Views of the shared memory. Fixed arrays:
+//   act, c1, c2, rnorm, norm, has_alpha   per solve: action in the pass, pass coefficients, rhsNorm, cg2dNorm,
+//                                          whether alpha_{k-1} exists
+//   opp, opn, ucnt                         per operator: in the pass; passes with sums completed (its counter
+//                                          target); units this CTA completed in the pass
+//   rowsum                                 row sums of the chunk in each stage [stage][4 sums][kWarps]
+//   tsum, misc                             reducer scratch; [0] barrier ok, [2] reducer ok, [3] units in utab
+//   full, empty                            stage mbarriers: copies landed / compute warps done with the stage
+//   pacc, uacc                             phase times (profiling); the current unit's partial sums
+//   utab, pend                             this CTA's work units; the chunk in each stage awaiting its row sums
+// then prod (FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]) and the stage buffers at `stage` (kMaxStages x
+// stage_bytes, 128-aligned; also the direct-pass staging area and the reducer's gather buffer).
 struct Smem {
-  int* act;          // [kMaxSolves] action of each solve in the current pass
-  double* c1;        // [kMaxSolves] pass coefficient (beta in S, alpha in X and R)
-  double* c2;        // [kMaxSolves] alpha_{k-1} for the deferred x update
-  double* rnorm;     // [kMaxSolves] rhsNorm
-  double* norm;      // [kMaxSolves] cg2dNorm
-  int* has_alpha;    // [kMaxSolves]
-  int* opp;          // [kMaxOps] operator takes part in the pass
-  double* rowsum;    // [kMaxStages][4 sums][kWarps] row sums of the chunk in each stage
-  double* tsum;      // [kMaxTiles]
-  int* misc;         // [4]: barrier ok flag, -, reducer ok flag, number of units in the unit table
-  unsigned long long* full;   // [kMaxStages] stage mbarriers: the chunk's copies have landed
-  unsigned long long* empty;  // [kMaxStages] stage mbarriers: the compute warps are done with the stage
-  unsigned long long* pacc;   // [8] phase times of this CTA (profiling)
-  unsigned* opn;            // [kMaxOps] passes with sums each operator has completed (its counter target)
-  double* uacc;             // [4] the current unit's partial sums (slot, kind)
-  unsigned* ucnt;           // [kMaxOps] units this CTA completed in the current pass, per operator
-  int2* utab;               // [kMaxUnitsPerCta] this CTA's work units (unit_pack)
-  int4* pend;               // [kMaxStages] chunk in each stage awaiting its row sums: unit, jc, nr
-  double* prod;      // FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]
-  unsigned stage;    // offset of the stage buffers (kMaxStages x stage_bytes, 128-aligned) in smem_raw; also
-                     // the direct-pass staging area and the reducer's gather buffer
+  unsigned stage;
+  template <class T>
+  __device__ __forceinline__ static T* at(size_t off) { return reinterpret_cast<T*>(smem_raw + off); }
+  __device__ __forceinline__ int* act() const { return at<int>(smo::act); }
+  __device__ __forceinline__ double* c1() const { return at<double>(smo::c1); }
+  __device__ __forceinline__ double* c2() const { return at<double>(smo::c2); }
+  __device__ __forceinline__ double* rnorm() const { return at<double>(smo::rnorm); }
+  __device__ __forceinline__ double* norm() const { return at<double>(smo::norm); }
+  __device__ __forceinline__ int* has_alpha() const { return at<int>(smo::has_alpha); }
+  __device__ __forceinline__ int* opp() const { return at<int>(smo::opp); }
+  __device__ __forceinline__ double* rowsum() const { return at<double>(smo::rowsum); }
+  __device__ __forceinline__ double* tsum() const { return at<double>(smo::tsum); }
+  __device__ __forceinline__ int* misc() const { return at<int>(smo::misc); }
+  __device__ __forceinline__ unsigned long long* full() const { return at<unsigned long long>(smo::full); }
+  __device__ __forceinline__ unsigned long long* empty() const { return at<unsigned long long>(smo::empty); }
+  __device__ __forceinline__ unsigned long long* pacc() const { return at<unsigned long long>(smo::pacc); }
+  __device__ __forceinline__ unsigned* opn() const { return at<unsigned>(smo::opn); }
+  __device__ __forceinline__ double* uacc() const { return at<double>(smo::uacc); }
+  __device__ __forceinline__ unsigned* ucnt() const { return at<unsigned>(smo::ucnt); }
+  __device__ __forceinline__ int2* utab() const { return at<int2>(smo::utab); }
+  __device__ __forceinline__ int4* pend() const { return at<int4>(smo::pend); }
+  __device__ __forceinline__ double* prod() const { return at<double>(smo::end); }
 };
 
-__host__ __device__ inline size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
-
-size_t fixed_smem_bytes(int max_ni, int serial) {
-  size_t s = 0;
-  s += a16(sizeof(int) * kMaxSolves);
-  s += 4 * a16(sizeof(double) * kMaxSolves);
-  s += a16(sizeof(int) * kMaxSolves);
-  s += a16(sizeof(int) * kMaxOps);
-  s += a16(sizeof(double) * kMaxStages * 4 * kWarps);
-  s += a16(sizeof(double) * kMaxTiles);
-  s += a16(sizeof(int) * 4);
-  s += 2 * a16(sizeof(unsigned long long) * kMaxStages);
-  s += a16(sizeof(unsigned long long) * 8);
-  s += a16(sizeof(unsigned) * kMaxOps);
-  s += a16(sizeof(double) * 4);
-  s += a16(sizeof(unsigned) * kMaxOps);
-  s += a16(sizeof(int2) * kMaxUnitsPerCta);
-  s += a16(sizeof(int4) * kMaxStages);
-  if (serial) s += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni);
-  return (s + 127) & ~size_t(127);
+static size_t prod_bytes(int max_ni, int serial) {
+  return serial ? a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni) : 0;
 }
+size_t fixed_smem_bytes(int max_ni, int serial) { return (smo::end + prod_bytes(max_ni, serial) + 127) & ~size_t(127); }
 
 __device__ inline Smem carve(int max_ni, int serial) {
-  unsigned char* base = smem_raw;
   Smem m;
-  size_t o = 0;
-  m.act = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxSolves);
-  m.c1 = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
-  m.c2 = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
-  m.rnorm = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
-  m.norm = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxSolves);
-  m.has_alpha = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxSolves);
-  m.opp = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * kMaxOps);
-  m.rowsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxStages * 4 * kWarps);
-  m.tsum = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * kMaxTiles);
-  m.misc = reinterpret_cast<int*>(base + o); o += a16(sizeof(int) * 4);
-  m.full = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * kMaxStages);
-  m.empty = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * kMaxStages);
-  m.pacc = reinterpret_cast<unsigned long long*>(base + o); o += a16(sizeof(unsigned long long) * 8);
-  m.opn = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
-  m.uacc = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 4);
-  m.ucnt = reinterpret_cast<unsigned*>(base + o); o += a16(sizeof(unsigned) * kMaxOps);
-  m.utab = reinterpret_cast<int2*>(base + o); o += a16(sizeof(int2) * kMaxUnitsPerCta);
-  m.pend = reinterpret_cast<int4*>(base + o); o += a16(sizeof(int4) * kMaxStages);
-  m.prod = nullptr;
-  if (serial) { m.prod = reinterpret_cast<double*>(base + o); o += a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni); }
-  o = (o + 127) & ~size_t(127);
-  m.stage = (unsigned)o;
+  const size_t pb = serial ? a16(sizeof(double) * 2 * 2 * kWarps * (size_t)max_ni) : 0;
+  m.stage = (unsigned)((smo::end + pb + 127) & ~size_t(127));
   return m;
 }
 
@@ -351,12 +363,12 @@ struct Slots {
   const Smem* sm;
   int rid0, nrhs;
   __device__ __forceinline__ int rid(int s) const { return rid0 + s; }
-  __device__ __forceinline__ int act(int s) const { return s < nrhs ? sm->act[rid0 + s] : (int)A_NONE; }
-  __device__ __forceinline__ double c1(int s) const { return sm->c1[rid0 + s]; }
-  __device__ __forceinline__ double c2(int s) const { return sm->c2[rid0 + s]; }
-  __device__ __forceinline__ double rnorm(int s) const { return sm->rnorm[rid0 + s]; }
-  __device__ __forceinline__ double norm(int s) const { return sm->norm[rid0 + s]; }
-  __device__ __forceinline__ int has_alpha(int s) const { return sm->has_alpha[rid0 + s]; }
+  __device__ __forceinline__ int act(int s) const { return s < nrhs ? sm->act()[rid0 + s] : (int)A_NONE; }
+  __device__ __forceinline__ double c1(int s) const { return sm->c1()[rid0 + s]; }
+  __device__ __forceinline__ double c2(int s) const { return sm->c2()[rid0 + s]; }
+  __device__ __forceinline__ double rnorm(int s) const { return sm->rnorm()[rid0 + s]; }
+  __device__ __forceinline__ double norm(int s) const { return sm->norm()[rid0 + s]; }
+  __device__ __forceinline__ int has_alpha(int s) const { return sm->has_alpha()[rid0 + s]; }
 };
 __device__ __forceinline__ Slots slots_of(const GroupDev& g, int inst, const Smem& sm) {
   Slots q;
@@ -383,7 +395,7 @@ __device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, con
   double r2 = 0.0, r3 = 0.0;
   if (g.nrhs > 1) { r2 = butterfly(lp.v[2]); r3 = butterfly(lp.v[3]); }
   if (lane == 0) {
-    double* rs = sm.rowsum + st * 4 * kWarps;
+    double* rs = sm.rowsum() + st * 4 * kWarps;
     rs[0 * kWarps + warp] = r0;
     rs[1 * kWarps + warp] = r1;
     rs[2 * kWarps + warp] = r2;
@@ -399,13 +411,13 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
   const int lane = threadIdx.x & 31;
   const int s = lane >> 1, q = lane & 1;
   if (lane < 4 && q < (s == 0 ? ns0 : ns1)) {
-    double a = first ? 0.0 : sm.uacc[lane];
+    double a = first ? 0.0 : sm.uacc()[lane];
     if (kp.serial) {
-      const double* pr = sm.prod + (lane * kWarps) * kp.max_ni;
+      const double* pr = sm.prod() + (lane * kWarps) * kp.max_ni;
       for (int w = 0; w < nr; ++w)
         for (int i = 0; i < g.tp.ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
     } else {
-      const double* rs = sm.rowsum + (st * 4 + lane) * kWarps;
+      const double* rs = sm.rowsum() + (st * 4 + lane) * kWarps;
       double v[kWarps];
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) v[w] = rs[w];
@@ -413,7 +425,7 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
       for (int w = 0; w < kWarps; ++w)
         if (w < nr) a = add(a, v[w]);
     }
-    sm.uacc[lane] = a;
+    sm.uacc()[lane] = a;
   }
   __syncwarp();
 }
@@ -427,11 +439,11 @@ __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g
                                             const Smem& sm) {
   if ((threadIdx.x & 31) != 0 || ns0 + ns1 == 0) return;
   const int rid0 = g.rhs_base + inst * g.nrhs;
-  if (ns0 > 0) stcg(kp.part + ((size_t)rid0 * 2 + 0) * kp.part_units + lu, sm.uacc[0]);
-  if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, sm.uacc[1]);
-  if (ns1 > 0) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 0) * kp.part_units + lu, sm.uacc[2]);
-  if (ns1 > 1) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 1) * kp.part_units + lu, sm.uacc[3]);
-  sm.ucnt[g.op_base + inst] += 1u;
+  if (ns0 > 0) stcg(kp.part + ((size_t)rid0 * 2 + 0) * kp.part_units + lu, sm.uacc()[0]);
+  if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, sm.uacc()[1]);
+  if (ns1 > 0) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 0) * kp.part_units + lu, sm.uacc()[2]);
+  if (ns1 > 1) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 1) * kp.part_units + lu, sm.uacc()[3]);
+  sm.ucnt()[g.op_base + inst] += 1u;
 }
 // every CTA, end of its units: add its unit counts to the operators' counters (release: the partials written
 // before are visible to whoever observes the count)
@@ -439,10 +451,10 @@ __device__ __forceinline__ void publish_counts(const KParams& kp, const Smem& sm
   if (threadIdx.x == 0 || threadIdx.x == kProducer * 32) __threadfence();   // the writers of the unit partials
   __syncthreads();
   for (int op = threadIdx.x; op < kp.total_ops; op += kThreads) {
-    const unsigned c = sm.ucnt[op];
+    const unsigned c = sm.ucnt()[op];
     if (c) {
       red_release_add(&kp.cnt[op], c);
-      sm.ucnt[op] = 0u;
+      sm.ucnt()[op] = 0u;
     }
   }
   __syncthreads();
@@ -460,7 +472,7 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
     const GroupDev& g = kp.g[gi];
     for (int inst = 0; inst < g.count; ++inst) {
       const int op = g.op_base + inst;
-      if (!sm.opp[op]) continue;
+      if (!sm.opp()[op]) continue;
       const int ulast = g.unit_base + inst * g.units + g.units - 1;
       if (ulast % (int)gridDim.x != (int)blockIdx.x) continue;
       const Slots si = slots_of(g, inst, sm);
@@ -469,7 +481,7 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
       const int nl = ns0 + ns1;
       if (!nl) continue;
       if (tid == 0) {
-        const unsigned target = (sm.opn[op] + 1u) * (unsigned)g.units;
+        const unsigned target = (sm.opn()[op] + 1u) * (unsigned)g.units;
         const unsigned long long t0 = globaltimer();
         int good = 1;
         for (unsigned spins = 0;; ++spins) {
@@ -482,10 +494,10 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
           }
         }
         __threadfence();
-        sm.misc[2] = good;
+        sm.misc()[2] = good;
       }
       __syncthreads();
-      if (!sm.misc[2]) { ok = false; break; }
+      if (!sm.misc()[2]) { ok = false; break; }
       const int U = g.units;
       for (int idx = tid; idx < nl * U; idx += kThreads) {
         const int l = idx / U, u = idx - (idx / U) * U;
@@ -498,12 +510,12 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
           for (int tt = lane; tt < g.tp.T; tt += 32) {
             double a = 0.0;
             for (int b = 0; b < g.nblk; ++b) a = add(a, buf[l * U + tt * g.nblk + b]);
-            sm.tsum[tt] = a;
+            sm.tsum()[tt] = a;
           }
           __syncwarp();
           if (lane == 0) {
             double a = 0.0;
-            for (int tt = 0; tt < g.tp.T; ++tt) a = add(a, sm.tsum[tt]);
+            for (int tt = 0; tt < g.tp.T; ++tt) a = add(a, sm.tsum()[tt]);
             const int sl = l < ns0 ? 0 : 1, ql = l < ns0 ? l : l - ns0;
             stcg(hist_ptr(kp, si.rid(sl), hist_kind(pt, ql), hidx), a);
           }
@@ -516,14 +528,14 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
   // every CTA: operators that produced sums in this pass expect one more round of unit counts
   __syncthreads();
   for (int op = tid; op < kp.total_ops; op += kThreads) {
-    if (!sm.opp[op]) continue;
+    if (!sm.opp()[op]) continue;
     int gi = 0;
     while (gi + 1 < kp.ngroups && op >= kp.g[gi + 1].op_base) ++gi;
     const GroupDev& g = kp.g[gi];
     const int inst = op - g.op_base;
     int any = 0;
-    for (int s = 0; s < g.nrhs; ++s) any |= nsums(pt, sm.act[g.rhs_base + inst * g.nrhs + s]);
-    if (any) sm.opn[op] += 1u;
+    for (int s = 0; s < g.nrhs; ++s) any |= nsums(pt, sm.act()[g.rhs_base + inst * g.nrhs + s]);
+    if (any) sm.opn()[op] += 1u;
   }
   __syncthreads();
   return ok;
@@ -640,7 +652,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
             p1 = bn;
           }
           if (kp.serial && pt != P_MAX) {
-            double* pr = sm.prod + ((s * 2 + 0) * kWarps + warp) * kp.max_ni;
+            double* pr = sm.prod() + ((s * 2 + 0) * kWarps + warp) * kp.max_ni;
             pr[i] = p0;
             pr[kWarps * kp.max_ni + i] = p1;
           } else if (s == 0) {
@@ -687,7 +699,7 @@ __device__ bool run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
     const GroupDev& g = kp.g[gi];
     const int rel = u - g.unit_base;
     const int inst = rel / g.units;
-    if (!sm.opp[g.op_base + inst]) continue;
+    if (!sm.opp()[g.op_base + inst]) continue;
     process_unit_direct<MIXED>(kp, g, inst, rel - inst * g.units, pt, sm);
   }
   const bool ok = reduce_pass(kp, pt, 0, sm);
@@ -725,7 +737,7 @@ __device__ void init_x_ring(const KParams& kp, const Smem& sm) {
         src = tp.nbr[2 * T * nj + side * T * ni + r];
       }
       const double* x0 = g.x0[s] + inst * g.pad_elems;
-      const double rn = sm.rnorm[g.rhs_base + inst * g.nrhs + s];
+      const double rn = sm.rnorm()[g.rhs_base + inst * g.nrhs + s];
       const double v = (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), rn)
                                   : __ldg(x0 + ((long long)t * tp.npy + (j + tp.OLy)) * tp.npx + (i + tp.OLx));
       vec_ptr<double>(g, inst, s, V_X)[vidx(tp, t, j, i)] = v;
@@ -742,7 +754,7 @@ struct Unit {
   int gi, inst, lu, t, j0, j1;
 };
 __device__ __forceinline__ Unit unit_at(const Smem& sm, int ui) {
-  const int2 e = sm.utab[ui];
+  const int2 e = sm.utab()[ui];
   Unit u;
   u.gi = e.x & 3; u.inst = (e.x >> 2) & 255; u.lu = (unsigned)e.x >> 10;
   u.t = e.y & 255; u.j0 = (e.y >> 8) & 2047; u.j1 = (unsigned)e.y >> 19;
@@ -761,9 +773,9 @@ __device__ void build_unit_table(const KParams& kp, const Smem& sm) {
     const int t = lu / g.nblk, blk = lu - t * g.nblk;
     const int R = kp.serial ? g.tp.nj : kp.rows_per_block;
     const int j0 = blk * R, j1 = min(g.tp.nj, j0 + R);
-    sm.utab[q] = make_int2(gi | (inst << 2) | (lu << 10), t | (j0 << 8) | (j1 << 19));
+    sm.utab()[q] = make_int2(gi | (inst << 2) | (lu << 10), t | (j0 << 8) | (j1 << 19));
   }
-  if (threadIdx.x == 0) sm.misc[3] = n > 0 ? n : 0;
+  if (threadIdx.x == 0) sm.misc()[3] = n > 0 ? n : 0;
 }
 
 // position in this CTA's chunk sequence of a pass: unit ui of the table, first row jc; units of operators that
@@ -772,10 +784,10 @@ struct Cursor {
   int ui, jc;
 };
 __device__ __forceinline__ bool cursor_unit(const KParams& kp, const Smem& sm, Cursor& c) {
-  const int n = sm.misc[3];
+  const int n = sm.misc()[3];
   for (++c.ui; c.ui < n; ++c.ui) {
     const Unit u = unit_at(sm, c.ui);
-    if (sm.opp[kp.g[u.gi].op_base + u.inst]) {
+    if (sm.opp()[kp.g[u.gi].op_base + u.inst]) {
       c.jc = u.j0;
       return true;
     }
@@ -827,10 +839,10 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
   const int lane = threadIdx.x & 31;
   const StageLay& L = kp.lay[c.gi][pt];
   unsigned char* sb = smem_raw + sm.stage + st * kp.stage_bytes;
-  unsigned long long* bar = &sm.full[st];
+  unsigned long long* bar = &sm.full()[st];
   const int rid0 = g.rhs_base + c.inst * g.nrhs;
-  const bool act0 = sm.act[rid0] == A_ACTIVE;
-  const bool act1 = g.nrhs > 1 && sm.act[rid0 + 1] == A_ACTIVE;
+  const bool act0 = sm.act()[rid0] == A_ACTIVE;
+  const bool act1 = g.nrhs > 1 && sm.act()[rid0 + 1] == A_ACTIVE;
   const bool any = act0 || act1;
   const int T = tp.T, nj = tp.nj, ni = tp.ni, P = tp.P;
   const bool bottom = c.jc == 0, top = c.jc + c.nr == nj;
@@ -872,7 +884,7 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
     }
   } else if (lane < 12) {
     const int s = lane - 10;
-    if (pt == P_S && s < g.nrhs && (s == 0 ? act0 : act1) && sm.has_alpha[rid0 + s]) {
+    if (pt == P_S && s < g.nrhs && (s == 0 ? act0 : act1) && sm.has_alpha()[rid0 + s]) {
       src = vec_ptr<const char>(g, c.inst, s, V_X) + ((long long)c.t * (nj + 2) + c.jc + 1) * P * 8;
       dst = sb + L.xo[s];
       bytes = (unsigned)(c.nr * P * 8);
@@ -884,10 +896,14 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
   if (bytes) bulk_g2s(dst, src, bytes, bar);
 }
 
-// compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m. In shared memory
-// point (w, i) of a vector is element (w + 1) P + i + 1 (its neighbours at -1, +1, -P, +P) and of the packed
-// coefficients element w 3 ldc + i (columns: W/pW, +ldc S/pS, +2 ldc C/pC; east face +1, north face +3 ldc).
-template <bool MIXED>
+// compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m, m = 0, 1, ...
+// (MAXM > 0: exactly MAXM column steps, unrolled; 0: any width). Both right-hand sides of the instance are
+// processed in the same step, sharing the coefficient loads. In shared memory point (w, i) of a vector is
+// element (w + 1) P + i + 1 (its neighbours at -1, +1, -P, +P) and of the packed coefficients element
+// w 3 ldc + i (columns: W/pW, +ldc S/pS, +2 ldc C/pC; east face +1, north face +3 ldc). A point pushes its new
+// values to the rings of the tiles that read it when it lies on the tile's edge (every point of the first and
+// last row, the first and last point of the others).
+template <bool MIXED, int MAXM>
 __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si, int st,
                                const Smem& sm) {
   Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
@@ -904,16 +920,35 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   const long long grow = ((long long)t * (nj + 2) + j + 1) * P + 1;   // element of (t, j, 0)
   const long long pe = g.pad_elems;
   const long long prow = (long long)c.inst * pe + ((long long)t * tp.npy + j + tp.OLy) * tp.npx + tp.OLx;
+  const bool er = (j == 0) | (j == nj - 1);
   PushTab ptab;
   ptab.twe = reinterpret_cast<const int4*>(sb + L.twe);
   ptab.ts = reinterpret_cast<const int2*>(sb + L.ts);
   ptab.tn = reinterpret_cast<const int2*>(sb + L.tn);
   ptab.ni = ni;
   ptab.nj = nj;
+  const int act0 = si.act(0), act1 = si.act(1);
 
+  // pass S after convergence: the pending x update, un-normalised (cg2d.py:254, 266)
+  for (int s = 0; s < g.nrhs; ++s) {
+    if ((s == 0 ? act0 : act1) != A_FIN) continue;
+    const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
+    const double* x = vec_ptr<double>(g, c.inst, s, V_X);
+    for (int i = lane; i < ni; i += 32) {
+      double xv = ldcg(x + grow + i);
+      if (si.has_alpha(s)) xv = add(xv, mul(si.c2(s), (double)ldcg(so + grow + i)));
+      const double xf = __ddiv_rn(xv, si.rnorm(s));
+      g.x_out[s][prow + i] = xf;
+      if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
+    }
+  }
+  const bool on0 = act0 == A_ACTIVE, on1 = act1 == A_ACTIVE;
+  if (!on0 && !on1) return lp;
+
+  // products of slot s at point i into the lane partials (ROWBLOCK) or the product rows (FORTRAN)
   auto emit = [&](int s, int i, double p0, double p1) {
     if (kp.serial) {
-      double* pr = sm.prod + ((s * 2) * kWarps + w) * kp.max_ni;
+      double* pr = sm.prod() + ((s * 2) * kWarps + w) * kp.max_ni;
       pr[i] = p0;
       pr[kWarps * kp.max_ni + i] = p1;
     } else if (s == 0) {
@@ -924,105 +959,135 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       lp.v[3] = add(lp.v[3], p1);
     }
   };
-
-  for (int s = 0; s < g.nrhs; ++s) {
-    const int a = si.act(s);
-    if (a == A_NONE) continue;
-    if (a == A_FIN) {
-      // pass S after convergence: the pending x update, un-normalised (cg2d.py:254, 266)
-      const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
-      const double* x = vec_ptr<double>(g, c.inst, s, V_X);
-      for (int i = lane; i < ni; i += 32) {
-        double xv = ldcg(x + grow + i);
-        if (si.has_alpha(s)) xv = add(xv, mul(si.c2(s), (double)ldcg(so + grow + i)));
-        const double xf = __ddiv_rn(xv, si.rnorm(s));
-        g.x_out[s][prow + i] = xf;
-        if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
+  // runs f(i) for this lane's columns
+  auto columns = [&](auto&& f) {
+    if (MAXM > 0) {
+#pragma unroll
+      for (int m = 0; m < (MAXM > 0 ? MAXM : 1); ++m) {
+        const int i = lane + 32 * m;
+        if (i < ni) f(i);
       }
-      continue;
+    } else {
+      for (int i = lane; i < ni; i += 32) f(i);
     }
-    const int cb0 = w * CR;
-    if (pt == P_S) {
-      const V* zr = reinterpret_cast<const V*>(sb + L.vec[s][0]);
-      const V* so = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      const double* xo = reinterpret_cast<const double*>(sb + L.xo[s]);
-      const C* cp = reinterpret_cast<const C*>(sb + L.coef);
-      const double beta = si.c1(s), alpha_prev = si.c2(s);
-      const bool upd = si.has_alpha(s) != 0;
-      V* s_out = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
-      V* q_out = vec_ptr<V>(g, c.inst, s, V_Q);
-      double* x_out = vec_ptr<double>(g, c.inst, s, V_X);
-      // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike (MIXED: in FP32)
-      const V betav = (V)beta;
-      auto sn = [&](V zz, V ss) -> V { return add(zz, mul(betav, ss)); };
-      for (int i = lane; i < ni; i += 32) {
-        const int rc = (w + 1) * P + i + 1;
-        const V vc = sn(zr[rc], so[rc]);
-        const V vw = sn(zr[rc - 1], so[rc - 1]);
-        const V ve = sn(zr[rc + 1], so[rc + 1]);
-        const V vs = sn(zr[rc - P], so[rc - P]);
-        const V vn = sn(zr[rc + P], so[rc + P]);
-        const int cr = cb0 + i;
-        const V q = (V)op_A<C>(cp[cr], cp[cr + 1], cp[cr + CL], cp[cr + CL + CR], cp[cr + 2 * CL], (C)vw, (C)ve,
-                               (C)vs, (C)vn, (C)vc);                                          // cg2d.py:251
-        stcg(s_out + grow + i, vc);
-        push_s(ptab, s_out, j, w, i, vc);
-        stcg(q_out + grow + i, q);
-        push_s(ptab, q_out, j, w, i, q);
-        if (upd) {
-          const double xn = add(xo[w * P + i + 1], mul(alpha_prev, (double)so[rc]));          // cg2d.py:254
-          stcg(x_out + grow + i, xn);
-          if (MIXED) push_s(ptab, x_out, j, w, i, xn);   // x's neighbours are read by the replacement pass only
-        }
-        emit(s, i, mul((double)vc, (double)q), 0.0);                                          // cg2d.py:252
+  };
+  const C* cp = reinterpret_cast<const C*>(sb + L.coef);
+
+  if (pt == P_S) {
+    // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike (MIXED: in FP32);
+    // q_k = A s_k (cg2d.py:251); x_k = x_{k-1} + alpha_{k-1} s_{k-1} (cg2d.py:254); s_k.q_k (cg2d.py:252)
+    struct SlotS {
+      const V *zr, *so;
+      const double* xo;
+      V *s_out, *q_out;
+      double* x_out;
+      V beta;
+      double alpha_prev;
+      bool upd;
+    };
+    auto slot = [&](int s) {
+      SlotS q;
+      q.zr = reinterpret_cast<const V*>(sb + L.vec[s][0]);
+      q.so = reinterpret_cast<const V*>(sb + L.vec[s][1]);
+      q.xo = reinterpret_cast<const double*>(sb + L.xo[s]);
+      q.s_out = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0) + grow;
+      q.q_out = vec_ptr<V>(g, c.inst, s, V_Q) + grow;
+      q.x_out = vec_ptr<double>(g, c.inst, s, V_X) + grow;
+      q.beta = (V)si.c1(s);
+      q.alpha_prev = si.c2(s);
+      q.upd = si.has_alpha(s) != 0;
+      return q;
+    };
+    const SlotS q0 = slot(0), q1 = slot(g.nrhs > 1 ? 1 : 0);
+    auto body = [&](const SlotS& q, int s, int i, int rc, C aw, C ae, C as, C an, C ac, bool edge) {
+      auto sn = [&](V zz, V ss) -> V { return add(zz, mul(q.beta, ss)); };
+      const V vc = sn(q.zr[rc], q.so[rc]);
+      const V vw = sn(q.zr[rc - 1], q.so[rc - 1]);
+      const V ve = sn(q.zr[rc + 1], q.so[rc + 1]);
+      const V vs = sn(q.zr[rc - P], q.so[rc - P]);
+      const V vn = sn(q.zr[rc + P], q.so[rc + P]);
+      const V qv = (V)op_A<C>(aw, ae, as, an, ac, (C)vw, (C)ve, (C)vs, (C)vn, (C)vc);
+      stcg(q.s_out + i, vc);
+      stcg(q.q_out + i, qv);
+      double xn = 0.0;
+      if (q.upd) {
+        xn = add(q.xo[w * P + i + 1], mul(q.alpha_prev, (double)q.so[rc]));
+        stcg(q.x_out + i, xn);
       }
-    } else if (pt == P_X) {
-      const V* ro = reinterpret_cast<const V*>(sb + L.vec[s][0]);
-      const V* qv = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      const C* cp = reinterpret_cast<const C*>(sb + L.coef);
-      const double alpha = si.c1(s);
-      V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
-      V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
-      // r_{k+1} = r_k - alpha_k q_k (cg2d.py:255) (MIXED: in FP32)
-      const V alphav = (V)alpha;
-      auto rn = [&](V rr, V qq) -> V { return sub(rr, mul(alphav, qq)); };
-      for (int i = lane; i < ni; i += 32) {
-        const int rc = (w + 1) * P + i + 1;
-        const V vc = rn(ro[rc], qv[rc]);
-        const V vw = rn(ro[rc - 1], qv[rc - 1]);
-        const V ve = rn(ro[rc + 1], qv[rc + 1]);
-        const V vs = rn(ro[rc - P], qv[rc - P]);
-        const V vn = rn(ro[rc + P], qv[rc + P]);
-        const int cr = cb0 + i;
-        const V z = (V)op_M<C>(cp[cr + 2 * CL], cp[cr], cp[cr + 1], cp[cr + CL], cp[cr + CL + CR], (C)vc, (C)vw,
-                               (C)ve, (C)vs, (C)vn);                                          // cg2d.py:245
-        stcg(r_out + grow + i, vc);
-        push_s(ptab, r_out, j, w, i, vc);
-        stcg(z_out + grow + i, z);
-        push_s(ptab, z_out, j, w, i, z);
-        emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));                 // cg2d.py:256, 246
+      if (edge) {
+        push_s(ptab, q.s_out - grow, j, w, i, vc);
+        push_s(ptab, q.q_out - grow, j, w, i, qv);
+        if (MIXED && q.upd) push_s(ptab, q.x_out - grow, j, w, i, xn);   // x's neighbours: replacement pass only
       }
-    } else if (pt == P_Z) {
-      const V* rr_ = reinterpret_cast<const V*>(sb + L.vec[s][0]);
-      const C* cp = reinterpret_cast<const C*>(sb + L.coef);
-      V* z_out = vec_ptr<V>(g, c.inst, s, V_Z);
-      for (int i = lane; i < ni; i += 32) {
-        const int rc = (w + 1) * P + i + 1;
-        const V vc = rr_[rc];
-        const int cr = cb0 + i;
-        const V z = (V)op_M<C>(cp[cr + 2 * CL], cp[cr], cp[cr + 1], cp[cr + CL], cp[cr + CL + CR], (C)vc,
-                               (C)rr_[rc - 1], (C)rr_[rc + 1], (C)rr_[rc - P], (C)rr_[rc + P]);
-        stcg(z_out + grow + i, z);
-        push_s(ptab, z_out, j, w, i, z);
-        emit(s, i, mul((double)z, (double)vc), 0.0);
+      emit(s, i, mul((double)vc, (double)qv), 0.0);
+    };
+    columns([&](int i) {
+      const int rc = (w + 1) * P + i + 1;
+      const int cr = w * CR + i;
+      const C aw = cp[cr], ae = cp[cr + 1], as = cp[cr + CL], an = cp[cr + CL + CR], ac = cp[cr + 2 * CL];
+      const bool edge = er | (i == 0) | (i == ni - 1);
+      if (on0) body(q0, 0, i, rc, aw, ae, as, an, ac, edge);
+      if (on1) body(q1, 1, i, rc, aw, ae, as, an, ac, edge);
+    });
+  } else if (pt == P_X || pt == P_Z) {
+    // X: r_{k+1} = r_k - alpha_k q_k (cg2d.py:255, MIXED: in FP32) at the point and its neighbours;
+    //    z_{k+1} = M r_{k+1} (cg2d.py:245); r.r and z.r (cg2d.py:256, 246)
+    // Z: z = M r and z.r
+    struct SlotX {
+      const V *ro, *qv;
+      V *r_out, *z_out;
+      V alpha;
+    };
+    const bool xp = pt == P_X;
+    auto slot = [&](int s) {
+      SlotX q;
+      q.ro = reinterpret_cast<const V*>(sb + L.vec[s][0]);
+      q.qv = reinterpret_cast<const V*>(sb + L.vec[s][1]);
+      q.r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0) + grow;
+      q.z_out = vec_ptr<V>(g, c.inst, s, V_Z) + grow;
+      q.alpha = (V)si.c1(s);
+      return q;
+    };
+    const SlotX q0 = slot(0), q1 = slot(g.nrhs > 1 ? 1 : 0);
+    auto body = [&](const SlotX& q, int s, int i, int rc, C pw, C pe_, C ps, C pn, C pc, bool edge) {
+      V vc, vw, ve, vs, vn;
+      if (xp) {
+        auto rn = [&](V rr, V qq) -> V { return sub(rr, mul(q.alpha, qq)); };
+        vc = rn(q.ro[rc], q.qv[rc]);
+        vw = rn(q.ro[rc - 1], q.qv[rc - 1]);
+        ve = rn(q.ro[rc + 1], q.qv[rc + 1]);
+        vs = rn(q.ro[rc - P], q.qv[rc - P]);
+        vn = rn(q.ro[rc + P], q.qv[rc + P]);
+      } else {
+        vc = q.ro[rc]; vw = q.ro[rc - 1]; ve = q.ro[rc + 1]; vs = q.ro[rc - P]; vn = q.ro[rc + P];
       }
-    } else {  // P_R: the FP64 true residual b - A x_{k+1}
+      const V z = (V)op_M<C>(pc, pw, pe_, ps, pn, (C)vc, (C)vw, (C)ve, (C)vs, (C)vn);
+      if (xp) stcg(q.r_out + i, vc);
+      stcg(q.z_out + i, z);
+      if (edge) {
+        if (xp) push_s(ptab, q.r_out - grow, j, w, i, vc);
+        push_s(ptab, q.z_out - grow, j, w, i, z);
+      }
+      if (xp) emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));
+      else emit(s, i, mul((double)z, (double)vc), 0.0);
+    };
+    columns([&](int i) {
+      const int rc = (w + 1) * P + i + 1;
+      const int cr = w * CR + i;
+      const C pw = cp[cr], pe_ = cp[cr + 1], ps = cp[cr + CL], pn = cp[cr + CL + CR], pc = cp[cr + 2 * CL];
+      const bool edge = er | (i == 0) | (i == ni - 1);
+      if (on0) body(q0, 0, i, rc, pw, pe_, ps, pn, pc, edge);
+      if (on1) body(q1, 1, i, rc, pw, pe_, ps, pn, pc, edge);
+    });
+  } else {  // P_R: the FP64 true residual b - A x_{k+1}, x_{k+1} = x_k + alpha_k s_k formed on the fly
+    const double* aw = reinterpret_cast<const double*>(sb + L.coef);
+    const double* as = reinterpret_cast<const double*>(sb + L.coef + L.coef_stride);
+    const double* ac = reinterpret_cast<const double*>(sb + L.coef + 2 * L.coef_stride);
+    const int NP = tp.npx, col0 = tp.OLx;
+    for (int s = 0; s < g.nrhs; ++s) {
+      if (!(s == 0 ? on0 : on1)) continue;
       const double* xr = reinterpret_cast<const double*>(sb + L.vec[s][0]);
       const V* sk = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      const double* aw = reinterpret_cast<const double*>(sb + L.coef);
-      const double* as = reinterpret_cast<const double*>(sb + L.coef + L.coef_stride);
-      const double* ac = reinterpret_cast<const double*>(sb + L.coef + 2 * L.coef_stride);
-      const int NP = tp.npx, col0 = tp.OLx;
       const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
       auto x1 = [&](double xx, V ss) -> double { return add(xx, mul(alpha, (double)ss)); };
@@ -1037,7 +1102,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
         const double bn = mul(mul(__ldg(g.b[s] + prow + i), si.norm(s)), si.rnorm(s));
         const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + NP], ac[cr], vw, ve, vs, vn, vc));
         stcg(r_out + grow + i, r);
-        push_s(ptab, r_out, j, w, i, r);
+        if (er | (i == 0) | (i == ni - 1)) push_s(ptab, r_out, j, w, i, r);
         emit(s, i, mul((double)r, (double)r), 0.0);
       }
     }
@@ -1063,12 +1128,12 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
 __device__ bool release_stage(const KParams& kp, int pt, const Smem& sm, int st, Pipe& pp,
                               unsigned long long& t_wait) {
   const unsigned long long t0 = kp.prof ? globaltimer() : 0ull;
-  const bool ok = mbar_wait(&sm.empty[st], (pp.eph >> st) & 1u, kp.timeout_ns);
+  const bool ok = mbar_wait(&sm.empty()[st], (pp.eph >> st) & 1u, kp.timeout_ns);
   pp.eph ^= 1u << st;
   if (kp.prof) t_wait += globaltimer() - t0;
   if (!__all_sync(0xffffffffu, ok)) return false;
   pp.pend &= ~(1u << st);
-  const int4 e = sm.pend[st];
+  const int4 e = sm.pend()[st];
   const Chunk c = chunk_at(kp, sm, e.x, e.y);
   const GroupDev& g = kp.g[c.gi];
   const Slots si = slots_of(g, c.inst, sm);
@@ -1095,7 +1160,7 @@ __device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const S
     const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
     issue_chunk(kp, c, pt, k, hidx, sm, st);
     pp.cph ^= 1u << st;
-    if (lane == 0) sm.pend[st] = make_int4(cur.ui, cur.jc, 0, 0);
+    if (lane == 0) sm.pend()[st] = make_int4(cur.ui, cur.jc, 0, 0);
     __syncwarp();
     pp.pend |= 1u << st;
     st = (st + 1 == ns) ? 0 : st + 1;
@@ -1110,14 +1175,14 @@ __device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const S
     if (lane == 0) note_timeout(kp.gs, 2u, (unsigned)pt);
     // a bounded wait for copies still in flight into this CTA's shared memory
     for (int s2 = 0; s2 < kMaxStages; ++s2)
-      if ((pp.pend >> s2) & 1u) mbar_wait(&sm.full[s2], ((pp.cph >> s2) & 1u) ^ 1u, kp.timeout_ns);
+      if ((pp.pend >> s2) & 1u) mbar_wait(&sm.full()[s2], ((pp.cph >> s2) & 1u) ^ 1u, kp.timeout_ns);
     pp.pend = 0u;
   }
-  if (kp.prof && lane == 0) sm.pacc[PR_ISSUE] += (globaltimer() - t_start) - t_wait;
+  if (kp.prof && lane == 0) sm.pacc()[PR_ISSUE] += (globaltimer() - t_start) - t_wait;
   return ok;
 }
 
-template <bool MIXED>
+template <bool MIXED, int MAXM>
 __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, Pipe& pp) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ns = kp.nstage[pt];
@@ -1126,7 +1191,7 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
   bool have = cursor_first(kp, sm, cur);
   while (have) {
     unsigned long long t0 = PROF_T0(kp);
-    const bool ok = mbar_wait(&sm.full[st], (pp.fph >> st) & 1u, kp.timeout_ns);
+    const bool ok = mbar_wait(&sm.full()[st], (pp.fph >> st) & 1u, kp.timeout_ns);
     pp.fph ^= 1u << st;
     PROF_ADD(kp, sm, PR_MBAR, t0);
     if (!__all_sync(0xffffffffu, ok)) {
@@ -1137,10 +1202,10 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
     const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
     const GroupDev& g = kp.g[c.gi];
     const Slots si = slots_of(g, c.inst, sm);
-    const Lanes lp = compute_chunk<MIXED>(kp, c, pt, k, si, st, sm);
+    const Lanes lp = compute_chunk<MIXED, MAXM>(kp, c, pt, k, si, st, sm);
     if (warp < c.nr && !kp.serial) row_sums(g, lp, sm, st);
     __syncwarp();
-    if (lane == 0) mbar_arrive(&sm.empty[st]);
+    if (lane == 0) mbar_arrive(&sm.empty()[st]);
     PROF_ADD(kp, sm, PR_COMP, t0);
     st = (st + 1 == ns) ? 0 : st + 1;
     have = cursor_next(kp, sm, cur);
@@ -1148,11 +1213,11 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
   return true;
 }
 
-template <bool MIXED>
+template <bool MIXED, int MAXM>
 __device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const Smem& sm, Pipe& pp) {
   bool ok;
   if ((threadIdx.x >> 5) == kProducer) ok = produce_pass(kp, pt, k, hidx, sm, pp);
-  else ok = consume_pass<MIXED>(kp, pt, k, sm, pp);
+  else ok = consume_pass<MIXED, MAXM>(kp, pt, k, sm, pp);
   if (__syncthreads_or(!ok)) return false;
   const unsigned long long t0 = PROF_T0(kp);
   ok = reduce_pass(kp, pt, hidx, sm);
@@ -1174,34 +1239,34 @@ __device__ __forceinline__ void locate(const KParams& kp, int r, int& gi, int& i
 // publish the actions of this pass: act[] for every solve and opp[] for every operator
 __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, double my_c1, double my_c2) {
   const int tid = threadIdx.x;
-  if (tid < kp.total_ops) sm.opp[tid] = 0;
+  if (tid < kp.total_ops) sm.opp()[tid] = 0;
   __syncthreads();
   if (tid < kp.total_rhs) {
-    sm.act[tid] = my_act;
-    sm.c1[tid] = my_c1;
-    sm.c2[tid] = my_c2;
+    sm.act()[tid] = my_act;
+    sm.c1()[tid] = my_c1;
+    sm.c2()[tid] = my_c2;
     if (my_act != A_NONE) {
       int gi, inst, slot;
       locate(kp, tid, gi, inst, slot);
-      sm.opp[kp.g[gi].op_base + inst] = 1;
+      sm.opp()[kp.g[gi].op_base + inst] = 1;
     }
   }
   __syncthreads();
 }
 
-template <bool MIXED>
+template <bool MIXED, int MAXM>
 __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const __grid_constant__ KParams kp) {
   const Smem sm = carve(kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
   unsigned target = (unsigned)kp.test_missing;
   Pipe pp = {0u, 0u, 0u, 0u};
   const unsigned long long t_start = PROF_T0(kp);
-  if (tid < 8) sm.pacc[tid] = 0ull;
-  for (int i = tid; i < kMaxOps; i += kThreads) { sm.opn[i] = 0u; sm.ucnt[i] = 0u; }
+  if (tid < 8) sm.pacc()[tid] = 0ull;
+  for (int i = tid; i < kMaxOps; i += kThreads) { sm.opn()[i] = 0u; sm.ucnt()[i] = 0u; }
   if (tid == 0) {
     for (int s = 0; s < kMaxStages; ++s) {
-      mbar_init(&sm.full[s], 1);          // the producer's arrive (with the copies' byte count)
-      mbar_init(&sm.empty[s], kWarps);    // one arrive per compute warp
+      mbar_init(&sm.full()[s], 1);          // the producer's arrive (with the copies' byte count)
+      mbar_init(&sm.empty()[s], kWarps);    // one arrive per compute warp
     }
     fence_mbar_init();
   }
@@ -1219,9 +1284,9 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     tol2 = g.tol[slot] * g.tol[slot];                      // cg2d.py:219
     rep2 = (kp.replace_above * g.tol[slot]) * (kp.replace_above * g.tol[slot]);
     maxit = g.max_iters[slot];
-    sm.norm[tid] = g.norm_arr ? g.norm_arr[inst] : g.norm;
-    sm.rnorm[tid] = 1.0;
-    sm.has_alpha[tid] = 0;
+    sm.norm()[tid] = g.norm_arr ? g.norm_arr[inst] : g.norm;
+    sm.rnorm()[tid] = 1.0;
+    sm.has_alpha()[tid] = 0;
   }
   int k = 0;
   bool ok = true;
@@ -1229,24 +1294,24 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   // ---- rhsMax = max |b cg2dNorm| (cg2d.py:221-225)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   ok = run_pass_direct<MIXED>(kp, P_MAX, sm);
-  ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+  ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
   if (!ok) goto epilogue;
   if (own) {
     rhsMax = __longlong_as_double((long long)__ldcg(&kp.rmax[tid]));
     rhsNorm = (rhsMax != 0.0) ? __ddiv_rn(1.0, rhsMax) : 1.0;
-    sm.rnorm[tid] = rhsNorm;
+    sm.rnorm()[tid] = rhsNorm;
   }
   // ---- x = x0 rhsNorm, r = b - A x, s = 0, err^2, sumRHS (cg2d.py:226-236)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   init_x_ring(kp, sm);
   ok = run_pass_direct<MIXED>(kp, P_INIT, sm);
-  ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+  ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
   if (!ok) goto epilogue;
   if (own) rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  ok = run_pass_pipe<MIXED>(kp, P_Z, 0, 0, sm, pp);
-  ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+  ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, 0, 0, sm, pp);
+  ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
   if (!ok) goto epilogue;
   if (own) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
 
@@ -1264,13 +1329,13 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
         eta_prev = eta;                                     // cg2d.py:248
       }
     }
-    if (own) sm.has_alpha[tid] = has_alpha;
+    if (own) sm.has_alpha()[tid] = has_alpha;
     set_actions(kp, sm, a, beta, alpha);
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
-    ok = run_pass_pipe<MIXED>(kp, P_S, k, k, sm, pp);
-    ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+    ok = run_pass_pipe<MIXED, MAXM>(kp, P_S, k, k, sm, pp);
+    ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
     if (a == A_ACTIVE) {
@@ -1287,8 +1352,8 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     }
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, alpha, 0.0);
-      ok = run_pass_pipe<MIXED>(kp, P_X, k, k + 1, sm, pp);
-      ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+      ok = run_pass_pipe<MIXED, MAXM>(kp, P_X, k, k + 1, sm, pp);
+      ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
         rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
@@ -1297,16 +1362,16 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     }
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, alpha, 0.0);
-      ok = run_pass_pipe<MIXED>(kp, P_R, k, k + 1, sm, pp);
-      ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+      ok = run_pass_pipe<MIXED, MAXM>(kp, P_R, k, k + 1, sm, pp);
+      ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
         rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
         ++nrep;
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
-      ok = run_pass_pipe<MIXED>(kp, P_Z, k, k + 1, sm, pp);
-      ok = grid_barrier(kp, target, sm.misc, sm.pacc) && ok;
+      ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, k, k + 1, sm, pp);
+      ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
     }
@@ -1342,7 +1407,7 @@ epilogue:
             const int spl = sp % plane;
             const int sj = spl / tp.npx, si_ = spl - (spl / tp.npx) * tp.npx;
             const bool sin = sj >= tp.OLy && sj < tp.OLy + tp.nj && si_ >= tp.OLx && si_ < tp.OLx + tp.ni;
-            const double rn = sm.rnorm[g.rhs_base + in * g.nrhs + s];
+            const double rn = sm.rnorm()[g.rhs_base + in * g.nrhs + s];
             v = sin ? mul(__ldg(x0 + sp), rn) : __ldg(x0 + sp);
           }
           g.x_fortran[s][off] = v;
@@ -1372,7 +1437,7 @@ epilogue:
     unsigned long long* o = kp.prof + 1 + (size_t)blockIdx.x * 8;
     const unsigned long long tot = globaltimer() - t_start;
     unsigned long long acc = 0;   // thread 0's phases (the copy issue runs on the producer warp, beside them)
-    for (int i = 0; i < PR_OTHER; ++i) { o[i] = sm.pacc[i]; if (i != PR_ISSUE) acc += sm.pacc[i]; }
+    for (int i = 0; i < PR_OTHER; ++i) { o[i] = sm.pacc()[i]; if (i != PR_ISSUE) acc += sm.pacc()[i]; }
     o[PR_OTHER] = tot > acc ? tot - acc : 0ull;
     o[PR_TOTAL] = tot;
     if (blockIdx.x == 0) kp.prof[0] = gridDim.x;
@@ -1510,15 +1575,28 @@ static int grid_for(long long work) {
   return (int)b;
 }
 
-cudaError_t solver_occupancy(int mixed, size_t smem, int* blocks_per_sm) {
-  const void* fn = mixed ? (const void*)cg2d_persistent<true> : (const void*)cg2d_persistent<false>;
+// the kernel instantiation for a launch: precision and the column steps per row (ceil(max_ni / 32), unrolled for
+// tiles up to 96 and 288 points wide)
+static const void* solver_fn(int mixed, int max_ni) {
+  if (mixed) {
+    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3>;
+    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9>;
+    return (const void*)cg2d_persistent<true, 0>;
+  }
+  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3>;
+  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9>;
+  return (const void*)cg2d_persistent<false, 0>;
+}
+
+cudaError_t solver_occupancy(int mixed, int max_ni, size_t smem, int* blocks_per_sm) {
+  const void* fn = solver_fn(mixed, max_ni);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, smem);
 }
 
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream) {
-  const void* fn = kp.mixed ? (const void*)cg2d_persistent<true> : (const void*)cg2d_persistent<false>;
+  const void* fn = solver_fn(kp.mixed, kp.max_ni);
   void* args[] = {const_cast<KParams*>(&kp)};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream);
 }
