@@ -178,9 +178,13 @@ cg2d_status_t cg2d_exchange_scalar(const cg2d_topology_t* topo, int batch, const
                                    cg2d_stream_t stream);
 
 /* Phase times of the last solve that used this workspace with params->profile = 1 (synchronises the
- * stream). out (host, >= 1 + 8 * cap values): out[0] = number of CTAs G, then for CTA c the
- * nanoseconds its thread 0 spent in [grid-wide waits, bulk-copy waits, copy issue, compute, unit
- * finish (partials and fixed-order sums), direct passes, other, total] at out[1 + 8c .. 8c + 8].
+ * stream). out (host, >= 1 + 12 * cap values): out[0] = number of CTAs G, then for CTA c at
+ * out[1 + 12c .. 12c + 12] the nanoseconds of
+ *   thread 0:        [0] grid-wide waits, [1] waits for bulk-copied chunk data, [3] compute, [4] end-of-pass
+ *                    reductions, [5] direct passes, [6] the rest, [7] total, [8] wait at the end of a pass for
+ *                    the copy warp's last row sums, [9] reducer waits for unit counts (within [4]),
+ *                    [10] control code between passes;
+ *   the copy warp:   [2] busy issuing copies and folding row sums, [11] waiting for the compute warps.
  * Returns CG2D_BAD_ARG when the groups/params do not describe that workspace's layout. */
 cg2d_status_t cg2d_workspace_profile(const void* workspace, const cg2d_group_t* groups, int ngroups,
                                      const cg2d_params_t* params, uint64_t* out, int cap, cg2d_stream_t stream);

@@ -193,6 +193,10 @@ class GroupSpec:
         self.want_fortran = x_fortran
 
 
+PROF_NAMES = ("bar", "mbar", "issue", "comp", "fin", "direct", "other", "total", "drain", "rwait", "ctrl", "pwait")
+PROF_SLOTS = len(PROF_NAMES)
+
+
 def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8, replace_every=25,
                  replace_above=100.0, timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, check_status=True,
                  test_missing_arrivals=0, profile=False):
@@ -200,8 +204,7 @@ def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8
 
     Returns per group a list (one entry per slot) of (x_out, x_fortran or None, diag ndarray of cg2d_diag_t).
     profile=True records per-CTA phase times; they are left in `solve_groups.last_profile` as an array
-    [ctas, 8] of nanoseconds (grid-wide waits, bulk-copy waits, copy issue, compute, unit finish, direct passes,
-    other, total)."""
+    [ctas, PROF_SLOTS] of nanoseconds, columns PROF_NAMES (include/cg2d.h, cg2d_workspace_profile)."""
     if not 1 <= len(groups) <= 4:
         raise ValueError("1 to 4 groups")
     dev = groups[0].b[0].device
@@ -252,10 +255,10 @@ def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8
             res.append((xo, xf, dg))
         result.append(res)
     if profile:
-        buf = np.zeros(1 + 8 * 1184, np.uint64)
+        buf = np.zeros(1 + PROF_SLOTS * 1184, np.uint64)
         capi.check(L.cg2d_workspace_profile(base + off, arr, len(groups), ctypes.byref(params), buf.ctypes.data, 1184,
                                             _stream(dev)), "cg2d_workspace_profile")
-        solve_groups.last_profile = buf[1:1 + 8 * int(buf[0])].reshape(-1, 8)
+        solve_groups.last_profile = buf[1:1 + PROF_SLOTS * int(buf[0])].reshape(-1, PROF_SLOTS)
     if check_status:
         st = L.cg2d_workspace_status(base + off, _stream(dev))
         if st != capi.CG2D_OK:

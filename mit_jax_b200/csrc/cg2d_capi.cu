@@ -147,7 +147,7 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
   L->rmax = o; o += al(sizeof(unsigned long long) * L->total_rhs);
   L->cnt = o; o += al(sizeof(unsigned) * L->total_ops);
   L->prof = o;
-  if (p->profile) o += al(sizeof(unsigned long long) * (1 + (size_t)kMaxCtas * 8));
+  if (p->profile) o += al(sizeof(unsigned long long) * (1 + (size_t)kMaxCtas * kProfSlots));
   L->zero_end = o;
   L->hist = o; o += al(sizeof(double) * (size_t)L->total_rhs * H_NKIND * L->hist_len);
   L->part = o; o += al(sizeof(double) * (size_t)L->total_rhs * 2 * L->part_units);
@@ -461,7 +461,7 @@ cg2d_status_t cg2d_workspace_profile(const void* workspace, const cg2d_group_t* 
   WsLayout L;
   if (check_params(params) != CG2D_OK || compute_layout(groups, ngroups, params, &L) != CG2D_OK) return CG2D_BAD_ARG;
   if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
-  const size_t n = 1 + (size_t)(cap < kMaxCtas ? cap : kMaxCtas) * 8;
+  const size_t n = 1 + (size_t)(cap < kMaxCtas ? cap : kMaxCtas) * kProfSlots;
   if (cudaMemcpy(out, static_cast<const char*>(workspace) + L.prof, n * sizeof(uint64_t), cudaMemcpyDeviceToHost) !=
       cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return CG2D_OK;

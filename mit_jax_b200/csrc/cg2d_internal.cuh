@@ -145,13 +145,17 @@ struct KParams {
   unsigned* gs;             // [0] grid barrier arrivals, [1] error word, [2] where, [3] pass << 16 | CTA
   unsigned long long timeout_ns;
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
-  unsigned long long* prof; // nullable: [1 + grid * 8] phase times (ns) per CTA
+  unsigned long long* prof; // nullable: [1 + grid * kProfSlots] phase times (ns) per CTA
   StageLay lay[kMaxGroups][P_NPASS];  // shared-memory image of a chunk, per group and pipelined pass
 };
 
 constexpr int kMaxCtas = 148 * 8;
+// phase times of a CTA: thread 0's timeline (grid-wide waits, waits for stage data, compute, end-of-pass
+// reductions, direct passes, the rest, total; within those: the wait for the producer's last row sums at the end
+// of a pass, a reducer's wait for the unit counts, the control code between passes) and the producer warp's
+// (busy issuing and folding row sums; waiting for the compute warps)
 enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FIN = 4, PR_DIRECT = 5, PR_OTHER = 6,
-                       PR_TOTAL = 7 };
+                       PR_TOTAL = 7, PR_DRAIN = 8, PR_RWAIT = 9, PR_CTRL = 10, PR_PWAIT = 11, kProfSlots = 12 };
 
 // launchers (cg2d_solver.cu)
 size_t fixed_smem_bytes(int max_ni, int serial);

@@ -182,8 +182,8 @@ constexpr size_t tsum = rowsum + a16(sizeof(double) * kMaxStages * 4 * kWarps); 
 constexpr size_t misc = tsum + a16(sizeof(double) * kMaxTiles);             // int [4]
 constexpr size_t full = misc + a16(sizeof(int) * 4);                        // mbarrier [kMaxStages]
 constexpr size_t empty = full + a16(8 * kMaxStages);                        // mbarrier [kMaxStages]
-constexpr size_t pacc = empty + a16(8 * kMaxStages);                        // u64 [8]
-constexpr size_t opn = pacc + a16(8 * 8);                                   // unsigned [kMaxOps]
+constexpr size_t pacc = empty + a16(8 * kMaxStages);                        // u64 [kProfSlots]
+constexpr size_t opn = pacc + a16(8 * kProfSlots);                          // unsigned [kMaxOps]
 constexpr size_t uacc = opn + a16(sizeof(unsigned) * kMaxOps);              // double [4]
 constexpr size_t ucnt = uacc + a16(sizeof(double) * 4);                     // unsigned [kMaxOps]
 constexpr size_t utab = ucnt + a16(sizeof(unsigned) * kMaxOps);             // int2 [kMaxUnitsPerCta]
@@ -495,6 +495,7 @@ __device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm)
         }
         __threadfence();
         sm.misc()[2] = good;
+        if (kp.prof) sm.pacc()[PR_RWAIT] += globaltimer() - t0;
       }
       __syncthreads();
       if (!sm.misc()[2]) { ok = false; break; }
@@ -1178,7 +1179,10 @@ __device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const S
       if ((pp.pend >> s2) & 1u) mbar_wait(&sm.full()[s2], ((pp.cph >> s2) & 1u) ^ 1u, kp.timeout_ns);
     pp.pend = 0u;
   }
-  if (kp.prof && lane == 0) sm.pacc()[PR_ISSUE] += (globaltimer() - t_start) - t_wait;
+  if (kp.prof && lane == 0) {
+    sm.pacc()[PR_ISSUE] += (globaltimer() - t_start) - t_wait;
+    sm.pacc()[PR_PWAIT] += t_wait;
+  }
   return ok;
 }
 
@@ -1218,7 +1222,10 @@ __device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const 
   bool ok;
   if ((threadIdx.x >> 5) == kProducer) ok = produce_pass(kp, pt, k, hidx, sm, pp);
   else ok = consume_pass<MIXED, MAXM>(kp, pt, k, sm, pp);
-  if (__syncthreads_or(!ok)) return false;
+  const unsigned long long td = PROF_T0(kp);
+  const int bad = __syncthreads_or(!ok);
+  PROF_ADD(kp, sm, PR_DRAIN, td);
+  if (bad) return false;
   const unsigned long long t0 = PROF_T0(kp);
   ok = reduce_pass(kp, pt, hidx, sm);
   PROF_ADD(kp, sm, PR_FIN, t0);
@@ -1239,6 +1246,7 @@ __device__ __forceinline__ void locate(const KParams& kp, int r, int& gi, int& i
 // publish the actions of this pass: act[] for every solve and opp[] for every operator
 __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, double my_c1, double my_c2) {
   const int tid = threadIdx.x;
+  const unsigned long long t0 = PROF_T0(kp);
   if (tid < kp.total_ops) sm.opp()[tid] = 0;
   __syncthreads();
   if (tid < kp.total_rhs) {
@@ -1252,6 +1260,7 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
     }
   }
   __syncthreads();
+  PROF_ADD(kp, sm, PR_CTRL, t0);
 }
 
 template <bool MIXED, int MAXM>
@@ -1261,7 +1270,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   unsigned target = (unsigned)kp.test_missing;
   Pipe pp = {0u, 0u, 0u, 0u};
   const unsigned long long t_start = PROF_T0(kp);
-  if (tid < 8) sm.pacc()[tid] = 0ull;
+  if (tid < kProfSlots) sm.pacc()[tid] = 0ull;
   for (int i = tid; i < kMaxOps; i += kThreads) { sm.opn()[i] = 0u; sm.ucnt()[i] = 0u; }
   if (tid == 0) {
     for (int s = 0; s < kMaxStages; ++s) {
@@ -1434,10 +1443,11 @@ epilogue:
   }
   if (kp.prof) __syncthreads();   // the producer warp's copy-issue time
   if (kp.prof && tid == 0 && blockIdx.x < kMaxCtas) {
-    unsigned long long* o = kp.prof + 1 + (size_t)blockIdx.x * 8;
+    unsigned long long* o = kp.prof + 1 + (size_t)blockIdx.x * kProfSlots;
     const unsigned long long tot = globaltimer() - t_start;
     unsigned long long acc = 0;   // thread 0's phases (the copy issue runs on the producer warp, beside them)
-    for (int i = 0; i < PR_OTHER; ++i) { o[i] = sm.pacc()[i]; if (i != PR_ISSUE) acc += sm.pacc()[i]; }
+    for (int i = 0; i < kProfSlots; ++i) o[i] = sm.pacc()[i];
+    for (int i : {PR_BAR, PR_MBAR, PR_COMP, PR_FIN, PR_DIRECT, PR_DRAIN, PR_CTRL}) acc += sm.pacc()[i];
     o[PR_OTHER] = tot > acc ? tot - acc : 0ull;
     o[PR_TOTAL] = tot;
     if (blockIdx.x == 0) kp.prof[0] = gridDim.x;
