@@ -42,7 +42,9 @@ typedef enum {
   CG2D_BAD_ARG = 4,
   CG2D_CUDA_ERROR = 5,
   CG2D_WORKSPACE_TOO_SMALL = 6,
-  CG2D_UNSUPPORTED = 7
+  CG2D_UNSUPPORTED = 7,
+  CG2D_INTERNAL_ERROR = 8     /* a device-side consistency check failed (e.g. a halo target outside its vector);
+                                 results are invalid */
 } cg2d_status_t;
 
 typedef enum { CG2D_PREC_F64 = 0, CG2D_PREC_MIXED = 1 } cg2d_precision_t;

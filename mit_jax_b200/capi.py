@@ -19,6 +19,7 @@ CG2D_BAD_ARG = 4
 CG2D_CUDA_ERROR = 5
 CG2D_WORKSPACE_TOO_SMALL = 6
 CG2D_UNSUPPORTED = 7
+CG2D_INTERNAL_ERROR = 8
 
 PREC_F64 = 0
 PREC_MIXED = 1
@@ -26,7 +27,7 @@ SUM_ROWBLOCK = 0
 SUM_FORTRAN = 1
 
 STATUS_NAMES = {0: "ok", 1: "not_converged", 2: "nan", 3: "barrier_timeout", 4: "bad_arg", 5: "cuda_error",
-                6: "workspace_too_small", 7: "unsupported"}
+                6: "workspace_too_small", 7: "unsupported", 8: "internal_error"}
 
 EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_params", "cg2d_workspace_size",
             "cg2d_solve_groups", "cg2d_solve_f64", "cg2d_workspace_status", "cg2d_apply_operator",

@@ -46,7 +46,7 @@ TopoDev topo_dev(const cg2d_topology* tp) {
 }
 
 struct WsLayout {
-  size_t gs, rmax, cnt, prof, zero_end, hist, part, total;
+  size_t gs, rmax, prof, zero_end, hist, part, total;
   size_t vec[kMaxGroups], cpk[kMaxGroups];
   long long vec_stride[kMaxGroups];
   long long vec_off[kMaxGroups][V_NVEC];
@@ -90,9 +90,10 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
     }
     // the direct-load passes stage (8 + 2) rows of (max_ni + 2) doubles per solve slot in the same area
     const unsigned direct = (unsigned)(2 * (kWarps + 2) * (L->max_ni + 2) * sizeof(double));
-    const unsigned red = (unsigned)(4 * L->part_units * sizeof(double));   // partials gathered by a reducer
+    // the sums of a pass are formed with a tile-sum buffer per warp in the same area
+    const unsigned sums = (unsigned)(kAllWarps * kMaxTiles * sizeof(double));
     unsigned sb = hot;
-    if (2 * sb < red) sb = (red + 1) / 2;
+    if (2 * sb < sums) sb = (sums + 1) / 2;
     if (2 * sb < rep) sb = (rep + 1) / 2;
     if (2 * sb < direct) sb = (direct + 1) / 2;
     sb = al128(sb);
@@ -143,9 +144,8 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
   if (st != CG2D_OK) return st;
   L->hist_len = max_iters + 2;
   size_t o = 0;
-  L->gs = o; o += al(2 * sizeof(unsigned));
+  L->gs = o; o += al(8 * sizeof(unsigned));
   L->rmax = o; o += al(sizeof(unsigned long long) * L->total_rhs);
-  L->cnt = o; o += al(sizeof(unsigned) * L->total_ops);
   L->prof = o;
   if (p->profile) o += al(sizeof(unsigned long long) * (1 + (size_t)kMaxCtas * kProfSlots));
   L->zero_end = o;
@@ -196,6 +196,7 @@ const char* cg2d_status_string(cg2d_status_t s) {
     case CG2D_CUDA_ERROR: return "CUDA error";
     case CG2D_WORKSPACE_TOO_SMALL: return "workspace too small";
     case CG2D_UNSUPPORTED: return "unsupported size";
+    case CG2D_INTERNAL_ERROR: return "device-side consistency check failed; results invalid";
   }
   return "unknown status";
 }
@@ -355,7 +356,6 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   kp.hist_len = L.hist_len;
   kp.part = reinterpret_cast<double*>(ws + L.part);
   kp.part_units = L.part_units;
-  kp.cnt = reinterpret_cast<unsigned*>(ws + L.cnt);
   kp.rmax = reinterpret_cast<unsigned long long*>(ws + L.rmax);
   kp.gs = reinterpret_cast<unsigned*>(ws + L.gs);
   kp.timeout_ns = (unsigned long long)(params->timeout_s * 1e9);

@@ -11,6 +11,7 @@ namespace cg2d {
 constexpr int kWarps = 8;                  // compute warps per CTA; a chunk has at most kWarps rows (one warp per row)
 constexpr int kProducer = kWarps;          // index of the warp that issues the bulk copies and folds the row sums
 constexpr int kThreads = (kWarps + 1) * 32;
+constexpr int kAllWarps = kThreads / 32;
 constexpr int kMaxStages = 2;              // stage buffers of the copy pipeline
 constexpr int kMaxUnitsPerCta = 512;       // work units one CTA owns in a launch (its unit table)
 constexpr int kMaxGroups = CG2D_MAX_GROUPS;
@@ -140,9 +141,9 @@ struct KParams {
   int hist_len;
   double* part;             // [total_rhs][2][part_units]
   int part_units;
-  unsigned* cnt;            // [total_ops] monotonic per-operator unit counters
   unsigned long long* rmax; // [total_rhs] max|b*cg2dNorm| as ordered bits
-  unsigned* gs;             // [0] grid barrier arrivals, [1] error word, [2] where, [3] pass << 16 | CTA
+  // [0] grid-wide wait arrivals, [1] error word, [2] where a time limit ran out, [3] pass << 16 | CTA
+  unsigned* gs;
   unsigned long long timeout_ns;
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
   unsigned long long* prof; // nullable: [1 + grid * kProfSlots] phase times (ns) per CTA

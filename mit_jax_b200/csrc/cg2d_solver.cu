@@ -178,15 +178,12 @@ constexpr size_t norm = rnorm + a16(sizeof(double) * kMaxSolves);           // d
 constexpr size_t has_alpha = norm + a16(sizeof(double) * kMaxSolves);       // int [kMaxSolves]
 constexpr size_t opp = has_alpha + a16(sizeof(int) * kMaxSolves);           // int [kMaxOps] operator in the pass
 constexpr size_t rowsum = opp + a16(sizeof(int) * kMaxOps);                 // double [kMaxStages][4][kWarps]
-constexpr size_t tsum = rowsum + a16(sizeof(double) * kMaxStages * 4 * kWarps);   // double [kMaxTiles]
-constexpr size_t misc = tsum + a16(sizeof(double) * kMaxTiles);             // int [4]
+constexpr size_t misc = rowsum + a16(sizeof(double) * kMaxStages * 4 * kWarps);   // int [4]
 constexpr size_t full = misc + a16(sizeof(int) * 4);                        // mbarrier [kMaxStages]
 constexpr size_t empty = full + a16(8 * kMaxStages);                        // mbarrier [kMaxStages]
 constexpr size_t pacc = empty + a16(8 * kMaxStages);                        // u64 [kProfSlots]
-constexpr size_t opn = pacc + a16(8 * kProfSlots);                          // unsigned [kMaxOps]
-constexpr size_t uacc = opn + a16(sizeof(unsigned) * kMaxOps);              // double [4]
-constexpr size_t ucnt = uacc + a16(sizeof(double) * 4);                     // unsigned [kMaxOps]
-constexpr size_t utab = ucnt + a16(sizeof(unsigned) * kMaxOps);             // int2 [kMaxUnitsPerCta]
+constexpr size_t uacc = pacc + a16(8 * kProfSlots);                         // double [4]
+constexpr size_t utab = uacc + a16(sizeof(double) * 4);                     // int2 [kMaxUnitsPerCta]
 constexpr size_t pend = utab + a16(sizeof(int2) * kMaxUnitsPerCta);         // int4 [kMaxStages]
 constexpr size_t end = pend + a16(sizeof(int4) * kMaxStages);               // then prod (FORTRAN order)
 }  // namespace smo
@@ -194,15 +191,14 @@ constexpr size_t end = pend + a16(sizeof(int4) * kMaxStages);               // t
 // Views of the shared memory. Fixed arrays:
 //   act, c1, c2, rnorm, norm, has_alpha   per solve: action in the pass, pass coefficients, rhsNorm, cg2dNorm,
 //                                          whether alpha_{k-1} exists
-//   opp, opn, ucnt                         per operator: in the pass; passes with sums completed (its counter
-//                                          target); units this CTA completed in the pass
+//   opp                                    per operator: takes part in the pass
 //   rowsum                                 row sums of the chunk in each stage [stage][4 sums][kWarps]
-//   tsum, misc                             reducer scratch; [0] barrier ok, [2] reducer ok, [3] units in utab
+//   misc                                   [0] grid-wide wait ok, [3] units in utab
 //   full, empty                            stage mbarriers: copies landed / compute warps done with the stage
 //   pacc, uacc                             phase times (profiling); the current unit's partial sums
 //   utab, pend                             this CTA's work units; the chunk in each stage awaiting its row sums
 // then prod (FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]) and the stage buffers at `stage` (kMaxStages x
-// stage_bytes, 128-aligned; also the direct-pass staging area and the reducer's gather buffer).
+// stage_bytes, 128-aligned; also the direct-pass staging area and the tile-sum buffers of the pass sums).
 struct Smem {
   unsigned stage;
   template <class T>
@@ -215,14 +211,11 @@ struct Smem {
   __device__ __forceinline__ int* has_alpha() const { return at<int>(smo::has_alpha); }
   __device__ __forceinline__ int* opp() const { return at<int>(smo::opp); }
   __device__ __forceinline__ double* rowsum() const { return at<double>(smo::rowsum); }
-  __device__ __forceinline__ double* tsum() const { return at<double>(smo::tsum); }
   __device__ __forceinline__ int* misc() const { return at<int>(smo::misc); }
   __device__ __forceinline__ unsigned long long* full() const { return at<unsigned long long>(smo::full); }
   __device__ __forceinline__ unsigned long long* empty() const { return at<unsigned long long>(smo::empty); }
   __device__ __forceinline__ unsigned long long* pacc() const { return at<unsigned long long>(smo::pacc); }
-  __device__ __forceinline__ unsigned* opn() const { return at<unsigned>(smo::opn); }
   __device__ __forceinline__ double* uacc() const { return at<double>(smo::uacc); }
-  __device__ __forceinline__ unsigned* ucnt() const { return at<unsigned>(smo::ucnt); }
   __device__ __forceinline__ int2* utab() const { return at<int2>(smo::utab); }
   __device__ __forceinline__ int4* pend() const { return at<int4>(smo::pend); }
   __device__ __forceinline__ double* prod() const { return at<double>(smo::end); }
@@ -241,39 +234,89 @@ __device__ inline Smem carve(int max_ni, int serial) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// grid-wide wait with a time limit: every CTA arrives once; the wait ends when all have arrived,
-// when another CTA has flagged an error, or after timeout_ns (then this CTA flags the error).
+// grid-wide wait: every CTA arrives once (after this CTA's stores, release); the wait ends when all have
+// arrived (acquire), when another CTA has flagged an error, or after timeout_ns (then this CTA flags the error).
 
-struct Smem;
-__device__ bool grid_barrier(const KParams& kp, unsigned& target, int* flag, unsigned long long* pacc) {
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// `target` counts the arrivals this CTA waits for (uniform in the grid)
+__device__ bool grid_wait(const KParams& kp, unsigned& target, int pt, const Smem& sm) {
   const unsigned long long tb = PROF_T0(kp);
   fence_proxy_async();        // this thread's stores before the next pass's bulk copies
   __syncthreads();
+  target += gridDim.x;
   if (threadIdx.x == 0) {
-    target += gridDim.x;
-    __threadfence();
-    atomicAdd(&kp.gs[0], 1u);
+    atom_add_release(&kp.gs[0], 1u);
     const unsigned long long t0 = globaltimer();
     int ok = 1;
     for (unsigned spins = 0;; ++spins) {
-      const unsigned v = ld_acquire(&kp.gs[0]);
-      if ((int)(v - target) >= 0) break;
-      if (spins > 8) __nanosleep(64);
-      if (ld_relaxed(&kp.gs[1]) != 0u) { ok = 0; break; }
-      if ((spins & 63u) == 63u && globaltimer() - t0 > kp.timeout_ns) {
-        note_timeout(kp.gs, 1u, 0u);
-        ok = 0;
-        break;
+      if ((int)(ld_acquire(&kp.gs[0]) - target) >= 0) break;
+      if (spins > 8) __nanosleep(32);
+      if ((spins & 63u) == 63u) {
+        if (ld_relaxed(&kp.gs[1]) != 0u) { ok = 0; break; }
+        if (globaltimer() - t0 > kp.timeout_ns) {
+          note_timeout(kp.gs, 1u, (unsigned)pt);
+          ok = 0;
+          break;
+        }
       }
     }
-    __threadfence();
     fence_proxy_async();
-    *flag = ok;
-    if (kp.prof) pacc[PR_BAR] += globaltimer() - tb;
+    sm.misc()[0] = ok;
+    if (kp.prof) sm.pacc()[PR_BAR] += globaltimer() - tb;
   }
   __syncthreads();
-  const int ok = *flag;
-  return ok != 0;
+  return sm.misc()[0] != 0;
+}
+
+__device__ __forceinline__ double* hist_ptr(const KParams& kp, int rid, int kind, int idx);
+__device__ __forceinline__ int nsums(int pt, int a);
+__device__ __forceinline__ int hist_kind(int pt, int kind);
+__device__ __forceinline__ void locate(const KParams& kp, int r, int& gi, int& inst, int& slot);
+
+// The sums of pass pt from the unit partials, in fixed order: blocks of a tile in order, then tiles in order
+// from 0 (GLOBAL_SUM_TILE, global_sum.py:20-26). Sum (solve r, kind q) is formed by warp r * 2 + q of the grid
+// (modulo its warps): lane l adds the blocks of tiles l, l + 32, ..., lane 0 the tile sums.
+__device__ void form_sums(const KParams& kp, int pt, int hidx, const Smem& sm) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* tbuf = reinterpret_cast<double*>(smem_raw + sm.stage) + warp * kMaxTiles;   // free between passes
+  const int nw = (int)gridDim.x * kAllWarps;
+  for (int s = (int)blockIdx.x * kAllWarps + warp; s < 2 * kp.total_rhs; s += nw) {
+    const int r = s >> 1, q = s & 1;
+    if (q >= nsums(pt, sm.act()[r])) continue;
+    int gi, inst, slot;
+    locate(kp, r, gi, inst, slot);
+    const GroupDev& g = kp.g[gi];
+    const double* p = kp.part + ((size_t)r * 2 + q) * kp.part_units;
+    for (int t = lane; t < g.tp.T; t += 32) {
+      const double* pt_ = p + t * g.nblk;
+      double a = 0.0;
+#pragma unroll 8
+      for (int b = 0; b < g.nblk; ++b) a = add(a, __ldcg(pt_ + b));
+      tbuf[t] = a;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      double total = 0.0;
+      for (int t = 0; t < g.tp.T; ++t) total = add(total, tbuf[t]);
+      stcg(hist_ptr(kp, r, hist_kind(pt, q), hidx), total);
+    }
+    __syncwarp();
+  }
+}
+
+// end of a pass: wait for every CTA's unit partials, form the sums, wait until every sum is written
+__device__ bool grid_sync(const KParams& kp, unsigned& target, int pt, int hidx, const Smem& sm) {
+  if (!grid_wait(kp, target, pt, sm)) return false;
+  if (pt == P_MAX) return true;
+  const unsigned long long tf = PROF_T0(kp);
+  form_sums(kp, pt, hidx, sm);
+  PROF_ADD(kp, sm, PR_FIN, tf);
+  return grid_wait(kp, target, pt, sm);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -293,18 +336,26 @@ __device__ __forceinline__ long long vidx(const TopoDev& tp, int t, int j, int i
   return ((long long)t * (tp.nj + 2) + j + 1) * tp.P + i + 1;
 }
 
+// one push store: target a (-1 = none) must lie inside the vector (lim elements); anything else is an internal
+// inconsistency, recorded in the error word instead of stored
+template <class T>
+__device__ __forceinline__ void push_one(T* vec, int a, T v, unsigned lim, unsigned* gs) {
+  if ((unsigned)a < lim) stcg(vec + a, v);
+  else if (a != -1) atomicCAS(&gs[1], 0u, (unsigned)CG2D_INTERNAL_ERROR);
+}
+
 // store the value of point (t, j, i) into the ring cells of the tiles that read it across an edge
 template <class T>
-__device__ __forceinline__ void push(const TopoDev& tp, T* vec, int t, int j, int i, T v) {
+__device__ __forceinline__ void push(const TopoDev& tp, T* vec, int t, int j, int i, T v, unsigned* gs) {
   const int* e;
   if (i == 0) e = tp.tg + ((size_t)t * tp.nj + j) * 4;
   else if (i == tp.ni - 1) e = tp.tg + ((size_t)t * tp.nj + j) * 4 + 2;
   else if (j == 0) e = tp.tg + (size_t)tp.T * tp.nj * 4 + ((size_t)t * tp.nip + i) * 2;
   else if (j == tp.nj - 1) e = tp.tg + (size_t)tp.T * tp.nj * 4 + ((size_t)(tp.T + t) * tp.nip + i) * 2;
   else return;
-  const int s0 = __ldg(e), s1 = __ldg(e + 1);
-  if (s0 >= 0) stcg(vec + s0, v);
-  if (s1 >= 0) stcg(vec + s1, v);
+  const unsigned lim = (unsigned)tp.T * (unsigned)(tp.nj + 2) * (unsigned)tp.P;
+  push_one(vec, __ldg(e), v, lim, gs);
+  push_one(vec, __ldg(e + 1), v, lim, gs);
 }
 
 // the same with the chunk's target lists staged in shared memory (row w of the chunk = tile row j)
@@ -312,6 +363,8 @@ struct PushTab {
   const int4* twe;
   const int2 *ts, *tn;
   int ni, nj;
+  unsigned lim;   // elements of a vector
+  unsigned* gs;
 };
 template <class T>
 __device__ __forceinline__ void push_s(const PushTab& pt, T* vec, int j, int w, int i, T v) {
@@ -321,8 +374,8 @@ __device__ __forceinline__ void push_s(const PushTab& pt, T* vec, int j, int w, 
   else if (j == 0) { const int2 e = pt.ts[i]; a = e.x; b = e.y; }
   else if (j == pt.nj - 1) { const int2 e = pt.tn[i]; a = e.x; b = e.y; }
   else return;
-  if (a >= 0) stcg(vec + a, v);
-  if (b >= 0) stcg(vec + b, v);
+  push_one(vec, a, v, pt.lim, pt.gs);
+  push_one(vec, b, v, pt.lim, pt.gs);
 }
 
 // compact index -> padded index of the same point
@@ -430,11 +483,8 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
   __syncwarp();
 }
 
-// lane 0 of the accumulating warp writes the unit's partials (no wait) and counts the unit in shared memory; the
-// counts are published once per pass (publish_counts)
-__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
+// lane 0 of the accumulating warp writes the unit's partials (the grid-wide wait at the end of the pass makes them
+// visible to the warps that form the sums)
 __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g, int inst, int lu, int ns0, int ns1,
                                             const Smem& sm) {
   if ((threadIdx.x & 31) != 0 || ns0 + ns1 == 0) return;
@@ -443,103 +493,6 @@ __device__ __forceinline__ void finish_unit(const KParams& kp, const GroupDev& g
   if (ns0 > 1) stcg(kp.part + ((size_t)rid0 * 2 + 1) * kp.part_units + lu, sm.uacc()[1]);
   if (ns1 > 0) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 0) * kp.part_units + lu, sm.uacc()[2]);
   if (ns1 > 1) stcg(kp.part + ((size_t)(rid0 + 1) * 2 + 1) * kp.part_units + lu, sm.uacc()[3]);
-  sm.ucnt()[g.op_base + inst] += 1u;
-}
-// every CTA, end of its units: add its unit counts to the operators' counters (release: the partials written
-// before are visible to whoever observes the count)
-__device__ __forceinline__ void publish_counts(const KParams& kp, const Smem& sm) {
-  if (threadIdx.x == 0 || threadIdx.x == kProducer * 32) __threadfence();   // the writers of the unit partials
-  __syncthreads();
-  for (int op = threadIdx.x; op < kp.total_ops; op += kThreads) {
-    const unsigned c = sm.ucnt()[op];
-    if (c) {
-      red_release_add(&kp.cnt[op], c);
-      sm.ucnt()[op] = 0u;
-    }
-  }
-  __syncthreads();
-}
-
-// End of a pass: the CTA that owns an instance's last unit waits until all of the instance's units are counted,
-// gathers their partials and forms the instance's sums in fixed order -- blocks of a tile in order, then tiles in
-// order from 0 (GLOBAL_SUM_TILE, global_sum.py:20-26). Then every CTA advances the operators' counter targets.
-__device__ bool reduce_pass(const KParams& kp, int pt, int hidx, const Smem& sm) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  publish_counts(kp, sm);
-  double* buf = reinterpret_cast<double*>(smem_raw + sm.stage);   // free at the end of a pass
-  bool ok = true;
-  for (int gi = 0; gi < kp.ngroups && ok; ++gi) {
-    const GroupDev& g = kp.g[gi];
-    for (int inst = 0; inst < g.count; ++inst) {
-      const int op = g.op_base + inst;
-      if (!sm.opp()[op]) continue;
-      const int ulast = g.unit_base + inst * g.units + g.units - 1;
-      if (ulast % (int)gridDim.x != (int)blockIdx.x) continue;
-      const Slots si = slots_of(g, inst, sm);
-      // sums l = 0 .. nl-1: slot 0's ns0 kinds, then slot 1's
-      const int ns0 = nsums(pt, si.act(0)), ns1 = nsums(pt, si.act(1));
-      const int nl = ns0 + ns1;
-      if (!nl) continue;
-      if (tid == 0) {
-        const unsigned target = (sm.opn()[op] + 1u) * (unsigned)g.units;
-        const unsigned long long t0 = globaltimer();
-        int good = 1;
-        for (unsigned spins = 0;; ++spins) {
-          if ((int)(ld_acquire(&kp.cnt[op]) - target) >= 0) break;
-          if (spins > 8) __nanosleep(64);
-          if ((spins & 63u) == 63u && (ld_relaxed(&kp.gs[1]) != 0u || globaltimer() - t0 > kp.timeout_ns)) {
-            note_timeout(kp.gs, 3u, (unsigned)pt);
-            good = 0;
-            break;
-          }
-        }
-        __threadfence();
-        sm.misc()[2] = good;
-        if (kp.prof) sm.pacc()[PR_RWAIT] += globaltimer() - t0;
-      }
-      __syncthreads();
-      if (!sm.misc()[2]) { ok = false; break; }
-      const int U = g.units;
-      for (int idx = tid; idx < nl * U; idx += kThreads) {
-        const int l = idx / U, u = idx - (idx / U) * U;
-        const int sl = l < ns0 ? 0 : 1, ql = l < ns0 ? l : l - ns0;
-        buf[idx] = ldcg(kp.part + ((size_t)si.rid(sl) * 2 + ql) * kp.part_units + u);
-      }
-      __syncthreads();
-      if (warp == 0) {
-        for (int l = 0; l < nl; ++l) {
-          for (int tt = lane; tt < g.tp.T; tt += 32) {
-            double a = 0.0;
-            for (int b = 0; b < g.nblk; ++b) a = add(a, buf[l * U + tt * g.nblk + b]);
-            sm.tsum()[tt] = a;
-          }
-          __syncwarp();
-          if (lane == 0) {
-            double a = 0.0;
-            for (int tt = 0; tt < g.tp.T; ++tt) a = add(a, sm.tsum()[tt]);
-            const int sl = l < ns0 ? 0 : 1, ql = l < ns0 ? l : l - ns0;
-            stcg(hist_ptr(kp, si.rid(sl), hist_kind(pt, ql), hidx), a);
-          }
-          __syncwarp();
-        }
-      }
-      __syncthreads();
-    }
-  }
-  // every CTA: operators that produced sums in this pass expect one more round of unit counts
-  __syncthreads();
-  for (int op = tid; op < kp.total_ops; op += kThreads) {
-    if (!sm.opp()[op]) continue;
-    int gi = 0;
-    while (gi + 1 < kp.ngroups && op >= kp.g[gi + 1].op_base) ++gi;
-    const GroupDev& g = kp.g[gi];
-    const int inst = op - g.op_base;
-    int any = 0;
-    for (int s = 0; s < g.nrhs; ++s) any |= nsums(pt, sm.act()[g.rhs_base + inst * g.nrhs + s]);
-    if (any) sm.opn()[op] += 1u;
-  }
-  __syncthreads();
-  return ok;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -647,7 +600,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
             const V r0 = (V)sub(bn, ax);                                                   // cg2d.py:232
             V* rv = vec_ptr<V>(g, inst, s, V_R0);
             stcg(rv + vo, r0);
-            push(tp, rv, t, j, i, r0);
+            push(tp, rv, t, j, i, r0, kp.gs);
             stcg(vec_ptr<V>(g, inst, s, V_S1) + vo, (V)0);                               // s = 0 (cg2d.py:231)
             p0 = mul((double)r0, (double)r0);
             p1 = bn;
@@ -703,9 +656,8 @@ __device__ bool run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
     if (!sm.opp()[g.op_base + inst]) continue;
     process_unit_direct<MIXED>(kp, g, inst, rel - inst * g.units, pt, sm);
   }
-  const bool ok = reduce_pass(kp, pt, 0, sm);
   PROF_ADD(kp, sm, PR_DIRECT, t0);
-  return ok;
+  return true;
 }
 
 // x ring cells at the start: the exchanged normalised first guess; unwritten points keep cg2d_x
@@ -762,18 +714,38 @@ __device__ __forceinline__ Unit unit_at(const Smem& sm, int ui) {
   return u;
 }
 __device__ void build_unit_table(const KParams& kp, const Smem& sm) {
+  // Units are dealt to the CTAs round-robin in this order: every group's full row blocks (instance, tile,
+  // block), then the shorter last blocks of the tiles, so that every CTA gets the same number of rows to within
+  // one unit.
+  const int R = kp.rows_per_block;
+  int nfull = 0;
+  for (int gi = 0; gi < kp.ngroups; ++gi) {
+    const GroupDev& g = kp.g[gi];
+    nfull += g.count * g.tp.T * (kp.serial ? 1 : g.tp.nj / R);
+  }
   const int n = (kp.total_units - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   for (int q = threadIdx.x; q < n; q += kThreads) {
-    const int u = (int)blockIdx.x + q * (int)gridDim.x;
-    int gi = 0;
-    while (gi + 1 < kp.ngroups && u >= kp.g[gi + 1].unit_base) ++gi;
+    int o = (int)blockIdx.x + q * (int)gridDim.x;
+    const bool full = o < nfull;
+    if (!full) o -= nfull;
+    int gi = 0, inst = 0, t = 0, blk = 0;
+    for (gi = 0; gi < kp.ngroups; ++gi) {
+      const GroupDev& g = kp.g[gi];
+      const int nf = kp.serial ? 1 : g.tp.nj / R;                                        // full blocks per tile
+      const int per = full ? g.tp.T * nf : ((!kp.serial && g.tp.nj % R) ? g.tp.T : 0);   // units per instance
+      if (o < g.count * per) {
+        inst = o / per;
+        const int r2 = o - inst * per;
+        if (full) { t = r2 / nf; blk = r2 - t * nf; }
+        else { t = r2; blk = nf; }
+        break;
+      }
+      o -= g.count * per;
+    }
     const GroupDev& g = kp.g[gi];
-    const int rel = u - g.unit_base;
-    const int inst = rel / g.units;
-    const int lu = rel - inst * g.units;
-    const int t = lu / g.nblk, blk = lu - t * g.nblk;
-    const int R = kp.serial ? g.tp.nj : kp.rows_per_block;
-    const int j0 = blk * R, j1 = min(g.tp.nj, j0 + R);
+    const int lu = t * g.nblk + blk;
+    const int Rg = kp.serial ? g.tp.nj : R;
+    const int j0 = blk * Rg, j1 = min(g.tp.nj, j0 + Rg);
     sm.utab()[q] = make_int2(gi | (inst << 2) | (lu << 10), t | (j0 << 8) | (j1 << 19));
   }
   if (threadIdx.x == 0) sm.misc()[3] = n > 0 ? n : 0;
@@ -928,6 +900,8 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   ptab.tn = reinterpret_cast<const int2*>(sb + L.tn);
   ptab.ni = ni;
   ptab.nj = nj;
+  ptab.lim = (unsigned)tp.T * (unsigned)(nj + 2) * (unsigned)P;
+  ptab.gs = kp.gs;
   const int act0 = si.act(0), act1 = si.act(1);
 
   // pass S after convergence: the pending x update, un-normalised (cg2d.py:254, 266)
@@ -1225,11 +1199,7 @@ __device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const 
   const unsigned long long td = PROF_T0(kp);
   const int bad = __syncthreads_or(!ok);
   PROF_ADD(kp, sm, PR_DRAIN, td);
-  if (bad) return false;
-  const unsigned long long t0 = PROF_T0(kp);
-  ok = reduce_pass(kp, pt, hidx, sm);
-  PROF_ADD(kp, sm, PR_FIN, t0);
-  return ok;
+  return !bad;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1271,7 +1241,6 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   Pipe pp = {0u, 0u, 0u, 0u};
   const unsigned long long t_start = PROF_T0(kp);
   if (tid < kProfSlots) sm.pacc()[tid] = 0ull;
-  for (int i = tid; i < kMaxOps; i += kThreads) { sm.opn()[i] = 0u; sm.ucnt()[i] = 0u; }
   if (tid == 0) {
     for (int s = 0; s < kMaxStages; ++s) {
       mbar_init(&sm.full()[s], 1);          // the producer's arrive (with the copies' byte count)
@@ -1303,7 +1272,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   // ---- rhsMax = max |b cg2dNorm| (cg2d.py:221-225)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   ok = run_pass_direct<MIXED>(kp, P_MAX, sm);
-  ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+  ok = grid_sync(kp, target, P_MAX, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) {
     rhsMax = __longlong_as_double((long long)__ldcg(&kp.rmax[tid]));
@@ -1314,13 +1283,13 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   init_x_ring(kp, sm);
   ok = run_pass_direct<MIXED>(kp, P_INIT, sm);
-  ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+  ok = grid_sync(kp, target, P_INIT, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, 0, 0, sm, pp);
-  ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+  ok = grid_sync(kp, target, P_Z, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
 
@@ -1344,7 +1313,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
     ok = run_pass_pipe<MIXED, MAXM>(kp, P_S, k, k, sm, pp);
-    ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+    ok = grid_sync(kp, target, P_S, k, sm) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
     if (a == A_ACTIVE) {
@@ -1362,7 +1331,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, alpha, 0.0);
       ok = run_pass_pipe<MIXED, MAXM>(kp, P_X, k, k + 1, sm, pp);
-      ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+      ok = grid_sync(kp, target, P_X, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
         rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
@@ -1372,7 +1341,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, alpha, 0.0);
       ok = run_pass_pipe<MIXED, MAXM>(kp, P_R, k, k + 1, sm, pp);
-      ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+      ok = grid_sync(kp, target, P_R, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
         rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
@@ -1380,7 +1349,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
       ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, k, k + 1, sm, pp);
-      ok = grid_barrier(kp, target, sm.misc(), sm.pacc()) && ok;
+      ok = grid_sync(kp, target, P_Z, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
     }
@@ -1434,7 +1403,8 @@ epilogue:
     d.numIters = k_done >= 0 ? k_done : k;
     d.replacements = nrep;
     d.reserved = 0;
-    if (!ok || __ldcg(&kp.gs[1]) != 0u) d.status = CG2D_BARRIER_TIMEOUT;
+    const unsigned err = __ldcg(&kp.gs[1]);
+    if (!ok || err != 0u) d.status = err != 0u ? (int)err : CG2D_BARRIER_TIMEOUT;
     else if (rr != rr) d.status = CG2D_NAN;
     else if (!(rr < tol2)) d.status = CG2D_NOT_CONVERGED;
     else d.status = CG2D_OK;
