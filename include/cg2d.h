@@ -151,6 +151,25 @@ cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2d
                              const cg2d_params_t* params,
                              void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
 
+/* cg2d_solve_f64 without a caller workspace and without any allocation (no counterpart in the reference, whose
+ * JAX arrays are allocated by XLA). For callers that cannot allocate device memory where they solve: a step
+ * inside a framework that owns the whole device pool and hands a custom call only its operands, or code that
+ * must not let a cudaMalloc synchronise the device. The workspace is a fixed array of
+ * CG2D_NOALLOC_SCRATCH_BYTES in the library's device memory, held by every GPU that loads the library until the
+ * process exits (enough for two LLC90 solves in FP64). A solve needing more returns CG2D_WORKSPACE_TOO_SMALL.
+ * The topology is created beforehand (cg2d_topology_create allocates); inputs and outputs are the caller's, as
+ * for cg2d_solve_f64. The first call on a device looks up the array's device address (with that device
+ * current); make it before any stream capture. All calls on a device share the array: calls that overlap on
+ * the GPU (other streams, other threads) race and give wrong results; serialise them. */
+#define CG2D_NOALLOC_SCRATCH_BYTES (32u << 20)
+cg2d_status_t cg2d_solve_f64_noalloc(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                     const double* aW2d, const double* aS2d, const double* aC2d,
+                                     const double* pW, const double* pS, const double* pC,
+                                     const double* cg2d_b, const double* cg2d_x,
+                                     double tolerance, int max_iters,
+                                     double* x_out, double* x_fortran, cg2d_diag_t* diag,
+                                     const cg2d_params_t* params, cg2d_stream_t stream);
+
 /* Host-side error word of the last solve that used this workspace (synchronises the stream). */
 cg2d_status_t cg2d_workspace_status(const void* workspace, cg2d_stream_t stream);
 

@@ -20,6 +20,7 @@ CG2D_CUDA_ERROR = 5
 CG2D_WORKSPACE_TOO_SMALL = 6
 CG2D_UNSUPPORTED = 7
 CG2D_INTERNAL_ERROR = 8
+NOALLOC_SCRATCH_BYTES = 32 << 20   # CG2D_NOALLOC_SCRATCH_BYTES
 
 PREC_F64 = 0
 PREC_MIXED = 1
@@ -31,7 +32,8 @@ STATUS_NAMES = {0: "ok", 1: "not_converged", 2: "nan", 3: "barrier_timeout", 4: 
 
 EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_params", "cg2d_workspace_size",
             "cg2d_solve_groups", "cg2d_solve_f64", "cg2d_workspace_status", "cg2d_apply_operator",
-            "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string", "cg2d_workspace_profile")
+            "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string", "cg2d_workspace_profile",
+            "cg2d_solve_f64_noalloc")
 
 
 class Params(ctypes.Structure):
@@ -87,6 +89,9 @@ def lib():
     L.cg2d_solve_f64.argtypes = [_P, i, d, _P, _P, _P, _P, _P, _P, _P, _P, d, i, _P, _P, _P,
                                  ctypes.POINTER(Params), _P, ctypes.c_size_t, _P]
     L.cg2d_solve_f64.restype = i
+    L.cg2d_solve_f64_noalloc.argtypes = [_P, i, d, _P, _P, _P, _P, _P, _P, _P, _P, d, i, _P, _P, _P,
+                                         ctypes.POINTER(Params), _P]
+    L.cg2d_solve_f64_noalloc.restype = i
     L.cg2d_workspace_status.argtypes = [_P, _P]
     L.cg2d_workspace_status.restype = i
     L.cg2d_apply_operator.argtypes = [_P, i, d, _P, _P, _P, _P, _P, _P]

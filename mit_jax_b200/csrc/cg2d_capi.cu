@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "cg2d_internal.cuh"
@@ -490,6 +491,72 @@ cg2d_status_t cg2d_exchange_scalar(const cg2d_topology_t* topo, int batch, const
   if (!topo || batch < 1 || !a || !out || a == out) return CG2D_BAD_ARG;
   if (launch_exchange(topo_dev(topo), batch, a, out, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return CG2D_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------------
+// Solve without any allocation. Some callers cannot allocate device memory at the point where they solve: a
+// solver step running inside a framework that owns the whole device pool (an XLA custom call handed only its
+// operands, a model step under a memory-capped allocator), or code where a cudaMalloc would synchronise the
+// device and stall its other streams. They use this entry point, whose workspace is a fixed array in the
+// library's device memory. Every GPU that loads the library holds CG2D_NOALLOC_SCRATCH_BYTES for it until the
+// process exits; all calls on a device share it.
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CG2D_NOALLOC_SCRATCH_BYTES];
+
+// device address of g_noalloc_scratch, looked up once per device (with that device current)
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+cg2d_status_t noalloc_scratch(void** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return CG2D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cg2d_status_t cg2d_solve_f64_noalloc(const cg2d_topology_t* topo, int batch, double cg2dNorm, const double* aW2d,
+                                     const double* aS2d, const double* aC2d, const double* pW, const double* pS,
+                                     const double* pC, const double* cg2d_b, const double* cg2d_x,
+                                     double tolerance, int max_iters, double* x_out, double* x_fortran,
+                                     cg2d_diag_t* diag, const cg2d_params_t* params, cg2d_stream_t stream) {
+  cg2d_group_t g;
+  std::memset(&g, 0, sizeof(g));
+  g.topo = topo;
+  g.count = batch;
+  g.nrhs = 1;
+  g.aW2d = aW2d; g.aS2d = aS2d; g.aC2d = aC2d; g.pW = pW; g.pS = pS; g.pC = pC;
+  g.cg2dNorm = cg2dNorm;
+  g.b[0] = cg2d_b;
+  g.x0[0] = cg2d_x;
+  g.x_out[0] = x_out;
+  g.x_fortran[0] = x_fortran;
+  g.diag[0] = diag;
+  g.tolerance[0] = tolerance;
+  g.max_iters[0] = max_iters;
+  // the workspace this solve needs must fit the fixed array
+  const size_t need = cg2d_workspace_size(&g, 1, params);
+  if (need == 0) return CG2D_BAD_ARG;
+  if (need > (size_t)CG2D_NOALLOC_SCRATCH_BYTES) return CG2D_WORKSPACE_TOO_SMALL;
+  void* ws = nullptr;
+  const cg2d_status_t st = noalloc_scratch(&ws);
+  if (st != CG2D_OK) return st;
+  // the solve zeroes the part of the workspace that must start at zero (the grid-wait counter, the error word,
+  // the rhsMax words) and writes everything else before reading it, so the previous call's contents do no harm
+  return cg2d_solve_groups(&g, 1, params, ws, (size_t)CG2D_NOALLOC_SCRATCH_BYTES, stream);
 }
 
 }  // extern "C"
