@@ -167,6 +167,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // compiler to address shared memory (shared loads, no aliasing with global stores)
 extern __shared__ __align__(128) unsigned char smem_raw[];
 
+// CG scalars of one solve between passes (one entry per solve; the thread of the same index owns it)
+struct SolveState {
+  double eta, eta_prev, alpha, rr;
+  int k_done, nrep;
+};
+static_assert(sizeof(SolveState) == 40, "SolveState layout");
+
 // Fixed part of the shared-memory layout: compile-time offsets, so that no registers hold its addresses.
 __host__ __device__ constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
 namespace smo {
@@ -185,7 +192,8 @@ constexpr size_t pacc = empty + a16(8 * kMaxStages);                        // u
 constexpr size_t uacc = pacc + a16(8 * kProfSlots);                         // double [4]
 constexpr size_t utab = uacc + a16(sizeof(double) * 4);                     // int2 [kMaxUnitsPerCta]
 constexpr size_t pend = utab + a16(sizeof(int2) * kMaxUnitsPerCta);         // int4 [kMaxStages]
-constexpr size_t end = pend + a16(sizeof(int4) * kMaxStages);               // then prod (FORTRAN order)
+constexpr size_t state = pend + a16(sizeof(int4) * kMaxStages);             // SolveState [kMaxSolves + 1]
+constexpr size_t end = state + a16(40 * (kMaxSolves + 1));                   // then prod (FORTRAN order)
 }  // namespace smo
 
 // Views of the shared memory. Fixed arrays:
@@ -197,6 +205,7 @@ constexpr size_t end = pend + a16(sizeof(int4) * kMaxStages);               // t
 //   full, empty                            stage mbarriers: copies landed / compute warps done with the stage
 //   pacc, uacc                             phase times (profiling); the current unit's partial sums
 //   utab, pend                             this CTA's work units; the chunk in each stage awaiting its row sums
+//   state                                  CG scalars of each solve (SolveState), one spare entry
 // then prod (FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]) and the stage buffers at `stage` (kMaxStages x
 // stage_bytes, 128-aligned; also the direct-pass staging area and the tile-sum buffers of the pass sums).
 struct Smem {
@@ -218,6 +227,7 @@ struct Smem {
   __device__ __forceinline__ double* uacc() const { return at<double>(smo::uacc); }
   __device__ __forceinline__ int2* utab() const { return at<int2>(smo::utab); }
   __device__ __forceinline__ int4* pend() const { return at<int4>(smo::pend); }
+  __device__ __forceinline__ SolveState* state() const { return at<SolveState>(smo::state); }
   __device__ __forceinline__ double* prod() const { return at<double>(smo::end); }
 };
 
@@ -1213,6 +1223,18 @@ __device__ __forceinline__ void locate(const KParams& kp, int r, int& gi, int& i
   slot = rel - inst * kp.g[gi].nrhs;
 }
 
+// tolerance and iteration limit of solve r
+__device__ __forceinline__ double solve_tol(const KParams& kp, int r) {
+  int gi, inst, slot;
+  locate(kp, r, gi, inst, slot);
+  return kp.g[gi].tol[slot];
+}
+__device__ __forceinline__ int solve_max_iters(const KParams& kp, int r) {
+  int gi, inst, slot;
+  locate(kp, r, gi, inst, slot);
+  return kp.g[gi].max_iters[slot];
+}
+
 // publish the actions of this pass: act[] for every solve and opp[] for every operator
 __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, double my_c1, double my_c2) {
   const int tid = threadIdx.x;
@@ -1251,20 +1273,23 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   build_unit_table(kp, sm);
   __syncthreads();
 
-  // state of solve `tid` (identical in every CTA: computed from the same write-once sums)
+  // state of solve `tid` (identical in every CTA: computed from the same write-once sums), kept in shared
+  // memory so that it holds no registers while the passes run
   const bool own = tid < kp.total_rhs;
-  int gi = 0, inst = 0, slot = 0;
-  double tol2 = 0.0, rep2 = 0.0, rhsNorm = 1.0, rhsMax = 0.0, eta = 0.0, eta_prev = 1.0, alpha = 0.0, rr = 0.0;
-  int maxit = 0, k_done = -1, nrep = 0, has_alpha = 0;
+  SolveState* S = sm.state() + (own ? tid : kMaxSolves);
   if (own) {
+    int gi, inst, slot;
     locate(kp, tid, gi, inst, slot);
     const GroupDev& g = kp.g[gi];
-    tol2 = g.tol[slot] * g.tol[slot];                      // cg2d.py:219
-    rep2 = (kp.replace_above * g.tol[slot]) * (kp.replace_above * g.tol[slot]);
-    maxit = g.max_iters[slot];
     sm.norm()[tid] = g.norm_arr ? g.norm_arr[inst] : g.norm;
     sm.rnorm()[tid] = 1.0;
     sm.has_alpha()[tid] = 0;
+    S->eta = 0.0;
+    S->eta_prev = 1.0;
+    S->alpha = 0.0;
+    S->rr = 0.0;
+    S->k_done = -1;
+    S->nrep = 0;
   }
   int k = 0;
   bool ok = true;
@@ -1275,9 +1300,8 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   ok = grid_sync(kp, target, P_MAX, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) {
-    rhsMax = __longlong_as_double((long long)__ldcg(&kp.rmax[tid]));
-    rhsNorm = (rhsMax != 0.0) ? __ddiv_rn(1.0, rhsMax) : 1.0;
-    sm.rnorm()[tid] = rhsNorm;
+    const double rhsMax = __longlong_as_double((long long)__ldcg(&kp.rmax[tid]));
+    sm.rnorm()[tid] = (rhsMax != 0.0) ? __ddiv_rn(1.0, rhsMax) : 1.0;
   }
   // ---- x = x0 rhsNorm, r = b - A x, s = 0, err^2, sumRHS (cg2d.py:226-236)
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
@@ -1285,30 +1309,30 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   ok = run_pass_direct<MIXED>(kp, P_INIT, sm);
   ok = grid_sync(kp, target, P_INIT, 0, sm) && ok;
   if (!ok) goto epilogue;
-  if (own) rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
+  if (own) S->rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
   ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, 0, 0, sm, pp);
   ok = grid_sync(kp, target, P_Z, 0, sm) && ok;
   if (!ok) goto epilogue;
-  if (own) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
+  if (own) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
 
   for (k = 0;; ++k) {
     // stop rule before every iteration (cg2d.py:238-241)
     int a = A_NONE;
     double beta = 0.0;
-    if (own && k_done < 0) {
-      if (!(k < maxit) || rr < tol2) {
-        k_done = k;
+    if (own && S->k_done < 0) {
+      const double tol = solve_tol(kp, tid);
+      if (!(k < solve_max_iters(kp, tid)) || S->rr < tol * tol) {       // cg2d.py:219, 241
+        S->k_done = k;
         a = A_FIN;
       } else {
         a = A_ACTIVE;
-        beta = __ddiv_rn(eta, eta_prev);                   // cg2d.py:247
-        eta_prev = eta;                                     // cg2d.py:248
+        beta = __ddiv_rn(S->eta, S->eta_prev);                           // cg2d.py:247
+        S->eta_prev = S->eta;                                             // cg2d.py:248
       }
     }
-    if (own) sm.has_alpha()[tid] = has_alpha;
-    set_actions(kp, sm, a, beta, alpha);
+    set_actions(kp, sm, a, beta, own ? S->alpha : 0.0);
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
@@ -1318,40 +1342,40 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     if (!any_active) break;
     if (a == A_ACTIVE) {
       const double sq = __ldcg(hist_ptr(kp, tid, H_SQ, k));
-      alpha = __ddiv_rn(eta, sq);                           // cg2d.py:252-253
-      has_alpha = 1;
+      S->alpha = __ddiv_rn(S->eta, sq);                                   // cg2d.py:252-253
+      sm.has_alpha()[tid] = 1;                                            // read from the next pass on
     }
     // ---- r, z, err^2 and the next eta; or, every replace_every iterations (MIXED), the true residual
     int ax = A_NONE, ar = A_NONE;
     if (a == A_ACTIVE) {
-      const bool rep = kp.mixed && kp.replace_every > 0 && ((k + 1) % kp.replace_every) == 0 && rr > rep2;
-      if (rep) ar = A_ACTIVE;
+      const double rep = kp.replace_above * solve_tol(kp, tid);
+      if (kp.mixed && kp.replace_every > 0 && ((k + 1) % kp.replace_every) == 0 && S->rr > rep * rep) ar = A_ACTIVE;
       else ax = A_ACTIVE;
     }
     if (__syncthreads_or(ax != A_NONE)) {
-      set_actions(kp, sm, ax, alpha, 0.0);
+      set_actions(kp, sm, ax, own ? S->alpha : 0.0, 0.0);
       ok = run_pass_pipe<MIXED, MAXM>(kp, P_X, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_X, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
-        rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
-        eta = __ldcg(hist_ptr(kp, tid, H_ETAX, k + 1));
+        S->rr = __ldcg(hist_ptr(kp, tid, H_RRX, k + 1));
+        S->eta = __ldcg(hist_ptr(kp, tid, H_ETAX, k + 1));
       }
     }
     if (__syncthreads_or(ar != A_NONE)) {
-      set_actions(kp, sm, ar, alpha, 0.0);
+      set_actions(kp, sm, ar, own ? S->alpha : 0.0, 0.0);
       ok = run_pass_pipe<MIXED, MAXM>(kp, P_R, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_R, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
-        rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
-        ++nrep;
+        S->rr = __ldcg(hist_ptr(kp, tid, H_RRR, k + 1));
+        ++S->nrep;
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
       ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_Z, k + 1, sm) && ok;
       if (!ok) goto epilogue;
-      if (ar == A_ACTIVE) eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
+      if (ar == A_ACTIVE) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
     }
   }
 
@@ -1394,19 +1418,22 @@ epilogue:
     }
   }
   if (blockIdx.x == 0 && own) {
+    int gi, inst, slot;
+    locate(kp, tid, gi, inst, slot);
     const GroupDev& g = kp.g[gi];
+    const double rr = S->rr, tol = solve_tol(kp, tid);
     cg2d_diag_t d;
     d.firstResidual = sqrt(__ldcg(hist_ptr(kp, tid, H_RRR, 0)));
     d.lastResidual = sqrt(rr);
     d.sumRHS = __ldcg(hist_ptr(kp, tid, H_SUM, 0));
-    d.rhsMax = rhsMax;
-    d.numIters = k_done >= 0 ? k_done : k;
-    d.replacements = nrep;
+    d.rhsMax = __longlong_as_double((long long)__ldcg(&kp.rmax[tid]));
+    d.numIters = S->k_done >= 0 ? S->k_done : k;
+    d.replacements = S->nrep;
     d.reserved = 0;
     const unsigned err = __ldcg(&kp.gs[1]);
     if (!ok || err != 0u) d.status = err != 0u ? (int)err : CG2D_BARRIER_TIMEOUT;
     else if (rr != rr) d.status = CG2D_NAN;
-    else if (!(rr < tol2)) d.status = CG2D_NOT_CONVERGED;
+    else if (!(rr < tol * tol)) d.status = CG2D_NOT_CONVERGED;
     else d.status = CG2D_OK;
     if (!ok) { d.firstResidual = d.lastResidual = d.sumRHS = __longlong_as_double(0x7ff8000000000000LL); }
     g.diag[slot][inst] = d;
