@@ -99,6 +99,15 @@ def _cpu_inputs(count, tol, maxit):
     return out
 
 
+def arm_config(a, world):
+    """The workload both arms report: the batched LLC90 forward + adjoint step of this bench."""
+    return {"workload": f"batch {a.batch} LLC90 CG2D forward + adjoint (2 right-hand sides per instance, one "
+                        f"persistent launch) + edge products, {a.precision}",
+            "batch_per_gpu": a.batch, "tolerance": a.tol, "max_iters": a.maxit,
+            "grid": "LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"instances sharded, {world} GPU(s), no collective in the solve"}
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -119,11 +128,11 @@ def run_reference(a):
         "ms_per_step": 1e3 * statistics.mean(walls), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": "LLC90 CG2D forward + adjoint (tight) solve + coefficient cotangents, FP64, one "
-                               "instance per host process", "instances_per_step": procs, "tolerance": a.tol,
-                   "max_iters": a.maxit, "parallelism": f"{procs} processes"},
+        "config": arm_config(a, a.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
-                         "sample": f"{procs} LLC90 instances per step (one per process), {a.steps} steps"},
+                         "sample": f"each step: {procs} of the {a.batch} LLC90 instances (one per host process), "
+                                   f"FP64 forward (fortran sum order) + adjoint + coefficient cotangents by the "
+                                   f"oracle port of cg2d_fortran; {a.steps} steps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -368,11 +377,7 @@ def run_gpu(a):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": f"batch {a.batch} LLC90 CG2D forward + adjoint (2 right-hand sides per "
-                                   f"instance, one persistent launch) + edge products, {a.precision}",
-                       "batch_per_gpu": a.batch, "tolerance": a.tol, "max_iters": a.maxit,
-                       "grid": "LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"instances sharded, {world} GPU(s), no collective in the solve"},
+            "config": arm_config(a, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "cg2d_persistent (solver launch incl. FP32 pack)",
