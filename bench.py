@@ -232,11 +232,13 @@ def run_gpu(a):
     from mit_jax_b200 import cg2d as cg
     from mit_jax_b200.synthetic import make_batch
 
-    # inputs: this rank's own batch of members (weak scaling: disjoint members per rank)
-    syn, B = make_batch(90, a.batch, with_cotangent=True)
-    if rank:
-        # distinct members per rank: rotate the batch (different instance order) -- the work per rank is the same
-        B = {k: np.roll(v, rank, axis=0) for k, v in B.items()}
+    from mit_jax_b200.sharding import estimated_work, max_over_ranks, shard_instances
+
+    # inputs: this rank's own batch of members (weak scaling: world x batch members in all, disjoint per rank)
+    members = None
+    if world > 1:
+        members = shard_instances(estimated_work([N_LLC90] * (world * a.batch)), world, rank)
+    syn, B = make_batch(90, a.batch, with_cotangent=True, members=members)
     ex = cg.default_exchanger(syn.L)
     ops = tuple(torch.as_tensor(B[k]).to(dev) for k in cg.OPS)
     b = torch.as_tensor(B["b"]).to(dev)
@@ -277,10 +279,7 @@ def run_gpu(a):
     total_ms = ev[0][0].elapsed_time(ev[-1][2])
     solver_ms = [e[0].elapsed_time(e[1]) for e in ev]
     edge_ms = [e[1].elapsed_time(e[2]) for e in ev]
-    t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dev)
     ms_per_step = total_ms / a.steps
     value = world * a.batch / (ms_per_step / 1e3)
 
@@ -331,10 +330,8 @@ def run_gpu(a):
             e2e_step()
         e1.record(stream)
         barrier()
-        et = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * a.batch * a.steps / (float(et.item()) / 1e3), "unit": UNIT,
+        et = max_over_ranks(e0.elapsed_time(e1), dev)
+        e2e = {"value": world * a.batch * a.steps / (et / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     # ---- the plain FP64 one-solve-per-launch kernel: one instance, forward launch then adjoint launch

@@ -160,13 +160,15 @@ class LLCSynthetic:
         return np.zeros(self.L.shape2d)
 
 
-def make_batch(N=90, count=1, ts=None, with_cotangent=False):
-    """Stacked inputs of `count` members: dict of [count, T, ny, nx] arrays plus cg2dNorm [count]."""
+def make_batch(N=90, count=1, ts=None, with_cotangent=False, members=None):
+    """Stacked inputs of `count` members (or of the listed ensemble members): dict of [count, T, ny, nx] arrays plus
+    cg2dNorm [count]. A single member without a list is the unperturbed configuration."""
     syn = LLCSynthetic(N, ts)
     out = {k: [] for k in ("aW2d", "aS2d", "aC2d", "pW", "pS", "pC", "b", "x0", "w")}
     norms = []
-    for m in range(count):
-        member = None if count == 1 else m
+    if members is None:
+        members = [None] if count == 1 else list(range(count))
+    for member in members:
         ops, norm = syn.operator(member)
         for k, a in zip(("aW2d", "aS2d", "aC2d", "pW", "pS", "pC"), ops):
             out[k].append(a)
