@@ -151,6 +151,29 @@ cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2d
                              const cg2d_params_t* params,
                              void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
 
+/* Exact-mode adjoint: the cotangents of x_out = cg2d_solve_f64(...) (its interior) with respect to cg2d_b and to
+ * the six coefficient arrays, for J = <x_bar, x_out>, by reverse mode through the CG iterations that the forward
+ * took (each instance's numIters, read from fwd_diag, the diag of the forward solve). The "exact mode" of the
+ * solver; the reference has no counterpart (its JAX code cannot reverse a while_loop; it differentiates implicitly, which is
+ * cg2d_edge_products after an adjoint solve). The forward must be an FP64 ROWBLOCK solve with rows_per_block rows
+ * per block; the recording forward inside reproduces it bit for bit (x_check, nullable, receives its x_out).
+ * Memory: r and the previous search direction every checkpoint_every iterations (0 = one segment), and one
+ * segment's r, z, s, q; segments are recomputed from their checkpoint with the recorded alpha and beta.
+ * Outputs (device, [batch][T][ny][nx], written in full): b_bar (interior), gW/gS/gC and gpW/gpS/gpC on the
+ * faces and points edge_products writes. x0 is treated as constant (cg2d.py:372). Synchronises the stream once
+ * to read the forward's iteration counts (each must be <= max_iters, which sizes the workspace). */
+size_t cg2d_adjoint_exact_workspace_size(const cg2d_topology_t* topo, int batch, int max_iters,
+                                         int checkpoint_every);
+cg2d_status_t cg2d_adjoint_exact(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                 const double* cg2dNorm_per_instance,
+                                 const double* aW2d, const double* aS2d, const double* aC2d,
+                                 const double* pW, const double* pS, const double* pC,
+                                 const double* cg2d_b, const double* cg2d_x, const cg2d_diag_t* fwd_diag,
+                                 const double* x_bar, int max_iters, int rows_per_block, int checkpoint_every,
+                                 double* b_bar, double* gW, double* gS, double* gC,
+                                 double* gpW, double* gpS, double* gpC, double* x_check,
+                                 void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
+
 /* cg2d_solve_f64 without a caller workspace and without any allocation (no counterpart in the reference, whose
  * JAX arrays are allocated by XLA). For callers that cannot allocate device memory where they solve: a step
  * inside a framework that owns the whole device pool and hands a custom call only its operands, or code that

@@ -33,7 +33,7 @@ STATUS_NAMES = {0: "ok", 1: "not_converged", 2: "nan", 3: "barrier_timeout", 4: 
 EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_params", "cg2d_workspace_size",
             "cg2d_solve_groups", "cg2d_solve_f64", "cg2d_workspace_status", "cg2d_apply_operator",
             "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string", "cg2d_workspace_profile",
-            "cg2d_solve_f64_noalloc")
+            "cg2d_solve_f64_noalloc", "cg2d_adjoint_exact", "cg2d_adjoint_exact_workspace_size")
 
 
 class Params(ctypes.Structure):
@@ -92,6 +92,11 @@ def lib():
     L.cg2d_solve_f64_noalloc.argtypes = [_P, i, d, _P, _P, _P, _P, _P, _P, _P, _P, d, i, _P, _P, _P,
                                          ctypes.POINTER(Params), _P]
     L.cg2d_solve_f64_noalloc.restype = i
+    L.cg2d_adjoint_exact_workspace_size.argtypes = [_P, i, i, i]
+    L.cg2d_adjoint_exact_workspace_size.restype = ctypes.c_size_t
+    L.cg2d_adjoint_exact.argtypes = [_P, i, d, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, i, i, i,
+                                     _P, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_size_t, _P]
+    L.cg2d_adjoint_exact.restype = i
     L.cg2d_workspace_status.argtypes = [_P, _P]
     L.cg2d_workspace_status.restype = i
     L.cg2d_apply_operator.argtypes = [_P, i, d, _P, _P, _P, _P, _P, _P]

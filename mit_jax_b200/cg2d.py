@@ -352,6 +352,54 @@ def edge_products(ex, lam, x, cg2dNorm):
     return tuple(back(g.reshape(lead + tuple(ex.L.shape2d))) for g in (gW, gS, gC))
 
 
+def exact_adjoint(ex, ops, cg2d_b, cg2d_x, x_bar, *, cg2dNorm, tolerance, max_iters, rows_per_block=8,
+                  checkpoint_every=30, x_check=False):
+    """Exact-mode adjoint (cg2d_adjoint_exact): solve A x = b in FP64 (ROWBLOCK sums), then reverse through the
+    iterations that solve took. Returns (x, diag records, grads) with x the solution (interior, 0 on halos) and grads
+    a dict of the cotangents of J = <x_bar, x> with respect to cg2d_b ("b") and to the six coefficient arrays
+    (names of OPS); x0 is constant. checkpoint_every: iterations between checkpoints (0 = keep all). x_check=True
+    adds the recording forward's solution ("x_check"), which equals x bit for bit. Arrays [batch, T, ny, nx] or
+    [T, ny, nx]; cg2dNorm a float or a [batch] tensor."""
+    b, back = _dev(cg2d_b)
+    dev = b.device
+    lead = b.shape[:-3]
+    shp = (-1,) + tuple(ex.L.shape2d)
+    b = b.reshape(shp)
+    ops_t = tuple(_dev(a, dev)[0].reshape(shp) for a in ops)
+    x0 = _dev(cg2d_x, dev)[0].reshape(shp)
+    xb = _dev(x_bar, dev)[0].reshape(shp)
+    batch = b.shape[0]
+    norm = cg2dNorm
+    if isinstance(norm, np.ndarray):
+        norm = torch.as_tensor(norm)
+    with torch.cuda.device(dev):
+        G = GroupSpec(ex, ops_t, [b], [x0], [tolerance], [max_iters], norm)
+        (res,), = solve_groups([G], precision="f64", sum_order="rowblock", rows_per_block=rows_per_block)
+        x, _, dg = res
+        L = capi.lib()
+        topo = ex.handle(dev)
+        nbytes = L.cg2d_adjoint_exact_workspace_size(topo, batch, int(max_iters), int(checkpoint_every))
+        if nbytes == 0:
+            raise capi.Cg2dError(capi.CG2D_BAD_ARG, "cg2d_adjoint_exact_workspace_size")
+        ws = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+        base = ws.data_ptr() + (-ws.data_ptr()) % 256
+        outs = {k: torch.empty_like(b) for k in ("b",) + OPS}
+        xc = torch.empty_like(b) if x_check else None
+        norm_arr = norm.to(dev, torch.float64).contiguous() if isinstance(norm, torch.Tensor) else None
+        nval = 0.0 if norm_arr is not None else float(norm)
+        capi.check(L.cg2d_adjoint_exact(topo, batch, nval, _ptr(norm_arr), *(t.data_ptr() for t in ops_t),
+                                        b.data_ptr(), x0.data_ptr(), dg.data_ptr(), xb.data_ptr(), int(max_iters),
+                                        int(rows_per_block), int(checkpoint_every), outs["b"].data_ptr(),
+                                        *(outs[k].data_ptr() for k in OPS), _ptr(xc), base, nbytes, _stream(dev)),
+                   "cg2d_adjoint_exact")
+    shape = lead + tuple(ex.L.shape2d)
+    grads = {k: back(v.reshape(shape)) for k, v in outs.items()}
+    if xc is not None:
+        grads["x_check"] = back(xc.reshape(shape))
+    recs = diag_records(dg)
+    return back(x.reshape(shape)), (recs[0] if not lead else recs), grads
+
+
 # ----------------------------------------------------------------------------------------------------------------
 # differentiable solve
 

@@ -1,0 +1,519 @@
+// Exact-mode adjoint of the FP64 CG2D iteration: reverse mode through the iterations of cg2d_fortran
+// (mitgcm_jax/core/cg2d.py:205-269) as they were taken, with the iteration count of the forward solve.
+//
+// The reference has no such adjoint: its JAX code cannot reverse a while_loop and differentiates implicitly
+// (cg2d.py:307-348). This one differentiates the map b, A, M -> x_K of K literal CG iterations:
+//   forward, iteration k:  z = M r;  eta = <z, r>;  beta = eta / eta_prev;  s = z + beta s_prev;  q = A s;
+//                          sigma = <s, q>;  alpha = eta / sigma;  x += alpha s;  r -= alpha q
+//   reverse, iteration k (given rbar = rbar_{k+1}, sbar = beta_{k+1} sbar_{k+1}, the eta cotangent carried from
+//   iteration k+1, and xbar, which is constant):
+//     abar = <xbar, s> - <rbar, q>;  sigbar = -abar alpha / sigma;  etabar = carry + abar / sigma
+//     qbar = sigbar s - alpha rbar;  sbar += alpha xbar + sigbar q;  sbar += A qbar;  Abar += qbar (x) s
+//     bbar = <sbar, s_prev>;  etabar += bbar / eta_prev;  carry = -bbar eta / eta_prev^2
+//     zbar = sbar + etabar r;  rbar += etabar z;  sbar = beta sbar;  rbar += M zbar;  Mbar += zbar (x) r
+// and at the start r_0 = b_n - A x_0: bbar_n = rbar_0, Abar -= rbar_0 (x) x_0. A and M are symmetric operators,
+// so their transposes are themselves; (x) is the transpose of the stencil in its coefficients (edge products,
+// as for the implicit derivative). The normalisation by rhsNorm cancels (x_K is homogeneous of degree 1 in
+// (b, x_0)), so it enters only as the scale of b and x.
+//
+// Memory: the recording forward keeps r and s_prev every `checkpoint` iterations; the reverse sweep takes the
+// segments from the last, recomputes each one's r, z, s, q from its checkpoint with the stored alpha and beta
+// (bit for bit the recorded values), then reverses through it. The recording forward performs the same
+// floating-point operations in the same order as cg2d_solve_f64 (ROWBLOCK sums), so it reproduces its iterates
+// exactly.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "cg2d_internal.cuh"
+
+namespace cg2d {
+namespace {
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+
+// apply_operator / apply_preconditioner addition orders (cg2d.py:181-198)
+__device__ __forceinline__ double opA(double aw, double ae, double as, double an, double ac, double vw, double ve,
+                                     double vs, double vn, double vc) {
+  double t = mul(aw, vw);
+  t = add(t, mul(ae, ve));
+  t = add(t, mul(as, vs));
+  t = add(t, mul(an, vn));
+  return add(t, mul(ac, vc));
+}
+__device__ __forceinline__ double opM(double pc, double pw, double pe, double ps, double pn, double vc, double vw,
+                                     double ve, double vs, double vn) {
+  double t = mul(pc, vc);
+  t = add(t, mul(pw, vw));
+  t = add(t, mul(pe, ve));
+  t = add(t, mul(ps, vs));
+  return add(t, mul(pn, vn));
+}
+
+__device__ __forceinline__ long long padded(const TopoDev& tp, int t, int j, int i) {
+  return ((long long)t * tp.npy + j + tp.OLy) * tp.npx + i + tp.OLx;
+}
+__device__ __forceinline__ long long cmp_pad(const TopoDev& tp, int c) {
+  const int per = tp.nj * tp.ni;
+  const int t = c / per, rem = c - t * per, j = rem / tp.ni;
+  return padded(tp, t, j, rem - j * tp.ni);
+}
+// source of the value at (t, j, i), -1 <= i <= ni, -1 <= j <= nj (not a corner): its padded index in the same
+// instance, or -1 for an unwritten halo point
+__device__ __forceinline__ long long source(const TopoDev& tp, int t, int j, int i) {
+  if (i >= 0 && i < tp.ni && j >= 0 && j < tp.nj) return padded(tp, t, j, i);
+  int src;
+  if (i < 0) src = tp.nbr[t * tp.nj + j];
+  else if (i >= tp.ni) src = tp.nbr[tp.T * tp.nj + t * tp.nj + j];
+  else if (j < 0) src = tp.nbr[2 * tp.T * tp.nj + t * tp.ni + i];
+  else src = tp.nbr[2 * tp.T * tp.nj + tp.T * tp.ni + t * tp.ni + i];
+  return src >= 0 ? cmp_pad(tp, src) : -1;
+}
+// a CG vector at (t, j, i) as the exchange gives it: unwritten halo points read 0
+__device__ __forceinline__ double nbv(const TopoDev& tp, const double* v, int t, int j, int i) {
+  const long long s = source(tp, t, j, i);
+  return s >= 0 ? v[s] : 0.0;
+}
+// the normalised first guess at (t, j, i): interior points scaled, unwritten halo points keep cg2d_x
+// (cg2d.py:227-228)
+__device__ __forceinline__ double nbx0(const TopoDev& tp, const double* x0, double rn, int t, int j, int i) {
+  const long long s = source(tp, t, j, i);
+  return s >= 0 ? mul(x0[s], rn) : x0[padded(tp, t, j, i)];
+}
+
+struct Geo {
+  TopoDev tp;
+  int batch;
+  long long pe;   // padded elements per instance
+  long long pts;  // interior points per instance
+};
+__device__ __forceinline__ bool decode(const Geo& G, long long idx, int& in, int& t, int& j, int& i, long long& p) {
+  in = (int)(idx / G.pts);
+  const long long r = idx - (long long)in * G.pts;
+  const int per = G.tp.nj * G.tp.ni;
+  t = (int)(r / per);
+  const int r2 = (int)(r - (long long)t * per);
+  j = r2 / G.tp.ni;
+  i = r2 - j * G.tp.ni;
+  p = (long long)in * G.pe + padded(G.tp, t, j, i);
+  return in < G.batch;
+}
+#define FOR_POINTS(G)                                                                                      \
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (long long)(G).batch * (G).pts; \
+       idx += (long long)gridDim.x * blockDim.x)
+__device__ __forceinline__ bool live(const int* K, int in, int k) { return k < K[in]; }
+
+// r = b_n - A x0_n and x = x0_n on the interior, b_n = b cg2dNorm rhsNorm (cg2d.py:221-232)
+__global__ void k_init(Geo G, const double* aW, const double* aS, const double* aC, const double* b, const double* x0,
+                       const double* norm, const double* rn, double* r, double* x) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    const TopoDev& tp = G.tp;
+    const double* x0i = x0 + (long long)in * G.pe;
+    const double rni = rn[in];
+    const double vc = nbx0(tp, x0i, rni, t, j, i);
+    const double ax = opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], nbx0(tp, x0i, rni, t, j, i - 1),
+                          nbx0(tp, x0i, rni, t, j, i + 1), nbx0(tp, x0i, rni, t, j - 1, i),
+                          nbx0(tp, x0i, rni, t, j + 1, i), vc);
+    r[p] = sub(mul(mul(b[p], norm[in]), rni), ax);
+    x[p] = vc;
+  }
+}
+
+// out = [base +] A v (mode 0) or M v (mode 1) on the interior of live instances
+__global__ void k_stencil(Geo G, int mode, const double* c0, const double* c1, const double* c2, const double* v,
+                          const double* base, double* out, const int* K, int k) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    if (!live(K, in, k)) continue;
+    const TopoDev& tp = G.tp;
+    const double* vi = v + (long long)in * G.pe;
+    const double vw = nbv(tp, vi, t, j, i - 1), ve = nbv(tp, vi, t, j, i + 1);
+    const double vs = nbv(tp, vi, t, j - 1, i), vn = nbv(tp, vi, t, j + 1, i), vc = v[p];
+    const double o = mode == 0 ? opA(c0[p], c0[p + 1], c1[p], c1[p + tp.npx], c2[p], vw, ve, vs, vn, vc)
+                               : opM(c2[p], c0[p], c0[p + 1], c1[p], c1[p + tp.npx], vc, vw, ve, vs, vn);
+    out[p] = base ? add(base[p], o) : o;
+  }
+}
+
+// row sums of up to two products a0 b0, a1 b1 of live instances: rs[(in 2 + q)][t nj + j], one warp per row,
+// lane partials over i = lane + 32 m in order, then an xor butterfly (the solver's ROWBLOCK row sums)
+__global__ void k_rowdot(Geo G, const double* a0, const double* b0, const double* a1, const double* b1, double* rs,
+                         const int* K, int k) {
+  const int lane = threadIdx.x & 31;
+  const int rows = G.tp.T * G.tp.nj;
+  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < (long long)G.batch * rows;
+       w += nwarps) {
+    const int in = (int)(w / rows), row = (int)(w - (long long)in * rows);
+    if (!live(K, in, k)) continue;
+    const int t = row / G.tp.nj, j = row - t * G.tp.nj;
+    const long long p0 = (long long)in * G.pe + padded(G.tp, t, j, 0);
+    double s0 = 0.0, s1 = 0.0;
+    for (int i = lane; i < G.tp.ni; i += 32) {
+      s0 = add(s0, mul(a0[p0 + i], b0[p0 + i]));
+      if (a1) s1 = add(s1, mul(a1[p0 + i], b1[p0 + i]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 = add(s0, __shfl_xor_sync(0xffffffffu, s0, o));
+      s1 = add(s1, __shfl_xor_sync(0xffffffffu, s1, o));
+    }
+    if (lane == 0) {
+      rs[((long long)in * 2 + 0) * rows + row] = s0;
+      if (a1) rs[((long long)in * 2 + 1) * rows + row] = s1;
+    }
+  }
+}
+
+// the sums in ROWBLOCK order (rows of a block in order, blocks of a tile in order, tiles in order from 0)
+__device__ double fold(const Geo& G, int R, const double* rs) {
+  double total = 0.0;
+  for (int t = 0; t < G.tp.T; ++t) {
+    double ts = 0.0;
+    for (int j0 = 0; j0 < G.tp.nj; j0 += R) {
+      double u = 0.0;
+      for (int j = j0; j < min(G.tp.nj, j0 + R); ++j) u = add(u, rs[t * G.tp.nj + j]);
+      ts = add(ts, u);
+    }
+    total = add(total, ts);
+  }
+  return total;
+}
+
+// per-instance scalar steps, one thread per live instance; S = scalar arrays [kind][Kmax][batch]
+struct Scal {
+  double *eta, *beta, *sig, *alpha;   // [Kmax][batch] (recorded)
+  double *carry, *etabar, *sigbar;    // [batch] (reverse)
+};
+__global__ void k_fwd_eta(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= G.batch || !live(K, in, k)) return;
+  const int rows = G.tp.T * G.tp.nj;
+  const double eta = fold(G, R, rs + (long long)in * 2 * rows);                  // cg2d.py:246
+  const double eta_prev = k > 0 ? S.eta[(long long)(k - 1) * G.batch + in] : 1.0;
+  S.eta[(long long)k * G.batch + in] = eta;
+  S.beta[(long long)k * G.batch + in] = __ddiv_rn(eta, eta_prev);             // cg2d.py:247
+}
+__global__ void k_fwd_sigma(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= G.batch || !live(K, in, k)) return;
+  const int rows = G.tp.T * G.tp.nj;
+  const double sig = fold(G, R, rs + (long long)in * 2 * rows);                  // cg2d.py:252
+  S.sig[(long long)k * G.batch + in] = sig;
+  S.alpha[(long long)k * G.batch + in] = __ddiv_rn(S.eta[(long long)k * G.batch + in], sig);   // cg2d.py:253
+}
+// reverse: abar = <xbar, s> - <rbar, q>
+__global__ void k_rev_alpha(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= G.batch || !live(K, in, k)) return;
+  const int rows = G.tp.T * G.tp.nj;
+  const double abar = fold(G, R, rs + (long long)in * 2 * rows) - fold(G, R, rs + ((long long)in * 2 + 1) * rows);
+  const long long o = (long long)k * G.batch + in;
+  S.sigbar[in] = -abar * S.alpha[o] / S.sig[o];
+  S.etabar[in] = S.carry[in] + abar / S.sig[o];
+}
+// reverse: bbar = <sbar, s_prev>
+__global__ void k_rev_beta(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= G.batch || !live(K, in, k)) return;
+  if (k == 0) { S.carry[in] = 0.0; return; }   // eta_{-1} = 1 is a constant, s_{-1} = 0
+  const int rows = G.tp.T * G.tp.nj;
+  const double bbar = fold(G, R, rs + (long long)in * 2 * rows);
+  const double eta = S.eta[(long long)k * G.batch + in], etap = S.eta[(long long)(k - 1) * G.batch + in];
+  S.etabar[in] += bbar / etap;
+  S.carry[in] = -bbar * eta / (etap * etap);
+}
+
+// forward updates of live instances
+__global__ void k_fwd_s(Geo G, const double* z, const double* sprev, double* s, Scal S, const int* K, int k) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    if (!live(K, in, k)) continue;
+    s[p] = add(z[p], mul(S.beta[(long long)k * G.batch + in], sprev[p]));        // cg2d.py:249
+  }
+}
+__global__ void k_fwd_rx(Geo G, const double* s, const double* q, const double* r, double* rout, double* x, Scal S,
+                         const int* K, int k) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    if (!live(K, in, k)) continue;
+    const double a = S.alpha[(long long)k * G.batch + in];
+    if (x) x[p] = add(x[p], mul(a, s[p]));                                      // cg2d.py:254
+    rout[p] = sub(r[p], mul(a, q[p]));                                          // cg2d.py:255
+  }
+}
+// reverse: qbar = sigbar s - alpha rbar;  sbar += alpha xbar + sigbar q
+__global__ void k_rev_q(Geo G, const double* s, const double* q, const double* xbar, const double* rbar, double* qbar,
+                        double* sbar, Scal S, const int* K, int k) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    if (!live(K, in, k)) continue;
+    const double a = S.alpha[(long long)k * G.batch + in], sg = S.sigbar[in];
+    qbar[p] = sg * s[p] - a * rbar[p];
+    sbar[p] = sbar[p] + a * xbar[p] + sg * q[p];
+  }
+}
+// reverse: zbar = sbar + etabar r;  rbar += etabar z;  sbar = beta sbar
+__global__ void k_rev_z(Geo G, const double* r, const double* z, double* zbar, double* rbar, double* sbar, Scal S,
+                        const int* K, int k) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    if (!live(K, in, k)) continue;
+    const double e = S.etabar[in];
+    zbar[p] = sbar[p] + e * r[p];
+    rbar[p] = rbar[p] + e * z[p];
+    sbar[p] = S.beta[(long long)k * G.batch + in] * sbar[p];
+  }
+}
+
+// coefficient cotangents of a stencil application out = C v: gW/gS/gC += sign (u (x) v) on the faces and points
+// of live instances, u the cotangent of out (interior), v the stencil input as the stencil read it (X0: the
+// first-guess rule); the same faces as edge_products_kernel
+template <bool X0>
+__global__ void k_edges(Geo G, const double* u, const double* v, const double* rn, double sign, double* gW,
+                        double* gS, double* gC, const int* K, int k) {
+  const TopoDev& tp = G.tp;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (long long)G.batch * G.pe;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int in = (int)(idx / G.pe);
+    if (K && !live(K, in, k)) continue;
+    const long long pp = idx - (long long)in * G.pe;
+    const int plane = tp.npy * tp.npx;
+    const int t = (int)(pp / plane);
+    const int rem = (int)(pp - (long long)t * plane);
+    const int j = rem / tp.npx - tp.OLy, i = rem - (rem / tp.npx) * tp.npx - tp.OLx;
+    const double* ui = u + (long long)in * G.pe;
+    const double* vi = v + (long long)in * G.pe;
+    auto V = [&](int jj, int ii) -> double {
+      return X0 ? nbx0(tp, vi, rn[in], t, jj, ii) : nbv(tp, vi, t, jj, ii);
+    };
+    auto U = [&](int jj, int ii) -> double { return ui[padded(tp, t, jj, ii)]; };
+    const bool jin = j >= 0 && j < tp.nj, iin = i >= 0 && i < tp.ni;
+    if (jin && i >= 0 && i <= tp.ni) {   // face between (j, i-1) and (j, i)
+      double a = 0.0;
+      if (i < tp.ni) a += U(j, i) * V(j, i - 1);
+      if (i >= 1) a += U(j, i - 1) * V(j, i);
+      gW[idx] += sign * a;
+    }
+    if (iin && j >= 0 && j <= tp.nj) {   // face between (j-1, i) and (j, i)
+      double a = 0.0;
+      if (j < tp.nj) a += U(j, i) * V(j - 1, i);
+      if (j >= 1) a += U(j - 1, i) * V(j, i);
+      gS[idx] += sign * a;
+    }
+    if (jin && iin) gC[idx] += sign * U(j, i) * V(j, i);
+  }
+}
+
+// xbar_K = xbar_out / rhsNorm on the interior;  bbar = rbar_0 cg2dNorm rhsNorm on the interior
+__global__ void k_scale(Geo G, const double* in_, const double* norm, const double* rn, double* out, int mode) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    out[p] = mode == 0 ? in_[p] / rn[in] : in_[p] * norm[in] * rn[in];
+  }
+}
+// x_out of the recording forward: x / rhsNorm on the interior (cg2d.py:266)
+__global__ void k_xout(Geo G, const double* x, const double* rn, double* out) {
+  FOR_POINTS(G) {
+    int in, t, j, i;
+    long long p;
+    decode(G, idx, in, t, j, i, p);
+    out[p] = __ddiv_rn(x[p], rn[in]);
+  }
+}
+// per-instance rhsNorm from the forward's rhsMax (cg2d.py:225) and cg2dNorm, iteration counts
+__global__ void k_setup(int batch, const cg2d_diag_t* diag, double norm, const double* norm_arr, double* rn,
+                        double* nrm, int* K) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= batch) return;
+  const double m = diag[in].rhsMax;
+  rn[in] = (m != 0.0) ? __ddiv_rn(1.0, m) : 1.0;
+  nrm[in] = norm_arr ? norm_arr[in] : norm;
+  K[in] = diag[in].numIters;
+}
+
+int grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)std::max(1ll, std::min(b, 148ll * 16));
+}
+
+}  // namespace
+
+size_t exact_adjoint_workspace(const TopoDev& tp, int batch, int max_iters, int checkpoint) {
+  const size_t pe = (size_t)tp.T * tp.npy * tp.npx, vec = pe * batch * sizeof(double);
+  const int C = checkpoint > 0 ? checkpoint : std::max(1, max_iters);
+  const int nseg = (max_iters + C - 1) / C;
+  const size_t rows = (size_t)tp.T * tp.nj;
+  size_t b = 0;
+  b += vec * 5;                                   // r, s, z, q, x of the recording forward
+  b += vec * 2 * (size_t)std::max(1, nseg);       // checkpoints: r_c, s_{c-1}
+  b += vec * 4 * (size_t)C;                       // a segment's r, z, s, q
+  b += vec * 5;                                   // xbar, rbar, sbar, zbar, qbar
+  b += sizeof(double) * batch * 2 * rows;         // row sums
+  b += sizeof(double) * ((size_t)4 * std::max(1, max_iters) * batch + 5 * batch);   // scalars, rn, norm
+  b += sizeof(int) * batch;
+  b += 256 * (size_t)(30 + 2 * std::max(1, nseg) + 4 * C);   // each buffer starts 256-byte aligned
+  return b;
+}
+
+cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaStream_t st) {
+  Geo G;
+  G.tp = tp;
+  G.batch = A.batch;
+  G.pe = (long long)tp.T * tp.npy * tp.npx;
+  G.pts = (long long)tp.T * tp.nj * tp.ni;
+  const int Kmax = A.max_iters;
+  const int C = A.checkpoint > 0 ? A.checkpoint : std::max(1, Kmax);
+  const int nseg = (Kmax + C - 1) / C;
+  const size_t vecn = (size_t)G.pe * A.batch;
+  const int rows = tp.T * tp.nj;
+  char* w = static_cast<char*>(ws);
+  auto take = [&](size_t bytes) { char* p = w; w += (bytes + 255) & ~size_t(255); return p; };
+  auto vec = [&]() { return reinterpret_cast<double*>(take(vecn * sizeof(double))); };
+  double *r = vec(), *s = vec(), *z = vec(), *q = vec(), *x = vec();
+  std::vector<double*> ck_r(std::max(1, nseg)), ck_s(std::max(1, nseg));
+  for (int c = 0; c < std::max(1, nseg); ++c) { ck_r[c] = vec(); ck_s[c] = vec(); }
+  std::vector<double*> sg_r(C), sg_z(C), sg_s(C), sg_q(C);
+  for (int c = 0; c < C; ++c) { sg_r[c] = vec(); sg_z[c] = vec(); sg_s[c] = vec(); sg_q[c] = vec(); }
+  double *xbar = vec(), *rbar = vec(), *sbar = vec(), *zbar = vec(), *qbar = vec();
+  double* rs = reinterpret_cast<double*>(take(sizeof(double) * A.batch * 2 * rows));
+  Scal S;
+  const size_t kb = (size_t)std::max(1, Kmax) * A.batch * sizeof(double);
+  S.eta = reinterpret_cast<double*>(take(kb));
+  S.beta = reinterpret_cast<double*>(take(kb));
+  S.sig = reinterpret_cast<double*>(take(kb));
+  S.alpha = reinterpret_cast<double*>(take(kb));
+  S.carry = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
+  S.etabar = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
+  S.sigbar = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
+  double* rn = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
+  double* nrm = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
+  int* K = reinterpret_cast<int*>(take(sizeof(int) * A.batch));
+
+  const int gp = grid_for((long long)A.batch * G.pts), ge = grid_for((long long)A.batch * G.pe);
+  const int gw = grid_for((long long)A.batch * rows * 32), gi = (A.batch + 127) / 128;
+  const size_t vb = vecn * sizeof(double);
+  cudaError_t e;
+#define CK(x)                              \
+  do {                                     \
+    if ((e = (x)) != cudaSuccess) return e; \
+  } while (0)
+#define LK()                                  \
+  do {                                        \
+    if ((e = cudaGetLastError()) != cudaSuccess) return e; \
+  } while (0)
+  CK(cudaMemsetAsync(s, 0, vb, st));          // s_{-1} = 0
+  for (double* g : {A.gW, A.gS, A.gC, A.gpW, A.gpS, A.gpC, A.b_bar}) CK(cudaMemsetAsync(g, 0, vb, st));
+  for (double* v : {xbar, rbar, sbar, zbar, qbar}) CK(cudaMemsetAsync(v, 0, vb, st));
+  CK(cudaMemsetAsync(S.carry, 0, sizeof(double) * A.batch, st));
+  k_setup<<<gi, 128, 0, st>>>(A.batch, A.fwd_diag, A.norm, A.norm_arr, rn, nrm, K);
+  LK();
+  k_init<<<gp, 256, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
+  LK();
+
+  // ---- recording forward: scalars of every iteration, checkpoints of r and s_prev
+  double* sprev = s;
+  double* snew = sg_s[0];   // scratch until the segments are recomputed
+  for (int k = 0; k < Kmax; ++k) {
+    if (k % C == 0) {
+      CK(cudaMemcpyAsync(ck_r[k / C], r, vb, cudaMemcpyDeviceToDevice, st));
+      CK(cudaMemcpyAsync(ck_s[k / C], sprev, vb, cudaMemcpyDeviceToDevice, st));
+    }
+    k_stencil<<<gp, 256, 0, st>>>(G, 1, A.pW, A.pS, A.pC, r, nullptr, z, K, k);
+    LK();
+    k_rowdot<<<gw, 256, 0, st>>>(G, z, r, nullptr, nullptr, rs, K, k);
+    LK();
+    k_fwd_eta<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+    LK();
+    k_fwd_s<<<gp, 256, 0, st>>>(G, z, sprev, snew, S, K, k);
+    LK();
+    k_stencil<<<gp, 256, 0, st>>>(G, 0, A.aW, A.aS, A.aC, snew, nullptr, q, K, k);
+    LK();
+    k_rowdot<<<gw, 256, 0, st>>>(G, snew, q, nullptr, nullptr, rs, K, k);
+    LK();
+    k_fwd_sigma<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+    LK();
+    k_fwd_rx<<<gp, 256, 0, st>>>(G, snew, q, r, r, x, S, K, k);
+    LK();
+    std::swap(sprev, snew);
+  }
+  if (A.x_check) {
+    k_xout<<<gp, 256, 0, st>>>(G, x, rn, A.x_check);
+    LK();
+  }
+
+  // ---- reverse sweep, segment by segment from the last
+  k_scale<<<gp, 256, 0, st>>>(G, A.xbar, nrm, rn, xbar, 0);
+  LK();
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int c0 = seg * C, c1 = std::min(Kmax, c0 + C);
+    // recompute the segment's r, z, s, q with the recorded alpha and beta
+    CK(cudaMemcpyAsync(sg_r[0], ck_r[seg], vb, cudaMemcpyDeviceToDevice, st));
+    for (int k = c0; k < c1; ++k) {
+      const int m = k - c0;
+      const double* sp = m == 0 ? ck_s[seg] : sg_s[m - 1];
+      k_stencil<<<gp, 256, 0, st>>>(G, 1, A.pW, A.pS, A.pC, sg_r[m], nullptr, sg_z[m], K, k);
+      LK();
+      k_fwd_s<<<gp, 256, 0, st>>>(G, sg_z[m], sp, sg_s[m], S, K, k);
+      LK();
+      k_stencil<<<gp, 256, 0, st>>>(G, 0, A.aW, A.aS, A.aC, sg_s[m], nullptr, sg_q[m], K, k);
+      LK();
+      if (m + 1 < c1 - c0) {
+        k_fwd_rx<<<gp, 256, 0, st>>>(G, sg_s[m], sg_q[m], sg_r[m], sg_r[m + 1], nullptr, S, K, k);
+        LK();
+      }
+    }
+    for (int k = c1 - 1; k >= c0; --k) {
+      const int m = k - c0;
+      const double* sp = m == 0 ? ck_s[seg] : sg_s[m - 1];
+      k_rowdot<<<gw, 256, 0, st>>>(G, xbar, sg_s[m], rbar, sg_q[m], rs, K, k);
+      LK();
+      k_rev_alpha<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+      LK();
+      k_rev_q<<<gp, 256, 0, st>>>(G, sg_s[m], sg_q[m], xbar, rbar, qbar, sbar, S, K, k);
+      LK();
+      k_stencil<<<gp, 256, 0, st>>>(G, 0, A.aW, A.aS, A.aC, qbar, sbar, sbar, K, k);
+      LK();
+      k_edges<false><<<ge, 256, 0, st>>>(G, qbar, sg_s[m], rn, 1.0, A.gW, A.gS, A.gC, K, k);
+      LK();
+      k_rowdot<<<gw, 256, 0, st>>>(G, sbar, sp, nullptr, nullptr, rs, K, k);
+      LK();
+      k_rev_beta<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+      LK();
+      k_rev_z<<<gp, 256, 0, st>>>(G, sg_r[m], sg_z[m], zbar, rbar, sbar, S, K, k);
+      LK();
+      k_stencil<<<gp, 256, 0, st>>>(G, 1, A.pW, A.pS, A.pC, zbar, rbar, rbar, K, k);
+      LK();
+      k_edges<false><<<ge, 256, 0, st>>>(G, zbar, sg_r[m], rn, 1.0, A.gpW, A.gpS, A.gpC, K, k);
+      LK();
+    }
+  }
+  // r_0 = b_n - A x0_n: the cotangents of b and, through x0_n, of A
+  k_scale<<<gp, 256, 0, st>>>(G, rbar, nrm, rn, A.b_bar, 1);
+  LK();
+  k_edges<true><<<ge, 256, 0, st>>>(G, rbar, A.x0, rn, -1.0, A.gW, A.gS, A.gC, nullptr, 0);
+  LK();
+#undef CK
+#undef LK
+  return cudaSuccess;
+}
+
+}  // namespace cg2d

@@ -448,6 +448,53 @@ cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2d
   return cg2d_solve_groups(&g, 1, params, workspace, workspace_bytes, stream);
 }
 
+size_t cg2d_adjoint_exact_workspace_size(const cg2d_topology_t* topo, int batch, int max_iters,
+                                         int checkpoint_every) {
+  if (!topo || batch < 1 || max_iters < 0 || checkpoint_every < 0) return 0;
+  return exact_adjoint_workspace(topo_dev(topo), batch, max_iters, checkpoint_every);
+}
+
+cg2d_status_t cg2d_adjoint_exact(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                 const double* cg2dNorm_per_instance, const double* aW2d, const double* aS2d,
+                                 const double* aC2d, const double* pW, const double* pS, const double* pC,
+                                 const double* cg2d_b, const double* cg2d_x, const cg2d_diag_t* fwd_diag,
+                                 const double* x_bar, int max_iters, int rows_per_block, int checkpoint_every,
+                                 double* b_bar, double* gW, double* gS, double* gC, double* gpW, double* gpS,
+                                 double* gpC, double* x_check, void* workspace, size_t workspace_bytes,
+                                 cg2d_stream_t stream_) {
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  if (!topo || batch < 1 || max_iters < 0 || checkpoint_every < 0 || rows_per_block < 1) return CG2D_BAD_ARG;
+  for (const void* p : {(const void*)aW2d, (const void*)aS2d, (const void*)aC2d, (const void*)pW, (const void*)pS,
+                        (const void*)pC, (const void*)cg2d_b, (const void*)cg2d_x, (const void*)fwd_diag,
+                        (const void*)x_bar, (const void*)b_bar, (const void*)gW, (const void*)gS, (const void*)gC,
+                        (const void*)gpW, (const void*)gpS, (const void*)gpC})
+    if (!p) return CG2D_BAD_ARG;
+  const size_t need = exact_adjoint_workspace(topo_dev(topo), batch, max_iters, checkpoint_every);
+  if (!workspace || (reinterpret_cast<uintptr_t>(workspace) % kAlign) != 0) return CG2D_BAD_ARG;
+  if (workspace_bytes < need) return CG2D_WORKSPACE_TOO_SMALL;
+  // the forward's iteration counts bound the reverse sweep: read them once
+  std::vector<cg2d_diag_t> d((size_t)batch);
+  if (cudaMemcpyAsync(d.data(), fwd_diag, sizeof(cg2d_diag_t) * batch, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  int kmax = 0;
+  for (const cg2d_diag_t& r : d) {
+    if (r.numIters < 0 || r.numIters > max_iters) return CG2D_BAD_ARG;
+    kmax = r.numIters > kmax ? r.numIters : kmax;
+  }
+  ExactArgs a;
+  a.batch = batch;
+  a.max_iters = kmax;
+  a.checkpoint = checkpoint_every;
+  a.rows_per_block = rows_per_block;
+  a.norm = cg2dNorm;
+  a.norm_arr = cg2dNorm_per_instance;
+  a.aW = aW2d; a.aS = aS2d; a.aC = aC2d; a.pW = pW; a.pS = pS; a.pC = pC;
+  a.b = cg2d_b; a.x0 = cg2d_x; a.xbar = x_bar; a.fwd_diag = fwd_diag;
+  a.b_bar = b_bar; a.gW = gW; a.gS = gS; a.gC = gC; a.gpW = gpW; a.gpS = gpS; a.gpC = gpC; a.x_check = x_check;
+  if (exact_adjoint(topo_dev(topo), a, workspace, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
 cg2d_status_t cg2d_workspace_status(const void* workspace, cg2d_stream_t stream) {
   if (!workspace) return CG2D_BAD_ARG;
   if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }

@@ -158,6 +158,18 @@ constexpr int kMaxCtas = 148 * 8;
 enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FIN = 4, PR_DIRECT = 5, PR_OTHER = 6,
                        PR_TOTAL = 7, PR_DRAIN = 8, PR_RWAIT = 9, PR_CTRL = 10, PR_PWAIT = 11, kProfSlots = 12 };
 
+// exact-mode adjoint (cg2d_adjoint.cu)
+struct ExactArgs {
+  int batch, max_iters, checkpoint, rows_per_block;
+  double norm;
+  const double* norm_arr;
+  const double *aW, *aS, *aC, *pW, *pS, *pC, *b, *x0, *xbar;
+  const cg2d_diag_t* fwd_diag;
+  double *b_bar, *gW, *gS, *gC, *gpW, *gpS, *gpC, *x_check;
+};
+size_t exact_adjoint_workspace(const TopoDev& tp, int batch, int max_iters, int checkpoint);
+cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& args, void* workspace, cudaStream_t stream);
+
 // launchers (cg2d_solver.cu)
 size_t fixed_smem_bytes(int max_ni, int serial);
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream);

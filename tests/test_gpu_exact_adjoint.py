@@ -1,0 +1,105 @@
+"""Exact-mode adjoint on the GPU (cg2d_adjoint_exact, reverse mode through the CG iterations the forward took):
+its recording forward equals the FP64 solve bit for bit; its gradients equal torch autograd through the same
+iterations (oracle/cg2d_exact_oracle.py) to rounding, for single and batched solves, whatever the checkpoint
+interval; and at a tight tolerance they approach the implicit derivative (measured here, not assumed)."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import cg2d_oracle as O
+from oracle.cg2d_exact_oracle import cg2d_exact_grad
+
+pytestmark = pytest.mark.gpu
+
+cg = pytest.importorskip("mit_jax_b200.cg2d")
+NAMES = ("b",) + cg.OPS
+
+
+def _np(a):
+    return a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+
+
+def _rel(a, b):
+    a, b = _np(a), _np(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def small():
+    from mit_jax_b200.synthetic import LLCSynthetic
+    syn = LLCSynthetic(16, 8, 4)
+    return syn, cg.default_exchanger(syn.L)
+
+
+def test_exact_adjoint_matches_autograd(small):
+    """Six iterations (tolerance 0): every gradient equals autograd's; converged (1e-12): the recording forward is
+    the solve bit for bit, and the gradients in b and in the operator equal autograd's. (At convergence the
+    preconditioner moves x only through the residual: its gradients are rounding-level there.)"""
+    syn, ex = small
+    L, tmap = syn.L, syn.topo.maps["T"]
+    inner = O.interior_mask(L)
+    ops, norm = syn.operator()
+    b, x0 = syn.rhs(), syn.first_guess()
+    w = np.random.default_rng(3).standard_normal(L.shape2d) * inner
+    x, d, g = cg.exact_adjoint(ex, ops, b, x0, w, cg2dNorm=norm, tolerance=0.0, max_iters=6, checkpoint_every=4)
+    assert d["numIters"] == 6
+    _, go = cg2d_exact_grad(L, tmap, ops, b, x0, w, cg2dNorm=norm, iters=6)
+    for k in NAMES:
+        assert _rel(g[k], go[k]) < 1e-10, (k, _rel(g[k], go[k]))
+    x, d, g = cg.exact_adjoint(ex, ops, b, x0, w, cg2dNorm=norm, tolerance=1e-12, max_iters=300,
+                               checkpoint_every=10, x_check=True)
+    np.testing.assert_array_equal(_np(g["x_check"])[:, inner], _np(x)[:, inner])
+    xo, go = cg2d_exact_grad(L, tmap, ops, b, x0, w, cg2dNorm=norm, iters=d["numIters"])
+    assert _rel(_np(x), xo) < 1e-13
+    for k in ("b", "aW2d", "aS2d", "aC2d"):
+        assert _rel(g[k], go[k]) < 1e-8, (k, _rel(g[k], go[k]))
+
+
+def test_exact_adjoint_checkpoints_and_batch(small):
+    """Three members with their own operators and iteration counts in one call; checkpoint intervals 0 (one
+    segment), 4 and 30 give the same gradients bit for bit, each equal to its member's autograd gradient (b and
+    the operator)."""
+    from mit_jax_b200.synthetic import make_batch
+    syn, B = make_batch(16, ts=8, members=[0, 1, 2])
+    ex = cg.default_exchanger(syn.L)
+    L, tmap = syn.L, syn.topo.maps["T"]
+    # right-hand sides whose oracle solves take 37, 39 and 36 iterations at tolerance 1e-12
+    B["b"][1] = O.interior_mask(L).astype(np.float64)
+    B["b"][2] = B["b"][2] ** 2 * np.sign(B["b"][2])
+    rng = np.random.default_rng(4)
+    w = rng.standard_normal((3,) + L.shape2d) * O.interior_mask(L)
+    ops = tuple(torch.as_tensor(B[k]).cuda() for k in cg.OPS)
+    norm = torch.as_tensor(B["cg2dNorm"])
+    runs = [cg.exact_adjoint(ex, ops, torch.as_tensor(B["b"]).cuda(), torch.as_tensor(B["x0"]).cuda(),
+                             torch.as_tensor(w).cuda(), cg2dNorm=norm, tolerance=1e-12, max_iters=300,
+                             checkpoint_every=c) for c in (0, 4, 30)]
+    for _, _, g in runs[1:]:
+        for k in NAMES:
+            torch.testing.assert_close(g[k], runs[0][2][k], rtol=0, atol=0)
+    x, d, g = runs[0]
+    assert len({r["numIters"] for r in d}) == 3, [r["numIters"] for r in d]
+    for m in range(3):
+        ops_m = tuple(B[k][m] for k in cg.OPS)
+        _, go = cg2d_exact_grad(L, tmap, ops_m, B["b"][m], B["x0"][m], w[m], cg2dNorm=B["cg2dNorm"][m],
+                                iters=d[m]["numIters"])
+        for k in ("b", "aW2d", "aS2d", "aC2d"):
+            assert _rel(g[k][m], go[k]) < 1e-8, (m, k)
+
+
+def test_exact_adjoint_approaches_implicit(small):
+    """At tolerance 1e-13 the exact derivative of the iteration and the implicit derivative of the converged
+    solution (cg2d.py:318-348) differ by O(residual): here well below 1e-6 relative in d/db and d/d(aW2d)."""
+    syn, ex = small
+    L = syn.L
+    ops, norm = syn.operator()
+    b, x0 = syn.rhs(), syn.first_guess()
+    w = np.random.default_rng(5).standard_normal(L.shape2d) * O.interior_mask(L)
+    _, _, g = cg.exact_adjoint(ex, ops, b, x0, w, cg2dNorm=norm, tolerance=1e-13, max_iters=1000)
+    p = cg.Cg2dParams(cg2dMaxIters=1000, cg2dTolerance=1e-13, cg2dNorm=norm, sum_order="rowblock")
+    bt = torch.as_tensor(b).cuda().requires_grad_(True)
+    opt = [torch.as_tensor(a).cuda().requires_grad_(i < 3) for i, a in enumerate(ops)]
+    xi, _ = cg.cg2d_solve(p, ex, tuple(opt), bt, torch.as_tensor(x0).cuda())
+    (xi * torch.as_tensor(w).cuda()).sum().backward()
+    assert _rel(g["b"], bt.grad) < 1e-6
+    assert _rel(g["aW2d"], opt[0].grad) < 1e-6
