@@ -8,9 +8,15 @@ instance sharing its operator in ONE persistent mixed-precision launch, followed
 (coefficient gradients of J = <w, x>). Unit: forward+adjoint solve pairs per second, whole job.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+  python bench.py --mode exact [--batch 16 --checkpoint 30]
 
 --impl reference times the reference's CPU path (the oracle restatement of cg2d_fortran, FP64, forward + tight
 adjoint solve + coefficient cotangents) on all host cores, one instance per process.
+
+--mode exact times the exact-mode adjoint instead (cg2d_adjoint_exact: FP64 forward, then reverse mode through
+every CG iteration with checkpointed, recomputed segments; default batch 16) and reports adjoint solves/s and the
+peak device memory of the step. The reference has no exact mode (it differentiates cg2d implicitly), so
+--impl reference --mode exact reports itself unavailable.
 """
 
 import argparse
@@ -39,14 +45,19 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--mode", default="forward_adjoint", choices=("forward_adjoint", "exact"))
+    ap.add_argument("--batch", type=int, default=None, help="instances per GPU (64; 16 with --mode exact)")
+    ap.add_argument("--checkpoint", type=int, default=30, help="--mode exact: iterations between checkpoints")
     ap.add_argument("--precision", default="mixed", choices=("mixed", "f64"))
     ap.add_argument("--tol", type=float, default=1e-12)
     ap.add_argument("--maxit", type=int, default=300)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.batch is None:
+        a.batch = 16 if a.mode == "exact" else 64
+    return a
 
 
 # ------------------------------------------------------------------------------------------------------------------
@@ -216,6 +227,14 @@ def algorithmic_bytes(diag_f, diag_a, precision):
     return tot
 
 
+def _gpu_uuid(torch, dev):
+    """The device's UUID as nvidia-smi -i accepts it (falls back to the ordinal)."""
+    u = getattr(torch.cuda.get_device_properties(dev), "uuid", None)
+    if u is None:
+        return dev.index
+    return str(u) if str(u).startswith("GPU-") else f"GPU-{u}"
+
+
 def run_gpu(a):
     import torch
     import torch.distributed as dist
@@ -263,9 +282,7 @@ def run_gpu(a):
         cg.edge_products(ex, slots[1][0], slots[0][0], norms)
     barrier()
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(a.steps)]
-    gpu_id = getattr(torch.cuda.get_device_properties(dev), "uuid", None)
-    gpu_id = f"GPU-{gpu_id}" if gpu_id is not None and not str(gpu_id).startswith("GPU-") else (gpu_id or local)
-    with Clocks(gpu_id) as clk:
+    with Clocks(_gpu_uuid(torch, dev)) as clk:
         time.sleep(0.25)
         barrier()
         for s in range(a.steps):
@@ -399,8 +416,192 @@ def run_gpu(a):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------------------------
+# exact-mode adjoint
+
+EXACT_METRIC = "CG2D exact-mode adjoint solves/s (FP64 forward + reverse through every iteration) on B200"
+
+
+def exact_config(a):
+    return {"workload": f"batch {a.batch} LLC90 exact-mode adjoint: FP64 ROWBLOCK forward to {a.tol:g}, reverse "
+                        f"through every iteration, r and s_prev checkpointed every {a.checkpoint} iterations, "
+                        f"segments recomputed with the recorded alpha and beta; gradients of <w, x> w.r.t. b and "
+                        f"all six coefficient arrays",
+            "batch_per_gpu": a.batch, "tolerance": a.tol, "max_iters": a.maxit, "checkpoint_every": a.checkpoint,
+            "grid": "LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)",
+            "parallelism": "1 GPU"}
+
+
+def exact_algorithmic_bytes(iters, checkpoint):
+    """Forward + segment recompute + reverse, counted as 3x the FP64 forward (96 B per point-iteration: six
+    coefficients, r, s, x read and r, s, x written), plus the checkpoint stores (r and s_prev, 16 B per point each
+    checkpoint)."""
+    tot = 0
+    for k in iters:
+        nck = 1 if checkpoint <= 0 else -(-k // checkpoint)
+        tot += N_LLC90 * (3 * 96 * k + 16 * nck)
+    return tot
+
+
+def exact_launches(kmax, checkpoint):
+    """Kernels cg2d_adjoint_exact launches for a batch whose largest iteration count is kmax (memsets and
+    device-to-device copies excluded): setup and init, 8 per recorded iteration, the cotangent scaling, 3 or 4 per
+    recomputed iteration (the last of a segment needs no new residual), 10 per reversed iteration, and the two
+    closing kernels."""
+    C = checkpoint if checkpoint > 0 else max(1, kmax)
+    nseg = -(-kmax // C) if kmax else 0
+    return 2 + 8 * kmax + 1 + (4 * kmax - nseg) + 10 * kmax + 2
+
+
+def _cpu_exact(B, syn, member, iters):
+    """The autograd oracle through the same iterations, one LLC90 instance, timed on host cores."""
+    import torch
+    from oracle.cg2d_exact_oracle import cg2d_exact_grad
+    ops = tuple(B[k][member] for k in ("aW2d", "aS2d", "aC2d", "pW", "pS", "pC"))
+    t0 = time.perf_counter()
+    cg2d_exact_grad(syn.L, syn.topo.maps["T"], ops, B["b"][member], np.zeros_like(B["b"][member]),
+                    B["w"][member], cg2dNorm=B["cg2dNorm"][member], iters=iters)
+    return time.perf_counter() - t0, torch.get_num_threads()
+
+
+def run_exact(a):
+    import torch
+
+    from mit_jax_b200 import capi
+    from mit_jax_b200 import cg2d as cg
+    from mit_jax_b200.synthetic import make_batch
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    syn, B = make_batch(90, a.batch, with_cotangent=True)
+    ex = cg.default_exchanger(syn.L)
+    ops = tuple(torch.as_tensor(B[k]).to(dev) for k in cg.OPS)
+    b = torch.as_tensor(B["b"]).to(dev)
+    mask = cg._interior_mask(syn.L, dev)
+    w = torch.where(mask, torch.as_tensor(B["w"]).to(dev), torch.zeros((), dtype=torch.float64, device=dev))
+    x0 = torch.zeros_like(b)
+    norms = torch.as_tensor(B["cg2dNorm"]).to(dev)
+    kw = dict(tolerance=a.tol, max_iters=a.maxit, checkpoint_every=a.checkpoint)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        return cg.exact_adjoint(ex, ops, b, x0, w, cg2dNorm=norms, **kw)
+
+    for _ in range(max(3, a.warmup)):
+        x, d, g = step()
+    torch.cuda.synchronize(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    resident = torch.cuda.memory_allocated(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(_gpu_uuid(torch, dev)) as clk:
+        time.sleep(0.25)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(a.steps):
+            x, d, g = step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    clocks = clk.summary()
+    ms = e0.elapsed_time(e1) / a.steps
+    peak_alloc = torch.cuda.max_memory_allocated(dev)
+    ws_bytes = capi.lib().cg2d_adjoint_exact_workspace_size(ex.handle(dev), a.batch, a.maxit, a.checkpoint)
+    iters = [r["numIters"] for r in d]
+    bad = [r for r in d if r["status"] != "ok"]
+    alg = exact_algorithmic_bytes(iters, a.checkpoint)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+
+    # the exact derivative of the iteration against the implicit derivative of the converged solution
+    imp = cg.solve_with_adjoint(ex, ops, b, w, x0, cg2dNorm=norms, tolerance=a.tol, max_iters=a.maxit,
+                                precision="f64")
+    from mit_jax_b200.topology import exch_vector_adjoint
+
+    def rel(u, ref):
+        u, ref = np.asarray(u).reshape(a.batch, -1), np.asarray(ref).reshape(a.batch, -1)
+        return float((np.abs(u - ref).max(1) / np.maximum(np.abs(ref).max(1), 1e-300)).max())
+
+    host = {k: v.cpu().numpy() for k, v in (("b", g["b"]), ("aW2d", g["aW2d"]), ("aS2d", g["aS2d"]),
+                                            ("aC2d", g["aC2d"]), ("lam", imp["lam"]), ("gW", imp["gW"]),
+                                            ("gS", imp["gS"]), ("gC", imp["gC"]))}
+    maps_u, maps_v = syn.topo.maps["UVn_u"], syn.topo.maps["UVn_v"]
+    eu, ev = exch_vector_adjoint(host["aW2d"], host["aS2d"], maps_u, maps_v)
+    iu, iv = exch_vector_adjoint(host["gW"], host["gS"], maps_u, maps_v)
+    gap = {"b": rel(host["b"], host["lam"]), "aC2d": rel(host["aC2d"], host["gC"]),
+           "aW2d_per_face": rel(eu, iu), "aS2d_per_face": rel(ev, iv),
+           "aW2d_per_entry": rel(host["aW2d"], host["gW"]), "aS2d_per_entry": rel(host["aS2d"], host["gS"]),
+           "note": "max over members of max|exact - implicit| / max|implicit|; per face = after the transpose of "
+                   "the face exchange (each halo face entry's cotangent added onto the edge entry it copies); per "
+                   "entry, the two stored copies of a tile-edge face are moved apart, an unsymmetric direction"}
+
+    # end to end: inputs from pinned host buffers, solution and gradients back to pinned host buffers
+    e2e = None
+    if not a.no_e2e:
+        host_in = {k: torch.as_tensor(B[k]).pin_memory() for k in (*cg.OPS, "b", "w")}
+        host_norm = torch.as_tensor(B["cg2dNorm"])
+        names = ("x", "b") + cg.OPS
+        outs = {k: torch.empty((a.batch, *syn.L.shape2d), dtype=torch.float64).pin_memory() for k in names}
+        h2d = sum(v.numel() * v.element_size() for v in host_in.values()) + host_norm.numel() * 8
+        d2h = sum(v.numel() * v.element_size() for v in outs.values()) + a.batch * capi.DIAG_BYTES
+
+        def e2e_step():
+            din = {k: v.to(dev, non_blocking=True) for k, v in host_in.items()}
+            xe, de, ge = cg.exact_adjoint(ex, tuple(din[k] for k in cg.OPS), din["b"], torch.zeros_like(din["b"]),
+                                          din["w"], cg2dNorm=host_norm.to(dev, non_blocking=True), **kw)
+            outs["x"].copy_(xe, non_blocking=True)
+            for k in names[1:]:
+                outs[k].copy_(ge[k], non_blocking=True)
+            return de
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(a.steps):
+            e2e_step()
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e = {"value": a.batch * a.steps / (t0.elapsed_time(t1) / 1e3), "unit": "adjoint solves/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if not a.no_cpu:
+        secs, threads = _cpu_exact(B, syn, 0, iters[0])
+        cpu = {"value": 1.0 / secs, "unit": "adjoint solves/s", "cores": threads, "kind": "port",
+               "sample": f"member 0 ({iters[0]} iterations): torch float64 autograd through the oracle's "
+                         f"iterations, {secs:.2f} s"}
+
+    line = {
+        "metric": EXACT_METRIC, "value": a.batch / (ms / 1e3), "unit": "adjoint solves/s", "n_gpus": 1,
+        "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": exact_config(a),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "whole step (forward solve + cg2d_adjoint_exact kernels, host syncs included)",
+                     "kernel_ms": ms, "algorithmic_bytes_per_launch": alg},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": a.steps * (1 + exact_launches(max(iters), a.checkpoint)),
+        "clocks": clocks,
+        "memory": {"peak_allocated_bytes": int(peak_alloc), "resident_inputs_bytes": int(resident),
+                   "workspace_bytes": int(ws_bytes)},
+        "iterations": {"mean": statistics.mean(iters), "min": min(iters), "max": max(iters), "not_ok": len(bad)},
+        "exact_vs_implicit_rel": gap,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     a = parse()
+    if a.mode == "exact":
+        if a.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no exact-mode adjoint: "
+                                  "it differentiates cg2d implicitly (mitgcm_jax/core/cg2d.py:307-348)"}))
+            return 0
+        return run_exact(a)
     if a.impl == "reference":
         return run_reference(a)
     return run_gpu(a)

@@ -196,3 +196,28 @@ def exch_vector(u, v, maps_u, maps_v):
         return out * sign
 
     return apply(maps_u, fu).reshape(u.shape), apply(maps_v, fv).reshape(v.shape)
+
+
+def exch_vector_adjoint(gu, gv, maps_u, maps_v):
+    """The transpose of exch_vector: cotangents of the (u, v) that exch_vector reads, given cotangents (gu, gv) of
+    the pair it returns. An entry that exch_vector copies from another adds its cotangent onto that source and
+    keeps none; an entry it keeps passes its own through.
+
+    Applied to coefficient cotangents of a solve (aW2d, aS2d), which are per array entry, it gives the cotangents
+    of the physical faces: a face on a tile edge is stored twice, as the tile's edge entry and as the
+    neighbour's halo entry filled by this exchange (mitgcm_jax/init.py:345-350), and moving the face moves both.
+    Per entry, the two copies may be moved apart, which makes the operator unsymmetric."""
+    gu = np.asarray(gu, np.float64)
+    gv = np.asarray(gv, np.float64)
+    shape = gu.shape
+    fu, fv = gu.reshape(-1, int(np.prod(shape[-3:]))), gv.reshape(-1, int(np.prod(shape[-3:])))
+    ou, ov = np.zeros_like(fu), np.zeros_like(fv)
+    for (src, comp, sign), g, own in ((maps_u, fu, ou), (maps_v, fv, ov)):
+        src, comp = np.asarray(src).astype(np.int64), np.asarray(comp)
+        sg = g * np.asarray(sign, np.float64)
+        keep = comp == 0
+        own[:, keep] += sg[:, keep]
+        for c, tgt in ((1, ou), (2, ov)):
+            sel = comp == c
+            np.add.at(tgt, (slice(None), src[sel]), sg[:, sel])
+    return ou.reshape(shape), ov.reshape(shape)

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 import torch
 
+from mit_jax_b200.topology import exch_vector_adjoint
 from oracle import cg2d_oracle as O
 from oracle.cg2d_exact_oracle import cg2d_exact_grad
 
@@ -89,7 +90,8 @@ def test_exact_adjoint_checkpoints_and_batch(small):
 
 def test_exact_adjoint_approaches_implicit(small):
     """At tolerance 1e-13 the exact derivative of the iteration and the implicit derivative of the converged
-    solution (cg2d.py:318-348) differ by O(residual): here well below 1e-6 relative in d/db and d/d(aW2d)."""
+    solution (cg2d.py:318-348) differ by O(residual): here well below 1e-6 relative in d/db and, per face (after
+    the transpose of the face exchange), in d/d(aW2d) and d/d(aS2d)."""
     syn, ex = small
     L = syn.L
     ops, norm = syn.operator()
@@ -102,4 +104,45 @@ def test_exact_adjoint_approaches_implicit(small):
     xi, _ = cg.cg2d_solve(p, ex, tuple(opt), bt, torch.as_tensor(x0).cuda())
     (xi * torch.as_tensor(w).cuda()).sum().backward()
     assert _rel(g["b"], bt.grad) < 1e-6
-    assert _rel(g["aW2d"], opt[0].grad) < 1e-6
+    maps_u, maps_v = syn.topo.maps["UVn_u"], syn.topo.maps["UVn_v"]
+    eu, ev = exch_vector_adjoint(_np(g["aW2d"]), _np(g["aS2d"]), maps_u, maps_v)
+    iu, iv = exch_vector_adjoint(_np(opt[0].grad), _np(opt[1].grad), maps_u, maps_v)
+    assert _rel(eu, iu) < 1e-6 and _rel(ev, iv) < 1e-6
+
+
+def test_exact_adjoint_finite_differences(small):
+    """The exact derivative of the iteration map: at a fixed iteration count (tolerance 0, 20 iterations) the
+    solution is a nonlinear function of b and of the coefficients; the directional derivative <g, d> equals the
+    central difference (J(p + h d) - J(p - h d)) / 2h, h = 1e-6 relative, on random directions of b, aW2d and
+    aS2d, to 1e-6 relative."""
+    syn, ex = small
+    L = syn.L
+    inner = O.interior_mask(L)
+    ops, norm = syn.operator()
+    ops = tuple(torch.as_tensor(a).cuda() for a in ops)
+    b, x0 = torch.as_tensor(syn.rhs()).cuda(), torch.as_tensor(syn.first_guess()).cuda()
+    w = torch.as_tensor(np.random.default_rng(6).standard_normal(L.shape2d) * inner).cuda()
+    kw = dict(cg2dNorm=norm, tolerance=0.0, max_iters=20, checkpoint_every=7)
+
+    def J(b_, ops_):
+        x, d, _ = cg.exact_adjoint(ex, ops_, b_, x0, w, **kw)
+        assert d["numIters"] == 20
+        return float((x * w).sum())
+
+    _, _, g = cg.exact_adjoint(ex, ops, b, x0, w, **kw)
+    rng = np.random.default_rng(7)
+    for name in ("b", "aW2d", "aS2d"):
+        base = b if name == "b" else ops[cg.OPS.index(name)]
+        for _ in range(3):
+            dvec = torch.as_tensor(rng.standard_normal(L.shape2d)).cuda() * (base != 0)
+            h = 1e-6 * float(base.abs().max()) / float(dvec.abs().max())
+
+            def moved(sign):
+                p = base + sign * h * dvec
+                if name == "b":
+                    return J(p, ops)
+                return J(b, tuple(p if k == name else o for k, o in zip(cg.OPS, ops)))
+
+            fd = (moved(1.0) - moved(-1.0)) / (2 * h)
+            an = float((g[name] * dvec).sum())
+            assert abs(fd - an) <= 1e-6 * abs(an), (name, fd, an)

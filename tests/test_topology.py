@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from golden_cases import GOLDEN
-from mit_jax_b200.topology import LLCTopology, exch_scalar
+from mit_jax_b200.topology import LLCTopology, exch_scalar, exch_vector, exch_vector_adjoint
 
 
 @pytest.fixture(scope="module")
@@ -86,3 +86,16 @@ def test_exchange_adjoint_identity():
     et = np.where(comp == 1, 0.0, yf)
     np.add.at(et, src[comp == 1], yf[comp == 1])
     np.testing.assert_allclose(np.vdot(ex, y), np.vdot(x.reshape(-1), et), rtol=1e-13)
+
+
+def test_face_exchange_adjoint_identity():
+    """<E (u, v), (a, b)> == <(u, v), E^T (a, b)> for the UVn face exchange and its transpose, batched."""
+    tp = LLCTopology(16, 8, 2)
+    rng = np.random.default_rng(1)
+    u, v, a, b = (rng.standard_normal((2,) + tp.L.shape2d) for _ in range(4))
+    eu, ev = exch_vector(u, v, tp.maps["UVn_u"], tp.maps["UVn_v"])
+    ta, tb = exch_vector_adjoint(a, b, tp.maps["UVn_u"], tp.maps["UVn_v"])
+    for m in range(2):
+        lhs = np.vdot(eu[m], a[m]) + np.vdot(ev[m], b[m])
+        rhs = np.vdot(u[m], ta[m]) + np.vdot(v[m], tb[m])
+        np.testing.assert_allclose(lhs, rhs, rtol=1e-13)
