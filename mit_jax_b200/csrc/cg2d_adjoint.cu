@@ -91,57 +91,44 @@ struct Geo {
   long long pe;   // padded elements per instance
   long long pts;  // interior points per instance
 };
-__device__ __forceinline__ bool decode(const Geo& G, long long idx, int& in, int& t, int& j, int& i, long long& p) {
-  in = (int)(idx / G.pts);
-  const long long r = idx - (long long)in * G.pts;
-  const int per = G.tp.nj * G.tp.ni;
-  t = (int)(r / per);
-  const int r2 = (int)(r - (long long)t * per);
-  j = r2 / G.tp.ni;
-  i = r2 - j * G.tp.ni;
-  p = (long long)in * G.pe + padded(G.tp, t, j, i);
-  return in < G.batch;
-}
-#define FOR_POINTS(G)                                                                                      \
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (long long)(G).batch * (G).pts; \
-       idx += (long long)gridDim.x * blockDim.x)
+// Point kernels run one thread per interior point: threadIdx.x = i, one tile row per threadIdx.y,
+// blockIdx.x = group of rows (row = t nj + j), blockIdx.y = instance. Face kernels use the same shape over
+// i = 0..ni and rows j = 0..nj of each tile.
+#define POINT(G, in, t, j, i, p)                                                         \
+  const int i = threadIdx.x, in = blockIdx.y;                                            \
+  const int row_ = blockIdx.x * blockDim.y + threadIdx.y;                                \
+  if (i >= (G).tp.ni || row_ >= (G).tp.T * (G).tp.nj) return;                            \
+  const int t = row_ / (G).tp.nj, j = row_ - t * (G).tp.nj;                              \
+  const long long p = (long long)in * (G).pe + padded((G).tp, t, j, i)
 __device__ __forceinline__ bool live(const int* K, int in, int k) { return k < K[in]; }
 
 // r = b_n - A x0_n and x = x0_n on the interior, b_n = b cg2dNorm rhsNorm (cg2d.py:221-232)
 __global__ void k_init(Geo G, const double* aW, const double* aS, const double* aC, const double* b, const double* x0,
                        const double* norm, const double* rn, double* r, double* x) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    const TopoDev& tp = G.tp;
-    const double* x0i = x0 + (long long)in * G.pe;
-    const double rni = rn[in];
-    const double vc = nbx0(tp, x0i, rni, t, j, i);
-    const double ax = opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], nbx0(tp, x0i, rni, t, j, i - 1),
-                          nbx0(tp, x0i, rni, t, j, i + 1), nbx0(tp, x0i, rni, t, j - 1, i),
-                          nbx0(tp, x0i, rni, t, j + 1, i), vc);
-    r[p] = sub(mul(mul(b[p], norm[in]), rni), ax);
-    x[p] = vc;
-  }
+  POINT(G, in, t, j, i, p);
+  const TopoDev& tp = G.tp;
+  const double* x0i = x0 + (long long)in * G.pe;
+  const double rni = rn[in];
+  const double vc = nbx0(tp, x0i, rni, t, j, i);
+  const double ax = opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], nbx0(tp, x0i, rni, t, j, i - 1),
+                        nbx0(tp, x0i, rni, t, j, i + 1), nbx0(tp, x0i, rni, t, j - 1, i),
+                        nbx0(tp, x0i, rni, t, j + 1, i), vc);
+  r[p] = sub(mul(mul(b[p], norm[in]), rni), ax);
+  x[p] = vc;
 }
 
 // out = [base +] A v (mode 0) or M v (mode 1) on the interior of live instances
 __global__ void k_stencil(Geo G, int mode, const double* c0, const double* c1, const double* c2, const double* v,
                           const double* base, double* out, const int* K, int k) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    if (!live(K, in, k)) continue;
-    const TopoDev& tp = G.tp;
-    const double* vi = v + (long long)in * G.pe;
-    const double vw = nbv(tp, vi, t, j, i - 1), ve = nbv(tp, vi, t, j, i + 1);
-    const double vs = nbv(tp, vi, t, j - 1, i), vn = nbv(tp, vi, t, j + 1, i), vc = v[p];
-    const double o = mode == 0 ? opA(c0[p], c0[p + 1], c1[p], c1[p + tp.npx], c2[p], vw, ve, vs, vn, vc)
-                               : opM(c2[p], c0[p], c0[p + 1], c1[p], c1[p + tp.npx], vc, vw, ve, vs, vn);
-    out[p] = base ? add(base[p], o) : o;
-  }
+  POINT(G, in, t, j, i, p);
+  if (!live(K, in, k)) return;
+  const TopoDev& tp = G.tp;
+  const double* vi = v + (long long)in * G.pe;
+  const double vw = nbv(tp, vi, t, j, i - 1), ve = nbv(tp, vi, t, j, i + 1);
+  const double vs = nbv(tp, vi, t, j - 1, i), vn = nbv(tp, vi, t, j + 1, i), vc = v[p];
+  const double o = mode == 0 ? opA(c0[p], c0[p + 1], c1[p], c1[p + tp.npx], c2[p], vw, ve, vs, vn, vc)
+                             : opM(c2[p], c0[p], c0[p + 1], c1[p], c1[p + tp.npx], vc, vw, ve, vs, vn);
+  out[p] = base ? add(base[p], o) : o;
 }
 
 // row sums of up to two products a0 b0, a1 b1 of live instances: rs[(in 2 + q)][t nj + j], one warp per row,
@@ -150,83 +137,105 @@ __global__ void k_rowdot(Geo G, const double* a0, const double* b0, const double
                          const int* K, int k) {
   const int lane = threadIdx.x & 31;
   const int rows = G.tp.T * G.tp.nj;
-  const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long w = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < (long long)G.batch * rows;
-       w += nwarps) {
-    const int in = (int)(w / rows), row = (int)(w - (long long)in * rows);
-    if (!live(K, in, k)) continue;
-    const int t = row / G.tp.nj, j = row - t * G.tp.nj;
-    const long long p0 = (long long)in * G.pe + padded(G.tp, t, j, 0);
-    double s0 = 0.0, s1 = 0.0;
-    for (int i = lane; i < G.tp.ni; i += 32) {
-      s0 = add(s0, mul(a0[p0 + i], b0[p0 + i]));
-      if (a1) s1 = add(s1, mul(a1[p0 + i], b1[p0 + i]));
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      s0 = add(s0, __shfl_xor_sync(0xffffffffu, s0, o));
-      s1 = add(s1, __shfl_xor_sync(0xffffffffu, s1, o));
-    }
-    if (lane == 0) {
-      rs[((long long)in * 2 + 0) * rows + row] = s0;
-      if (a1) rs[((long long)in * 2 + 1) * rows + row] = s1;
-    }
+  const int in = blockIdx.y;
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= rows || !live(K, in, k)) return;
+  const int t = row / G.tp.nj, j = row - t * G.tp.nj;
+  const long long p0 = (long long)in * G.pe + padded(G.tp, t, j, 0);
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = lane; i < G.tp.ni; i += 32) {
+    s0 = add(s0, mul(a0[p0 + i], b0[p0 + i]));
+    if (a1) s1 = add(s1, mul(a1[p0 + i], b1[p0 + i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 = add(s0, __shfl_xor_sync(0xffffffffu, s0, o));
+    s1 = add(s1, __shfl_xor_sync(0xffffffffu, s1, o));
+  }
+  if (lane == 0) {
+    rs[((long long)in * 2 + 0) * rows + row] = s0;
+    if (a1) rs[((long long)in * 2 + 1) * rows + row] = s1;
   }
 }
 
-// the sums in ROWBLOCK order (rows of a block in order, blocks of a tile in order, tiles in order from 0)
-__device__ double fold(const Geo& G, int R, const double* rs) {
-  double total = 0.0;
-  for (int t = 0; t < G.tp.T; ++t) {
-    double ts = 0.0;
-    for (int j0 = 0; j0 < G.tp.nj; j0 += R) {
-      double u = 0.0;
-      for (int j = j0; j < min(G.tp.nj, j0 + R); ++j) u = add(u, rs[t * G.tp.nj + j]);
-      ts = add(ts, u);
-    }
-    total = add(total, ts);
+// The sum of an instance's row sums in ROWBLOCK order (rows of a block of R in order, blocks of a tile in order,
+// tiles in order from 0), by the whole thread block: the block sums in parallel, then the tile sums, then the
+// total -- the same additions in the same order as one thread summing row by row. sh holds T (ceil(nj / R) + 1)
+// doubles. The result is valid in thread 0.
+__device__ double fold(const Geo& G, int R, const double* rs, double* sh) {
+  const int T = G.tp.T, nj = G.tp.nj, nb = (nj + R - 1) / R;
+  for (int u = threadIdx.x; u < T * nb; u += blockDim.x) {
+    const int t = u / nb, j0 = (u - t * nb) * R, j1 = min(nj, j0 + R);
+    double v = 0.0;
+    for (int j = j0; j < j1; ++j) v = add(v, rs[t * nj + j]);
+    sh[u] = v;
   }
+  __syncthreads();
+  for (int t = threadIdx.x; t < T; t += blockDim.x) {
+    double ts = 0.0;
+    for (int b = 0; b < nb; ++b) ts = add(ts, sh[t * nb + b]);
+    sh[T * nb + t] = ts;
+  }
+  __syncthreads();
+  double total = 0.0;
+  if (threadIdx.x == 0)
+    for (int t = 0; t < T; ++t) total = add(total, sh[T * nb + t]);
+  __syncthreads();   // sh may be reused by a second fold
   return total;
 }
 
-// per-instance scalar steps, one thread per live instance; S = scalar arrays [kind][Kmax][batch]
+// per-instance scalar steps, one thread block per instance (blockIdx.x), thread 0 updating the scalars;
+// S = scalar arrays [kind][Kmax][batch]
 struct Scal {
   double *eta, *beta, *sig, *alpha;   // [Kmax][batch] (recorded)
   double *carry, *etabar, *sigbar;    // [batch] (reverse)
 };
 __global__ void k_fwd_eta(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
-  const int in = blockIdx.x * blockDim.x + threadIdx.x;
-  if (in >= G.batch || !live(K, in, k)) return;
+  extern __shared__ double sh[];
+  const int in = blockIdx.x;
+  if (!live(K, in, k)) return;
   const int rows = G.tp.T * G.tp.nj;
-  const double eta = fold(G, R, rs + (long long)in * 2 * rows);                  // cg2d.py:246
+  const double eta = fold(G, R, rs + (long long)in * 2 * rows, sh);              // cg2d.py:246
+  if (threadIdx.x != 0) return;
   const double eta_prev = k > 0 ? S.eta[(long long)(k - 1) * G.batch + in] : 1.0;
   S.eta[(long long)k * G.batch + in] = eta;
   S.beta[(long long)k * G.batch + in] = __ddiv_rn(eta, eta_prev);             // cg2d.py:247
 }
 __global__ void k_fwd_sigma(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
-  const int in = blockIdx.x * blockDim.x + threadIdx.x;
-  if (in >= G.batch || !live(K, in, k)) return;
+  extern __shared__ double sh[];
+  const int in = blockIdx.x;
+  if (!live(K, in, k)) return;
   const int rows = G.tp.T * G.tp.nj;
-  const double sig = fold(G, R, rs + (long long)in * 2 * rows);                  // cg2d.py:252
+  const double sig = fold(G, R, rs + (long long)in * 2 * rows, sh);              // cg2d.py:252
+  if (threadIdx.x != 0) return;
   S.sig[(long long)k * G.batch + in] = sig;
   S.alpha[(long long)k * G.batch + in] = __ddiv_rn(S.eta[(long long)k * G.batch + in], sig);   // cg2d.py:253
 }
 // reverse: abar = <xbar, s> - <rbar, q>
 __global__ void k_rev_alpha(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
-  const int in = blockIdx.x * blockDim.x + threadIdx.x;
-  if (in >= G.batch || !live(K, in, k)) return;
+  extern __shared__ double sh[];
+  const int in = blockIdx.x;
+  if (!live(K, in, k)) return;
   const int rows = G.tp.T * G.tp.nj;
-  const double abar = fold(G, R, rs + (long long)in * 2 * rows) - fold(G, R, rs + ((long long)in * 2 + 1) * rows);
+  const double f0 = fold(G, R, rs + (long long)in * 2 * rows, sh);
+  const double f1 = fold(G, R, rs + ((long long)in * 2 + 1) * rows, sh);
+  if (threadIdx.x != 0) return;
+  const double abar = f0 - f1;
   const long long o = (long long)k * G.batch + in;
   S.sigbar[in] = -abar * S.alpha[o] / S.sig[o];
   S.etabar[in] = S.carry[in] + abar / S.sig[o];
 }
 // reverse: bbar = <sbar, s_prev>
 __global__ void k_rev_beta(Geo G, int R, const double* rs, Scal S, const int* K, int k) {
-  const int in = blockIdx.x * blockDim.x + threadIdx.x;
-  if (in >= G.batch || !live(K, in, k)) return;
-  if (k == 0) { S.carry[in] = 0.0; return; }   // eta_{-1} = 1 is a constant, s_{-1} = 0
+  extern __shared__ double sh[];
+  const int in = blockIdx.x;
+  if (!live(K, in, k)) return;
+  if (k == 0) {   // eta_{-1} = 1 is a constant, s_{-1} = 0
+    if (threadIdx.x == 0) S.carry[in] = 0.0;
+    return;
+  }
   const int rows = G.tp.T * G.tp.nj;
-  const double bbar = fold(G, R, rs + (long long)in * 2 * rows);
+  const double bbar = fold(G, R, rs + (long long)in * 2 * rows, sh);
+  if (threadIdx.x != 0) return;
   const double eta = S.eta[(long long)k * G.batch + in], etap = S.eta[(long long)(k - 1) * G.batch + in];
   S.etabar[in] += bbar / etap;
   S.carry[in] = -bbar * eta / (etap * etap);
@@ -234,110 +243,82 @@ __global__ void k_rev_beta(Geo G, int R, const double* rs, Scal S, const int* K,
 
 // forward updates of live instances
 __global__ void k_fwd_s(Geo G, const double* z, const double* sprev, double* s, Scal S, const int* K, int k) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    if (!live(K, in, k)) continue;
-    s[p] = add(z[p], mul(S.beta[(long long)k * G.batch + in], sprev[p]));        // cg2d.py:249
-  }
+  POINT(G, in, t, j, i, p);
+  if (!live(K, in, k)) return;
+  s[p] = add(z[p], mul(S.beta[(long long)k * G.batch + in], sprev[p]));          // cg2d.py:249
 }
 __global__ void k_fwd_rx(Geo G, const double* s, const double* q, const double* r, double* rout, double* x, Scal S,
                          const int* K, int k) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    if (!live(K, in, k)) continue;
-    const double a = S.alpha[(long long)k * G.batch + in];
-    if (x) x[p] = add(x[p], mul(a, s[p]));                                      // cg2d.py:254
-    rout[p] = sub(r[p], mul(a, q[p]));                                          // cg2d.py:255
-  }
+  POINT(G, in, t, j, i, p);
+  if (!live(K, in, k)) return;
+  const double a = S.alpha[(long long)k * G.batch + in];
+  if (x) x[p] = add(x[p], mul(a, s[p]));                                        // cg2d.py:254
+  rout[p] = sub(r[p], mul(a, q[p]));                                            // cg2d.py:255
 }
 // reverse: qbar = sigbar s - alpha rbar;  sbar += alpha xbar + sigbar q
 __global__ void k_rev_q(Geo G, const double* s, const double* q, const double* xbar, const double* rbar, double* qbar,
                         double* sbar, Scal S, const int* K, int k) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    if (!live(K, in, k)) continue;
-    const double a = S.alpha[(long long)k * G.batch + in], sg = S.sigbar[in];
-    qbar[p] = sg * s[p] - a * rbar[p];
-    sbar[p] = sbar[p] + a * xbar[p] + sg * q[p];
-  }
+  POINT(G, in, t, j, i, p);
+  if (!live(K, in, k)) return;
+  const double a = S.alpha[(long long)k * G.batch + in], sg = S.sigbar[in];
+  qbar[p] = sg * s[p] - a * rbar[p];
+  sbar[p] = sbar[p] + a * xbar[p] + sg * q[p];
 }
 // reverse: zbar = sbar + etabar r;  rbar += etabar z;  sbar = beta sbar
 __global__ void k_rev_z(Geo G, const double* r, const double* z, double* zbar, double* rbar, double* sbar, Scal S,
                         const int* K, int k) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    if (!live(K, in, k)) continue;
-    const double e = S.etabar[in];
-    zbar[p] = sbar[p] + e * r[p];
-    rbar[p] = rbar[p] + e * z[p];
-    sbar[p] = S.beta[(long long)k * G.batch + in] * sbar[p];
-  }
+  POINT(G, in, t, j, i, p);
+  if (!live(K, in, k)) return;
+  const double e = S.etabar[in];
+  zbar[p] = sbar[p] + e * r[p];
+  rbar[p] = rbar[p] + e * z[p];
+  sbar[p] = S.beta[(long long)k * G.batch + in] * sbar[p];
 }
 
 // coefficient cotangents of a stencil application out = C v: gW/gS/gC += sign (u (x) v) on the faces and points
 // of live instances, u the cotangent of out (interior), v the stencil input as the stencil read it (X0: the
-// first-guess rule); the same faces as edge_products_kernel
+// first-guess rule); the same faces as edge_products_kernel. One thread per (j, i), 0 <= j <= nj, 0 <= i <= ni.
 template <bool X0>
 __global__ void k_edges(Geo G, const double* u, const double* v, const double* rn, double sign, double* gW,
                         double* gS, double* gC, const int* K, int k) {
   const TopoDev& tp = G.tp;
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (long long)G.batch * G.pe;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const int in = (int)(idx / G.pe);
-    if (K && !live(K, in, k)) continue;
-    const long long pp = idx - (long long)in * G.pe;
-    const int plane = tp.npy * tp.npx;
-    const int t = (int)(pp / plane);
-    const int rem = (int)(pp - (long long)t * plane);
-    const int j = rem / tp.npx - tp.OLy, i = rem - (rem / tp.npx) * tp.npx - tp.OLx;
-    const double* ui = u + (long long)in * G.pe;
-    const double* vi = v + (long long)in * G.pe;
-    auto V = [&](int jj, int ii) -> double {
-      return X0 ? nbx0(tp, vi, rn[in], t, jj, ii) : nbv(tp, vi, t, jj, ii);
-    };
-    auto U = [&](int jj, int ii) -> double { return ui[padded(tp, t, jj, ii)]; };
-    const bool jin = j >= 0 && j < tp.nj, iin = i >= 0 && i < tp.ni;
-    if (jin && i >= 0 && i <= tp.ni) {   // face between (j, i-1) and (j, i)
-      double a = 0.0;
-      if (i < tp.ni) a += U(j, i) * V(j, i - 1);
-      if (i >= 1) a += U(j, i - 1) * V(j, i);
-      gW[idx] += sign * a;
-    }
-    if (iin && j >= 0 && j <= tp.nj) {   // face between (j-1, i) and (j, i)
-      double a = 0.0;
-      if (j < tp.nj) a += U(j, i) * V(j - 1, i);
-      if (j >= 1) a += U(j - 1, i) * V(j, i);
-      gS[idx] += sign * a;
-    }
-    if (jin && iin) gC[idx] += sign * U(j, i) * V(j, i);
+  const int i = threadIdx.x, in = blockIdx.y;
+  const int row = blockIdx.x * blockDim.y + threadIdx.y;
+  if (i > tp.ni || row >= tp.T * (tp.nj + 1)) return;
+  if (K && !live(K, in, k)) return;
+  const int t = row / (tp.nj + 1), j = row - t * (tp.nj + 1);
+  const long long idx = (long long)in * G.pe + padded(tp, t, j, i);
+  const double* ui = u + (long long)in * G.pe;
+  const double* vi = v + (long long)in * G.pe;
+  auto V = [&](int jj, int ii) -> double {
+    return X0 ? nbx0(tp, vi, rn[in], t, jj, ii) : nbv(tp, vi, t, jj, ii);
+  };
+  auto U = [&](int jj, int ii) -> double { return ui[padded(tp, t, jj, ii)]; };
+  const bool jin = j < tp.nj, iin = i < tp.ni;
+  if (jin) {   // face between (j, i-1) and (j, i)
+    double a = 0.0;
+    if (i < tp.ni) a += U(j, i) * V(j, i - 1);
+    if (i >= 1) a += U(j, i - 1) * V(j, i);
+    gW[idx] += sign * a;
   }
+  if (iin) {   // face between (j-1, i) and (j, i)
+    double a = 0.0;
+    if (j < tp.nj) a += U(j, i) * V(j - 1, i);
+    if (j >= 1) a += U(j - 1, i) * V(j, i);
+    gS[idx] += sign * a;
+  }
+  if (jin && iin) gC[idx] += sign * U(j, i) * V(j, i);
 }
 
 // xbar_K = xbar_out / rhsNorm on the interior;  bbar = rbar_0 cg2dNorm rhsNorm on the interior
 __global__ void k_scale(Geo G, const double* in_, const double* norm, const double* rn, double* out, int mode) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    out[p] = mode == 0 ? in_[p] / rn[in] : in_[p] * norm[in] * rn[in];
-  }
+  POINT(G, in, t, j, i, p);
+  out[p] = mode == 0 ? in_[p] / rn[in] : in_[p] * norm[in] * rn[in];
 }
 // x_out of the recording forward: x / rhsNorm on the interior (cg2d.py:266)
 __global__ void k_xout(Geo G, const double* x, const double* rn, double* out) {
-  FOR_POINTS(G) {
-    int in, t, j, i;
-    long long p;
-    decode(G, idx, in, t, j, i, p);
-    out[p] = __ddiv_rn(x[p], rn[in]);
-  }
+  POINT(G, in, t, j, i, p);
+  out[p] = __ddiv_rn(x[p], rn[in]);
 }
 // per-instance rhsNorm from the forward's rhsMax (cg2d.py:225) and cg2dNorm, iteration counts
 __global__ void k_setup(int batch, const cg2d_diag_t* diag, double norm, const double* norm_arr, double* rn,
@@ -350,10 +331,6 @@ __global__ void k_setup(int batch, const cg2d_diag_t* diag, double norm, const d
   K[in] = diag[in].numIters;
 }
 
-int grid_for(long long n) {
-  long long b = (n + 255) / 256;
-  return (int)std::max(1ll, std::min(b, 148ll * 16));
-}
 
 }  // namespace
 
@@ -408,8 +385,16 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   double* nrm = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
   int* K = reinterpret_cast<int*>(take(sizeof(int) * A.batch));
 
-  const int gp = grid_for((long long)A.batch * G.pts), ge = grid_for((long long)A.batch * G.pe);
-  const int gw = grid_for((long long)A.batch * rows * 32), gi = (A.batch + 127) / 128;
+  // point kernels: a row of ni threads (rounded up to whole warps) per threadIdx.y; face kernels the same over
+  // ni + 1 faces and nj + 1 face rows; row sums one warp per row; scalar steps one block per instance
+  const int bxp = 32 * ((tp.ni + 31) / 32), bxe = 32 * ((tp.ni + 1 + 31) / 32);
+  if (bxe > 1024 || A.batch > 65535) return cudaErrorInvalidValue;
+  const dim3 bp(bxp, std::max(1, 384 / bxp)), be(bxe, std::max(1, 384 / bxe));
+  const dim3 gp((rows + bp.y - 1) / bp.y, A.batch), ge((tp.T * (tp.nj + 1) + be.y - 1) / be.y, A.batch);
+  const dim3 gw((rows + 7) / 8, A.batch);
+  const int gi = (A.batch + 127) / 128, nbk = (tp.nj + A.rows_per_block - 1) / A.rows_per_block;
+  const size_t fold_sh = sizeof(double) * (size_t)tp.T * (nbk + 1);
+  if (fold_sh > 48 * 1024) return cudaErrorInvalidValue;
   const size_t vb = vecn * sizeof(double);
   cudaError_t e;
 #define CK(x)                              \
@@ -426,7 +411,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   CK(cudaMemsetAsync(S.carry, 0, sizeof(double) * A.batch, st));
   k_setup<<<gi, 128, 0, st>>>(A.batch, A.fwd_diag, A.norm, A.norm_arr, rn, nrm, K);
   LK();
-  k_init<<<gp, 256, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
+  k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
   LK();
 
   // ---- recording forward: scalars of every iteration, checkpoints of r and s_prev
@@ -437,31 +422,31 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
       CK(cudaMemcpyAsync(ck_r[k / C], r, vb, cudaMemcpyDeviceToDevice, st));
       CK(cudaMemcpyAsync(ck_s[k / C], sprev, vb, cudaMemcpyDeviceToDevice, st));
     }
-    k_stencil<<<gp, 256, 0, st>>>(G, 1, A.pW, A.pS, A.pC, r, nullptr, z, K, k);
+    k_stencil<<<gp, bp, 0, st>>>(G, 1, A.pW, A.pS, A.pC, r, nullptr, z, K, k);
     LK();
     k_rowdot<<<gw, 256, 0, st>>>(G, z, r, nullptr, nullptr, rs, K, k);
     LK();
-    k_fwd_eta<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+    k_fwd_eta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
     LK();
-    k_fwd_s<<<gp, 256, 0, st>>>(G, z, sprev, snew, S, K, k);
+    k_fwd_s<<<gp, bp, 0, st>>>(G, z, sprev, snew, S, K, k);
     LK();
-    k_stencil<<<gp, 256, 0, st>>>(G, 0, A.aW, A.aS, A.aC, snew, nullptr, q, K, k);
+    k_stencil<<<gp, bp, 0, st>>>(G, 0, A.aW, A.aS, A.aC, snew, nullptr, q, K, k);
     LK();
     k_rowdot<<<gw, 256, 0, st>>>(G, snew, q, nullptr, nullptr, rs, K, k);
     LK();
-    k_fwd_sigma<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+    k_fwd_sigma<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
     LK();
-    k_fwd_rx<<<gp, 256, 0, st>>>(G, snew, q, r, r, x, S, K, k);
+    k_fwd_rx<<<gp, bp, 0, st>>>(G, snew, q, r, r, x, S, K, k);
     LK();
     std::swap(sprev, snew);
   }
   if (A.x_check) {
-    k_xout<<<gp, 256, 0, st>>>(G, x, rn, A.x_check);
+    k_xout<<<gp, bp, 0, st>>>(G, x, rn, A.x_check);
     LK();
   }
 
   // ---- reverse sweep, segment by segment from the last
-  k_scale<<<gp, 256, 0, st>>>(G, A.xbar, nrm, rn, xbar, 0);
+  k_scale<<<gp, bp, 0, st>>>(G, A.xbar, nrm, rn, xbar, 0);
   LK();
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int c0 = seg * C, c1 = std::min(Kmax, c0 + C);
@@ -470,14 +455,14 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
     for (int k = c0; k < c1; ++k) {
       const int m = k - c0;
       const double* sp = m == 0 ? ck_s[seg] : sg_s[m - 1];
-      k_stencil<<<gp, 256, 0, st>>>(G, 1, A.pW, A.pS, A.pC, sg_r[m], nullptr, sg_z[m], K, k);
+      k_stencil<<<gp, bp, 0, st>>>(G, 1, A.pW, A.pS, A.pC, sg_r[m], nullptr, sg_z[m], K, k);
       LK();
-      k_fwd_s<<<gp, 256, 0, st>>>(G, sg_z[m], sp, sg_s[m], S, K, k);
+      k_fwd_s<<<gp, bp, 0, st>>>(G, sg_z[m], sp, sg_s[m], S, K, k);
       LK();
-      k_stencil<<<gp, 256, 0, st>>>(G, 0, A.aW, A.aS, A.aC, sg_s[m], nullptr, sg_q[m], K, k);
+      k_stencil<<<gp, bp, 0, st>>>(G, 0, A.aW, A.aS, A.aC, sg_s[m], nullptr, sg_q[m], K, k);
       LK();
       if (m + 1 < c1 - c0) {
-        k_fwd_rx<<<gp, 256, 0, st>>>(G, sg_s[m], sg_q[m], sg_r[m], sg_r[m + 1], nullptr, S, K, k);
+        k_fwd_rx<<<gp, bp, 0, st>>>(G, sg_s[m], sg_q[m], sg_r[m], sg_r[m + 1], nullptr, S, K, k);
         LK();
       }
     }
@@ -486,30 +471,30 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
       const double* sp = m == 0 ? ck_s[seg] : sg_s[m - 1];
       k_rowdot<<<gw, 256, 0, st>>>(G, xbar, sg_s[m], rbar, sg_q[m], rs, K, k);
       LK();
-      k_rev_alpha<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+      k_rev_alpha<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rev_q<<<gp, 256, 0, st>>>(G, sg_s[m], sg_q[m], xbar, rbar, qbar, sbar, S, K, k);
+      k_rev_q<<<gp, bp, 0, st>>>(G, sg_s[m], sg_q[m], xbar, rbar, qbar, sbar, S, K, k);
       LK();
-      k_stencil<<<gp, 256, 0, st>>>(G, 0, A.aW, A.aS, A.aC, qbar, sbar, sbar, K, k);
+      k_stencil<<<gp, bp, 0, st>>>(G, 0, A.aW, A.aS, A.aC, qbar, sbar, sbar, K, k);
       LK();
-      k_edges<false><<<ge, 256, 0, st>>>(G, qbar, sg_s[m], rn, 1.0, A.gW, A.gS, A.gC, K, k);
+      k_edges<false><<<ge, be, 0, st>>>(G, qbar, sg_s[m], rn, 1.0, A.gW, A.gS, A.gC, K, k);
       LK();
       k_rowdot<<<gw, 256, 0, st>>>(G, sbar, sp, nullptr, nullptr, rs, K, k);
       LK();
-      k_rev_beta<<<gi, 128, 0, st>>>(G, A.rows_per_block, rs, S, K, k);
+      k_rev_beta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rev_z<<<gp, 256, 0, st>>>(G, sg_r[m], sg_z[m], zbar, rbar, sbar, S, K, k);
+      k_rev_z<<<gp, bp, 0, st>>>(G, sg_r[m], sg_z[m], zbar, rbar, sbar, S, K, k);
       LK();
-      k_stencil<<<gp, 256, 0, st>>>(G, 1, A.pW, A.pS, A.pC, zbar, rbar, rbar, K, k);
+      k_stencil<<<gp, bp, 0, st>>>(G, 1, A.pW, A.pS, A.pC, zbar, rbar, rbar, K, k);
       LK();
-      k_edges<false><<<ge, 256, 0, st>>>(G, zbar, sg_r[m], rn, 1.0, A.gpW, A.gpS, A.gpC, K, k);
+      k_edges<false><<<ge, be, 0, st>>>(G, zbar, sg_r[m], rn, 1.0, A.gpW, A.gpS, A.gpC, K, k);
       LK();
     }
   }
   // r_0 = b_n - A x0_n: the cotangents of b and, through x0_n, of A
-  k_scale<<<gp, 256, 0, st>>>(G, rbar, nrm, rn, A.b_bar, 1);
+  k_scale<<<gp, bp, 0, st>>>(G, rbar, nrm, rn, A.b_bar, 1);
   LK();
-  k_edges<true><<<ge, 256, 0, st>>>(G, rbar, A.x0, rn, -1.0, A.gW, A.gS, A.gC, nullptr, 0);
+  k_edges<true><<<ge, be, 0, st>>>(G, rbar, A.x0, rn, -1.0, A.gW, A.gS, A.gC, nullptr, 0);
   LK();
 #undef CK
 #undef LK
