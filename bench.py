@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch schedule instead of the autotuner's")
+    ap.add_argument("--no-graph", action="store_true", help="eager launches instead of CUDA graph replay")
     a = ap.parse_args()
     if a.batch is None:
         a.batch = 16 if a.mode == "exact" else 64
@@ -268,9 +270,22 @@ def run_gpu(a):
     G = cg.GroupSpec(ex, ops, [b, w], [x0, torch.zeros_like(w)], [a.tol, a.tol], [a.maxit, a.maxit], norms)
     stream = torch.cuda.current_stream(dev)
 
-    def step():
-        (slots,) = cg.solve_groups([G], precision=a.precision, check_status=False)
-        return slots
+    # launch schedule from the autotuner (timed on this workload before the timed region), then the solve
+    # captured once in a CUDA graph and replayed every step
+    from mit_jax_b200 import autotune
+    from mit_jax_b200.graph import GraphedSolve
+    tune_report = []
+    sched = None if a.no_tune else autotune.tune([G], precision=a.precision, report=tune_report)
+    if a.no_graph:
+        def step():
+            (slots,) = cg.solve_groups([G], precision=a.precision, check_status=False, schedule=sched)
+            return slots
+    else:
+        graphed = GraphedSolve([G], precision=a.precision, schedule=sched)
+
+        def step():
+            (slots,), _ = graphed.replay()
+            return slots
 
     def barrier():
         torch.cuda.synchronize(dev)
@@ -406,6 +421,8 @@ def run_gpu(a):
                            "replacements_mean": statistics.mean(d["replacements"] for d in diag_f + diag_a),
                            "not_ok": len(bad)},
             "edge_products_ms": statistics.mean(edge_ms),
+            "schedule": {"chosen": sched or "library default", "launch": "eager" if a.no_graph else "CUDA graph replay",
+                         "candidates_ms": [[c, ms] for c, ms in tune_report]},
             "plain_f64_one_solve_per_launch": plain,
             "speedup_vs_plain_f64": (value / world) / plain["solves_per_s"] if plain else None,
         }

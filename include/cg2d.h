@@ -73,6 +73,10 @@ typedef struct {
                                 arrivals more than there are CTAs, so it runs out after timeout_s and
                                 every solve reports CG2D_BARRIER_TIMEOUT (exercises the bounded wait) */
   int profile;         /* 1: record per-CTA phase times in the workspace (cg2d_workspace_profile) */
+  int unit_deal;       /* how the work units (instance, tile, row block) are dealt to the CTAs:
+                          0 = round-robin (default), 1 = contiguous runs. Like grid_ctas and ctas_per_sm it moves
+                          work between CTAs only: every sum is formed in the same fixed order, so results are the
+                          same bit for bit whatever the schedule (the autotuner's search space) */
 } cg2d_params_t;
 
 /* Per-solve diagnostics: the diag dict of cg2d_fortran (cg2d.py:267-268) plus a status. */

@@ -69,6 +69,7 @@ cg2d_status_t check_params(const cg2d_params_t* p) {
   if (p->grid_ctas < 0 || p->ctas_per_sm < 0) return CG2D_BAD_ARG;
   if (!(p->timeout_s > 0.0) || p->timeout_s > 3600.0) return CG2D_BAD_ARG;
   if (p->test_missing_arrivals < 0 || p->test_missing_arrivals > 1024) return CG2D_BAD_ARG;
+  if (p->unit_deal != 0 && p->unit_deal != 1) return CG2D_BAD_ARG;
   return CG2D_OK;
 }
 
@@ -185,6 +186,7 @@ void cg2d_default_params(cg2d_params_t* p) {
   p->timeout_s = 10.0;
   p->test_missing_arrivals = 0;
   p->profile = 0;
+  p->unit_deal = 0;
 }
 
 const char* cg2d_status_string(cg2d_status_t s) {
@@ -361,6 +363,7 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   kp.gs = reinterpret_cast<unsigned*>(ws + L.gs);
   kp.timeout_ns = (unsigned long long)(params->timeout_s * 1e9);
   kp.test_missing = params->test_missing_arrivals;
+  kp.unit_deal = params->unit_deal;
   kp.prof = params->profile ? reinterpret_cast<unsigned long long*>(ws + L.prof) : nullptr;
   for (int g = 0; g < ngroups; ++g) {
     const cg2d_topology* tp = groups[g].topo;

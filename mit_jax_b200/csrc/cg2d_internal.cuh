@@ -145,6 +145,7 @@ struct KParams {
   // [0] grid-wide wait arrivals, [1] error word, [2] where a time limit ran out, [3] pass << 16 | CTA
   unsigned* gs;
   unsigned long long timeout_ns;
+  int unit_deal;            // 0: units dealt round-robin to the CTAs; 1: contiguous runs (cg2d_params_t)
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
   unsigned long long* prof; // nullable: [1 + grid * kProfSlots] phase times (ns) per CTA
   StageLay lay[kMaxGroups][P_NPASS];  // shared-memory image of a chunk, per group and pipelined pass

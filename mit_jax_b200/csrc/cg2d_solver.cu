@@ -711,7 +711,7 @@ __device__ void init_x_ring(const KParams& kp, const Smem& sm) {
 // ------------------------------------------------------------------------------------------------
 // pipelined passes: chunks of this CTA in order, bulk copies into two stage buffers
 
-// this CTA's work units: u = blockIdx.x + n gridDim.x, packed once at the start of the launch
+// this CTA's work units (dealt by build_unit_table), packed once at the start of the launch
 //   x = gi | inst << 2 | lu << 10,   y = t | j0 << 8 | j1 << 19
 struct Unit {
   int gi, inst, lu, t, j0, j1;
@@ -724,18 +724,21 @@ __device__ __forceinline__ Unit unit_at(const Smem& sm, int ui) {
   return u;
 }
 __device__ void build_unit_table(const KParams& kp, const Smem& sm) {
-  // Units are dealt to the CTAs round-robin in this order: every group's full row blocks (instance, tile,
-  // block), then the shorter last blocks of the tiles, so that every CTA gets the same number of rows to within
-  // one unit.
+  // Units are taken in this order: every group's full row blocks (instance, tile, block), then the shorter last
+  // blocks of the tiles. They are dealt to the CTAs round-robin (unit_deal 0: every CTA gets the same number of
+  // rows to within one unit) or as contiguous runs of that order (unit_deal 1: neighbouring blocks of a tile on
+  // one CTA; the runs differ in length by at most one unit).
   const int R = kp.rows_per_block;
   int nfull = 0;
   for (int gi = 0; gi < kp.ngroups; ++gi) {
     const GroupDev& g = kp.g[gi];
     nfull += g.count * g.tp.T * (kp.serial ? 1 : g.tp.nj / R);
   }
-  const int n = (kp.total_units - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int lo = (int)((long long)blockIdx.x * kp.total_units / gridDim.x);
+  const int hi = (int)((long long)(blockIdx.x + 1) * kp.total_units / gridDim.x);
+  const int n = kp.unit_deal ? hi - lo : (kp.total_units - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
   for (int q = threadIdx.x; q < n; q += kThreads) {
-    int o = (int)blockIdx.x + q * (int)gridDim.x;
+    int o = kp.unit_deal ? lo + q : (int)blockIdx.x + q * (int)gridDim.x;
     const bool full = o < nfull;
     if (!full) o -= nfull;
     int gi = 0, inst = 0, t = 0, blk = 0;

@@ -28,7 +28,8 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_struct_layouts():
-    assert ctypes.sizeof(capi.Params) == 48
+    assert ctypes.sizeof(capi.Params) == 56
+    assert capi.Params.unit_deal.offset == 48
     assert ctypes.sizeof(capi.Diag) == 48
     assert ctypes.sizeof(capi.Group) == 8 + 4 + 4 + 6 * 8 + 8 + 8 + 5 * 16 + 16 + 8
 
@@ -48,3 +49,29 @@ def test_bad_arguments_are_rejected_without_a_gpu():
     g = (capi.Group * 1)()
     assert lib.cg2d_workspace_size(g, 1, None) == 0          # no topology
     assert lib.cg2d_solve_groups(g, 0, None, None, 0, None) == capi.CG2D_BAD_ARG
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """sizeof and every field offset of cg2d_params_t and cg2d_diag_t as gcc lays out include/cg2d.h."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no gcc")
+    root = Path(__file__).resolve().parents[1]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cg2d.h"', 'int main(void) {']
+    for cname, st in (("cg2d_params_t", capi.Params), ("cg2d_diag_t", capi.Diag)):
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in st._fields_:
+            lines.append(f'  printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-I", str(root / "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                         text=True).stdout.splitlines())
+    for cname, st in (("cg2d_params_t", capi.Params), ("cg2d_diag_t", capi.Diag)):
+        assert int(got[cname]) == ctypes.sizeof(st), cname
+        for f, _ in st._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(st, f).offset, (cname, f)
