@@ -88,9 +88,20 @@ __device__ __forceinline__ double nbx0(const TopoDev& tp, const double* x0, doub
 struct Geo {
   TopoDev tp;
   int batch;
-  long long pe;   // padded elements per instance
-  long long pts;  // interior points per instance
+  long long pe;     // padded elements per instance
+  long long pts;    // interior points per instance
+  const int* nbp;   // tp.nbr with padded offsets in the instance instead of compact indices (-1: unwritten)
 };
+
+// nbp from tp.nbr: the same [W: T nj][E: T nj][S: T ni][N: T ni] layout, each entry the padded offset of the
+// source point (cmp_pad) or -1
+__global__ void k_nbp(TopoDev tp, int* nbp) {
+  const int n = 2 * tp.T * (tp.nj + tp.ni);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int src = tp.nbr[e];
+    nbp[e] = src >= 0 ? (int)cmp_pad(tp, src) : -1;
+  }
+}
 // Point kernels run one thread per interior point: threadIdx.x = i, one tile row per threadIdx.y,
 // blockIdx.x = group of rows (row = t nj + j), blockIdx.y = instance. Face kernels use the same shape over
 // i = 0..ni and rows j = 0..nj of each tile.
@@ -115,20 +126,6 @@ __global__ void k_init(Geo G, const double* aW, const double* aS, const double* 
                         nbx0(tp, x0i, rni, t, j + 1, i), vc);
   r[p] = sub(mul(mul(b[p], norm[in]), rni), ax);
   x[p] = vc;
-}
-
-// out = [base +] A v (mode 0) or M v (mode 1) on the interior of live instances
-__global__ void k_stencil(Geo G, int mode, const double* c0, const double* c1, const double* c2, const double* v,
-                          const double* base, double* out, const int* K, int k) {
-  POINT(G, in, t, j, i, p);
-  if (!live(K, in, k)) return;
-  const TopoDev& tp = G.tp;
-  const double* vi = v + (long long)in * G.pe;
-  const double vw = nbv(tp, vi, t, j, i - 1), ve = nbv(tp, vi, t, j, i + 1);
-  const double vs = nbv(tp, vi, t, j - 1, i), vn = nbv(tp, vi, t, j + 1, i), vc = v[p];
-  const double o = mode == 0 ? opA(c0[p], c0[p + 1], c1[p], c1[p + tp.npx], c2[p], vw, ve, vs, vn, vc)
-                             : opM(c2[p], c0[p], c0[p + 1], c1[p], c1[p + tp.npx], vc, vw, ve, vs, vn);
-  out[p] = base ? add(base[p], o) : o;
 }
 
 // row sums of up to two products a0 b0, a1 b1 of live instances: rs[(in 2 + q)][t nj + j], one warp per row,
@@ -241,38 +238,187 @@ __global__ void k_rev_beta(Geo G, int R, const double* rs, Scal S, const int* K,
   S.carry[in] = -bbar * eta / (etap * etap);
 }
 
-// forward updates of live instances
-__global__ void k_fwd_s(Geo G, const double* z, const double* sprev, double* s, Scal S, const int* K, int k) {
-  POINT(G, in, t, j, i, p);
-  if (!live(K, in, k)) return;
-  s[p] = add(z[p], mul(S.beta[(long long)k * G.batch + in], sprev[p]));          // cg2d.py:249
+// ---- fused iteration kernels: one thread per interior point (POINT layout), the whole block returning together
+// when its instance (blockIdx.y) takes no part, so that the row sums may synchronise the block
+
+#define POINT_IN(G)                                                                       \
+  const TopoDev& tp = (G).tp;                                                             \
+  const int i = threadIdx.x, in = blockIdx.y;                                             \
+  const int row = blockIdx.x * blockDim.y + threadIdx.y;                                  \
+  const bool inb = i < tp.ni && row < tp.T * tp.nj;                                       \
+  const int t = inb ? row / tp.nj : 0, j = inb ? row - t * tp.nj : 0;                     \
+  const long long base = (long long)in * (G).pe;                                          \
+  const int off = ((t * tp.npy + j + tp.OLy) * tp.npx) + i + tp.OLx;                      \
+  const long long p = base + off;                                                         \
+  int ow = -1, oe = -1, os = -1, on = -1;                                                 \
+  if (inb) neighbours(G, t, j, i, off, ow, oe, os, on)
+
+// padded offsets (in the instance) of the west, east, south and north neighbours of interior point (t, j, i) at
+// offset off, as the exchange supplies them: the next point in the tile, or across a tile edge the source the
+// exch2 map names (-1: unwritten, reads 0)
+__device__ __forceinline__ void neighbours(const Geo& G, int t, int j, int i, int off, int& ow, int& oe, int& os,
+                                           int& on) {
+  const TopoDev& tp = G.tp;
+  const int T = tp.T, nj = tp.nj, ni = tp.ni;
+  ow = i > 0 ? off - 1 : G.nbp[t * nj + j];
+  oe = i < ni - 1 ? off + 1 : G.nbp[T * nj + t * nj + j];
+  os = j > 0 ? off - tp.npx : G.nbp[2 * T * nj + t * ni + i];
+  on = j < nj - 1 ? off + tp.npx : G.nbp[2 * T * nj + T * ni + t * ni + i];
 }
-__global__ void k_fwd_rx(Geo G, const double* s, const double* q, const double* r, double* rout, double* x, Scal S,
-                         const int* K, int k) {
-  POINT(G, in, t, j, i, p);
-  if (!live(K, in, k)) return;
-  const double a = S.alpha[(long long)k * G.batch + in];
-  if (x) x[p] = add(x[p], mul(a, s[p]));                                        // cg2d.py:254
-  rout[p] = sub(r[p], mul(a, q[p]));                                            // cg2d.py:255
+
+// Row sums of up to two per-point products (v0, v1; points outside the tile pass inb = false) for the row of
+// threadIdx.y, in k_rowdot's order: lane partials over i = lane + 32 m in order, then the xor butterfly. The
+// products go through shared memory ([2][blockDim.y][blockDim.x] doubles). Every thread of the block calls it.
+__device__ void row_sums(const Geo& G, int in, int row, bool inb, double v0, double v1, int nq, double* rs) {
+  extern __shared__ double shp[];
+  const int bx = blockDim.x, by = blockDim.y, x = threadIdx.x, y = threadIdx.y;
+  shp[y * bx + x] = inb ? v0 : 0.0;
+  if (nq > 1) shp[(by + y) * bx + x] = inb ? v1 : 0.0;
+  __syncthreads();
+  const int rows = G.tp.T * G.tp.nj;
+  if (x < 32 && row < rows) {
+    for (int q = 0; q < nq; ++q) {
+      double v = 0.0;
+      for (int ii = x; ii < G.tp.ni; ii += 32) v = add(v, shp[(q * by + y) * bx + ii]);
+      for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (x == 0) rs[((long long)in * 2 + q) * rows + row] = v;
+    }
+  }
 }
-// reverse: qbar = sigbar s - alpha rbar;  sbar += alpha xbar + sigbar q
-__global__ void k_rev_q(Geo G, const double* s, const double* q, const double* xbar, const double* rbar, double* qbar,
-                        double* sbar, Scal S, const int* K, int k) {
-  POINT(G, in, t, j, i, p);
-  if (!live(K, in, k)) return;
-  const double a = S.alpha[(long long)k * G.batch + in], sg = S.sigbar[in];
-  qbar[p] = sg * s[p] - a * rbar[p];
-  sbar[p] = sbar[p] + a * xbar[p] + sg * q[p];
+
+// Iteration k, first half, with the updates of iteration k-1 (upd, k >= 1):
+//   r_k = r_{k-1} - alpha_{k-1} q_{k-1}  (cg2d.py:255; written to rout when non-null),
+//   x += alpha_{k-1} s_{k-1}              (cg2d.py:254; when x is non-null),
+//   z_k = M r_k (cg2d.py:245), the row sums of z_k r_k (cg2d.py:246; when rs is non-null),
+//   checkpoints of r_k and s_{k-1} (when ckr / cks are non-null).
+// Without upd, r_k is rp itself. r_k at a neighbour is formed from that neighbour's r_{k-1} and q_{k-1}: the
+// value its owner computes, as the exchange of r gives it (cg2d.py:260). The updates of iteration k-1 run for
+// instances that took it (k - 1 < K), the rest for instances that take iteration k.
+__global__ void k_fa(Geo G, const double* pW, const double* pS, const double* pC, const double* rp, const double* qp,
+                     const double* sp, double* x, double* rout, double* z, double* ckr, double* cks, double* rs,
+                     Scal S, const int* K, int k, int upd) {
+  const int Kin = K[blockIdx.y];
+  const bool zl = k < Kin, ul = upd && k - 1 < Kin;
+  if (!zl && !ul) return;
+  POINT_IN(G);
+  const double a = ul ? S.alpha[(long long)(k - 1) * G.batch + in] : 0.0;
+  auto R = [&](int o) -> double {
+    if (o < 0) return 0.0;
+    return upd ? sub(rp[base + o], mul(a, qp[base + o])) : rp[base + o];
+  };
+  double prod = 0.0;
+  if (inb) {
+    const double rc = R(off);
+    if (ul && rout) rout[p] = rc;
+    if (ul && x) x[p] = add(x[p], mul(a, sp[p]));
+    if (zl) {
+      if (ckr) ckr[p] = rc;
+      if (cks) cks[p] = sp[p];
+      const double zc = opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], rc, R(ow), R(oe), R(os), R(on));
+      z[p] = zc;
+      prod = mul(zc, rc);
+    }
+  }
+  if (rs && zl) row_sums(G, in, row, inb, prod, 0.0, 1, rs);
 }
-// reverse: zbar = sbar + etabar r;  rbar += etabar z;  sbar = beta sbar
-__global__ void k_rev_z(Geo G, const double* r, const double* z, double* zbar, double* rbar, double* sbar, Scal S,
-                        const int* K, int k) {
-  POINT(G, in, t, j, i, p);
-  if (!live(K, in, k)) return;
-  const double e = S.etabar[in];
-  zbar[p] = sbar[p] + e * r[p];
-  rbar[p] = rbar[p] + e * z[p];
-  sbar[p] = S.beta[(long long)k * G.batch + in] * sbar[p];
+
+// Iteration k, second half: s_k = z_k + beta_k s_{k-1} (cg2d.py:249), q_k = A s_k (cg2d.py:251), the row sums of
+// s_k q_k (cg2d.py:252; when rs is non-null). s_k at a neighbour is formed from that neighbour's z_k and s_{k-1}.
+__global__ void k_fb(Geo G, const double* aW, const double* aS, const double* aC, const double* z, const double* sp,
+                     double* s, double* q, double* rs, Scal S, const int* K, int k) {
+  if (k >= K[blockIdx.y]) return;
+  POINT_IN(G);
+  const double beta = S.beta[(long long)k * G.batch + in];
+  auto Sv = [&](int o) -> double { return o < 0 ? 0.0 : add(z[base + o], mul(beta, sp[base + o])); };
+  double prod = 0.0;
+  if (inb) {
+    const double sc = Sv(off);
+    const double qc = opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], Sv(ow), Sv(oe), Sv(os), Sv(on), sc);
+    s[p] = sc;
+    q[p] = qc;
+    prod = mul(sc, qc);
+  }
+  if (rs) row_sums(G, in, row, inb, prod, 0.0, 1, rs);
+}
+
+// Edge products of one point's faces for a stencil out = C v with out's cotangent u: the west and south faces of
+// the point, its own diagonal entry, and the east / north halo face when the point is the last of its row /
+// column (the faces edge_products_kernel writes). uc, uw, us: u at the point and its west / south neighbours
+// (interior only); vc, vw, ve, vs, vn: v at the point and its neighbours as the stencil reads it.
+__device__ __forceinline__ void point_edges(const TopoDev& tp, int j, int i, long long p, double uc, double uw,
+                                            double us, double vc, double vw, double ve, double vs, double vn,
+                                            double* gW, double* gS, double* gC) {
+  gW[p] += add(mul(uc, vw), i >= 1 ? mul(uw, vc) : 0.0);
+  gS[p] += add(mul(uc, vs), j >= 1 ? mul(us, vc) : 0.0);
+  gC[p] += mul(uc, vc);
+  if (i == tp.ni - 1) gW[p + 1] += mul(uc, ve);
+  if (j == tp.nj - 1) gS[p + tp.npx] += mul(uc, vn);
+}
+
+// Reverse of iteration k, first half. With qbar = sigbar s_k - alpha_k rbar (formed at each stencil point):
+//   sbar = bs sbar + alpha_k xbar + sigbar q_k + A qbar, bs = beta_{k+1} (the scaling of sbar left from the
+//   reverse of iteration k+1; none when k + 1 = K), gA += qbar (x) s_k, and the row sums of sbar s_{k-1}.
+__global__ void k_rq(Geo G, const double* aW, const double* aS, const double* aC, const double* s, const double* q,
+                     const double* xbar, const double* rbar, double* sbar, const double* sp, double* gW, double* gS,
+                     double* gC, double* rs, Scal S, const int* K, int k) {
+  const int Kin = K[blockIdx.y];
+  if (k >= Kin) return;
+  POINT_IN(G);
+  const long long o = (long long)k * G.batch + in;
+  const double a = S.alpha[o], sg = S.sigbar[in];
+  const bool scale = k + 1 < Kin;
+  const double bs = scale ? S.beta[o + G.batch] : 0.0;
+  auto SV = [&](int o) -> double { return o < 0 ? 0.0 : s[base + o]; };
+  auto RB = [&](int o) -> double { return o < 0 ? 0.0 : rbar[base + o]; };
+  double prod = 0.0;
+  if (inb) {
+    const double sc = SV(off), sw = SV(ow), se = SV(oe), ss = SV(os), sn = SV(on);
+    auto QB = [&](double sv, double rv) -> double { return sub(mul(sg, sv), mul(a, rv)); };
+    const double qc = QB(sc, RB(off)), qw = QB(sw, RB(ow)), qe = QB(se, RB(oe)), qs = QB(ss, RB(os)),
+                 qn = QB(sn, RB(on));
+    double sb = scale ? mul(bs, sbar[p]) : sbar[p];
+    sb = add(add(sb, mul(a, xbar[p])), mul(sg, q[p]));
+    sb = add(sb, opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], qw, qe, qs, qn, qc));
+    sbar[p] = sb;
+    point_edges(tp, j, i, p, qc, qw, qs, sc, sw, se, ss, sn, gW, gS, gC);
+    prod = mul(sb, sp[p]);
+  }
+  row_sums(G, in, row, inb, prod, 0.0, 1, rs);
+}
+
+// Reverse of iteration k, second half. With zbar = sbar + etabar r_k (formed at each stencil point):
+//   rbar += etabar z_k + M zbar, gM += zbar (x) r_k; and, when s1 / q1 (s_{k-1}, q_{k-1}) are given, the row sums
+//   of xbar s_{k-1} and rbar q_{k-1} for the reverse of iteration k-1. Those row sums are also formed for the
+//   instances whose last iteration is k-1 (K = k): their reverse starts there, with rbar still 0.
+__global__ void k_rz(Geo G, const double* pW, const double* pS, const double* pC, const double* r, const double* z,
+                     const double* sbar, double* rbar, double* gpW, double* gpS, double* gpC, const double* xbar,
+                     const double* s1, const double* q1, double* rs, Scal S, const int* K, int k) {
+  const int Kin = K[blockIdx.y];
+  const bool live = k < Kin, next = s1 != nullptr && k - 1 < Kin;
+  if (!live && !next) return;
+  POINT_IN(G);
+  const double e = live ? S.etabar[in] : 0.0;
+  auto RV = [&](int o) -> double { return o < 0 ? 0.0 : r[base + o]; };
+  auto SB = [&](int o) -> double { return o < 0 ? 0.0 : sbar[base + o]; };
+  double p0 = 0.0, p1 = 0.0;
+  if (inb) {
+    double rb = rbar[p];
+    if (live) {
+      const double rc = RV(off), rw = RV(ow), re = RV(oe), rs_ = RV(os), rn_ = RV(on);
+      auto ZB = [&](double sv, double rv) -> double { return add(sv, mul(e, rv)); };
+      const double zc = ZB(SB(off), rc), zw = ZB(SB(ow), rw), ze = ZB(SB(oe), re), zs = ZB(SB(os), rs_),
+                   zn = ZB(SB(on), rn_);
+      rb = add(rb, mul(e, z[p]));
+      rb = add(rb, opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], zc, zw, ze, zs, zn));
+      rbar[p] = rb;
+      point_edges(tp, j, i, p, zc, zw, zs, rc, rw, re, rs_, rn_, gpW, gpS, gpC);
+    }
+    if (next) {
+      p0 = mul(xbar[p], s1[p]);
+      p1 = mul(rb, q1[p]);
+    }
+  }
+  if (next) row_sums(G, in, row, inb, p0, p1, 2, rs);
 }
 
 // coefficient cotangents of a stencil application out = C v: gW/gS/gC += sign (u (x) v) on the faces and points
@@ -343,11 +489,12 @@ size_t exact_adjoint_workspace(const TopoDev& tp, int batch, int max_iters, int 
   b += vec * 5;                                   // r, s, z, q, x of the recording forward
   b += vec * 2 * (size_t)std::max(1, nseg);       // checkpoints: r_c, s_{c-1}
   b += vec * 4 * (size_t)C;                       // a segment's r, z, s, q
-  b += vec * 5;                                   // xbar, rbar, sbar, zbar, qbar
+  b += vec * 3;                                   // xbar, rbar, sbar
   b += sizeof(double) * batch * 2 * rows;         // row sums
   b += sizeof(double) * ((size_t)4 * std::max(1, max_iters) * batch + 5 * batch);   // scalars, rn, norm
   b += sizeof(int) * batch;
-  b += 256 * (size_t)(30 + 2 * std::max(1, nseg) + 4 * C);   // each buffer starts 256-byte aligned
+  b += sizeof(int) * 2 * (size_t)tp.T * (tp.nj + tp.ni);   // padded-offset neighbour table
+  b += 256 * (size_t)(31 + 2 * std::max(1, nseg) + 4 * C);   // each buffer starts 256-byte aligned
   return b;
 }
 
@@ -370,7 +517,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   for (int c = 0; c < std::max(1, nseg); ++c) { ck_r[c] = vec(); ck_s[c] = vec(); }
   std::vector<double*> sg_r(C), sg_z(C), sg_s(C), sg_q(C);
   for (int c = 0; c < C; ++c) { sg_r[c] = vec(); sg_z[c] = vec(); sg_s[c] = vec(); sg_q[c] = vec(); }
-  double *xbar = vec(), *rbar = vec(), *sbar = vec(), *zbar = vec(), *qbar = vec();
+  double *xbar = vec(), *rbar = vec(), *sbar = vec();
   double* rs = reinterpret_cast<double*>(take(sizeof(double) * A.batch * 2 * rows));
   Scal S;
   const size_t kb = (size_t)std::max(1, Kmax) * A.batch * sizeof(double);
@@ -384,6 +531,8 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   double* rn = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
   double* nrm = reinterpret_cast<double*>(take(sizeof(double) * A.batch));
   int* K = reinterpret_cast<int*>(take(sizeof(int) * A.batch));
+  int* nbp = reinterpret_cast<int*>(take(sizeof(int) * 2 * (size_t)tp.T * (tp.nj + tp.ni)));
+  G.nbp = nbp;
 
   // point kernels: a row of ni threads (rounded up to whole warps) per threadIdx.y; face kernels the same over
   // ni + 1 faces and nj + 1 face rows; row sums one warp per row; scalar steps one block per instance
@@ -394,6 +543,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   const dim3 gw((rows + 7) / 8, A.batch);
   const int gi = (A.batch + 127) / 128, nbk = (tp.nj + A.rows_per_block - 1) / A.rows_per_block;
   const size_t fold_sh = sizeof(double) * (size_t)tp.T * (nbk + 1);
+  const size_t row_sh = sizeof(double) * 2 * bp.x * bp.y;   // row_sums: two products per thread
   if (fold_sh > 48 * 1024) return cudaErrorInvalidValue;
   const size_t vb = vecn * sizeof(double);
   cudaError_t e;
@@ -407,36 +557,34 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   } while (0)
   CK(cudaMemsetAsync(s, 0, vb, st));          // s_{-1} = 0
   for (double* g : {A.gW, A.gS, A.gC, A.gpW, A.gpS, A.gpC, A.b_bar}) CK(cudaMemsetAsync(g, 0, vb, st));
-  for (double* v : {xbar, rbar, sbar, zbar, qbar}) CK(cudaMemsetAsync(v, 0, vb, st));
+  for (double* v : {xbar, rbar, sbar}) CK(cudaMemsetAsync(v, 0, vb, st));
   CK(cudaMemsetAsync(S.carry, 0, sizeof(double) * A.batch, st));
   k_setup<<<gi, 128, 0, st>>>(A.batch, A.fwd_diag, A.norm, A.norm_arr, rn, nrm, K);
+  LK();
+  k_nbp<<<(2 * tp.T * (tp.nj + tp.ni) + 255) / 256, 256, 0, st>>>(tp, nbp);
   LK();
   k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
   LK();
 
-  // ---- recording forward: scalars of every iteration, checkpoints of r and s_prev
-  double* sprev = s;
-  double* snew = sg_s[0];   // scratch until the segments are recomputed
-  for (int k = 0; k < Kmax; ++k) {
-    if (k % C == 0) {
-      CK(cudaMemcpyAsync(ck_r[k / C], r, vb, cudaMemcpyDeviceToDevice, st));
-      CK(cudaMemcpyAsync(ck_s[k / C], sprev, vb, cudaMemcpyDeviceToDevice, st));
-    }
-    k_stencil<<<gp, bp, 0, st>>>(G, 1, A.pW, A.pS, A.pC, r, nullptr, z, K, k);
+  // ---- recording forward: scalars of every iteration, checkpoints of r_k and s_{k-1} every C iterations. r and s
+  // alternate between two buffers (a stencil reads its neighbours' old values while every point writes its new
+  // one); the second ones borrow the first segment buffers, which the reverse sweep fills later.
+  double *rcur = r, *rnext = sg_r[0];
+  double *sprev = s, *snew = sg_s[0];
+  for (int k = 0; k <= Kmax; ++k) {
+    const bool ck = k < Kmax && k % C == 0;
+    if (k == Kmax && !A.x_check) break;   // the last updates only move x
+    k_fa<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rcur, q, sprev, A.x_check ? x : nullptr, rnext, z,
+                                 ck ? ck_r[k / C] : nullptr, ck ? ck_s[k / C] : nullptr, k < Kmax ? rs : nullptr,
+                                 S, K, k, k > 0);
     LK();
-    k_rowdot<<<gw, 256, 0, st>>>(G, z, r, nullptr, nullptr, rs, K, k);
-    LK();
+    if (k > 0) std::swap(rcur, rnext);
+    if (k == Kmax) break;
     k_fwd_eta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
     LK();
-    k_fwd_s<<<gp, bp, 0, st>>>(G, z, sprev, snew, S, K, k);
-    LK();
-    k_stencil<<<gp, bp, 0, st>>>(G, 0, A.aW, A.aS, A.aC, snew, nullptr, q, K, k);
-    LK();
-    k_rowdot<<<gw, 256, 0, st>>>(G, snew, q, nullptr, nullptr, rs, K, k);
+    k_fb<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, z, sprev, snew, q, rs, S, K, k);
     LK();
     k_fwd_sigma<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
-    LK();
-    k_fwd_rx<<<gp, bp, 0, st>>>(G, snew, q, r, r, x, S, K, k);
     LK();
     std::swap(sprev, snew);
   }
@@ -449,45 +597,33 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   k_scale<<<gp, bp, 0, st>>>(G, A.xbar, nrm, rn, xbar, 0);
   LK();
   for (int seg = nseg - 1; seg >= 0; --seg) {
-    const int c0 = seg * C, c1 = std::min(Kmax, c0 + C);
-    // recompute the segment's r, z, s, q with the recorded alpha and beta
-    CK(cudaMemcpyAsync(sg_r[0], ck_r[seg], vb, cudaMemcpyDeviceToDevice, st));
-    for (int k = c0; k < c1; ++k) {
-      const int m = k - c0;
-      const double* sp = m == 0 ? ck_s[seg] : sg_s[m - 1];
-      k_stencil<<<gp, bp, 0, st>>>(G, 1, A.pW, A.pS, A.pC, sg_r[m], nullptr, sg_z[m], K, k);
+    const int c0 = seg * C, c1 = std::min(Kmax, c0 + C), len = c1 - c0;
+    auto rr = [&](int m) -> double* { return m == 0 ? ck_r[seg] : sg_r[m]; };
+    auto sp = [&](int m) -> double* { return m == 0 ? ck_s[seg] : sg_s[m - 1]; };
+    // recompute the segment's r, z, s, q with the recorded alpha and beta (the recording forward's operations)
+    for (int m = 0; m < len; ++m) {
+      const int k = c0 + m;
+      k_fa<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, m == 0 ? ck_r[seg] : rr(m - 1), m == 0 ? nullptr : sg_q[m - 1],
+                                   nullptr, nullptr, m == 0 ? nullptr : sg_r[m], sg_z[m], nullptr, nullptr, nullptr,
+                                   S, K, k, m > 0);
       LK();
-      k_fwd_s<<<gp, bp, 0, st>>>(G, sg_z[m], sp, sg_s[m], S, K, k);
+      k_fb<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_z[m], sp(m), sg_s[m], sg_q[m], nullptr, S, K, k);
       LK();
-      k_stencil<<<gp, bp, 0, st>>>(G, 0, A.aW, A.aS, A.aC, sg_s[m], nullptr, sg_q[m], K, k);
-      LK();
-      if (m + 1 < c1 - c0) {
-        k_fwd_rx<<<gp, bp, 0, st>>>(G, sg_s[m], sg_q[m], sg_r[m], sg_r[m + 1], nullptr, S, K, k);
-        LK();
-      }
     }
-    for (int k = c1 - 1; k >= c0; --k) {
-      const int m = k - c0;
-      const double* sp = m == 0 ? ck_s[seg] : sg_s[m - 1];
-      k_rowdot<<<gw, 256, 0, st>>>(G, xbar, sg_s[m], rbar, sg_q[m], rs, K, k);
-      LK();
+    // the row sums of alphabar for the segment's last iteration (inside a segment k_rz forms them)
+    k_rowdot<<<gw, 256, 0, st>>>(G, xbar, sg_s[len - 1], rbar, sg_q[len - 1], rs, K, c1 - 1);
+    LK();
+    for (int m = len - 1; m >= 0; --m) {
+      const int k = c0 + m;
       k_rev_alpha<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rev_q<<<gp, bp, 0, st>>>(G, sg_s[m], sg_q[m], xbar, rbar, qbar, sbar, S, K, k);
-      LK();
-      k_stencil<<<gp, bp, 0, st>>>(G, 0, A.aW, A.aS, A.aC, qbar, sbar, sbar, K, k);
-      LK();
-      k_edges<false><<<ge, be, 0, st>>>(G, qbar, sg_s[m], rn, 1.0, A.gW, A.gS, A.gC, K, k);
-      LK();
-      k_rowdot<<<gw, 256, 0, st>>>(G, sbar, sp, nullptr, nullptr, rs, K, k);
+      k_rq<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_s[m], sg_q[m], xbar, rbar, sbar, sp(m), A.gW, A.gS, A.gC,
+                                   rs, S, K, k);
       LK();
       k_rev_beta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rev_z<<<gp, bp, 0, st>>>(G, sg_r[m], sg_z[m], zbar, rbar, sbar, S, K, k);
-      LK();
-      k_stencil<<<gp, bp, 0, st>>>(G, 1, A.pW, A.pS, A.pC, zbar, rbar, rbar, K, k);
-      LK();
-      k_edges<false><<<ge, be, 0, st>>>(G, zbar, sg_r[m], rn, 1.0, A.gpW, A.gpS, A.gpC, K, k);
+      k_rz<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rr(m), sg_z[m], sbar, rbar, A.gpW, A.gpS, A.gpC, xbar,
+                                   m > 0 ? sg_s[m - 1] : nullptr, m > 0 ? sg_q[m - 1] : nullptr, rs, S, K, k);
       LK();
     }
   }
