@@ -159,6 +159,81 @@ class LLCSynthetic:
     def first_guess(self):
         return np.zeros(self.L.shape2d)
 
+    # ---------------------------------------------------------------------------------------------------------
+    def model_fields(self, Nr=50, member=None):
+        """Inputs of UPDATE_CG2D and SOLVE_FOR_PRESSURE (mitgcm_jax/core/solve_for_pressure.py:29-123) for one member:
+        a dict of float64 arrays, 3-D fields [T, Nr, ny, nx], 2-D fields [T, ny, nx], plus the scalars of the
+        free-surface and CG2D parameters (V4r4 values: dt = 3600 s, freeSurfFac = implicSurfPress =
+        implicDiv2DFlow = 1, rhoConst = 1029, cg2dpcOffDFac = 0.51).
+
+        * drF: layer thicknesses growing geometrically from 10 m, scaled to 6000 m in all;
+        * hFacC(k): wet fraction of level k above the member's depth (0 below it and on land); hFacW, hFacS:
+          min of the two cells of a face on the interior faces (Fortran i, j = 1..N), the east / north face halos
+          through the UVn exchange (EXCH_UV_XYZ), so that the operator built from them is symmetric;
+        * face metrics dyG, recip_dxC (u faces) and dxG, recip_dyC (v faces) from the spacing, exchanged as pairs;
+          rA through the scalar exchange; maskInC = ocean;
+        * Bo_surf = g (1 + 0.01 e), recip_Bo = 1 / Bo_surf; gU, gV: smooth noise of 1e-5 m/s^2 on wet faces;
+          EmPmR: smooth noise of 1e-5 on ocean; etaN, etaH: smooth noise of 0.5 m on ocean (scalar exchange);
+        * cg2dNorm: 1 / max|aW, aS| of the level-summed faces (ini_cg2d.F as in mitgcm_jax/init.py:325-345)."""
+        L, maps = self.L, self.topo.maps
+        J, I = L.interior
+        T, ny, nx = L.shape2d
+        tsrc, tcomp = maps["T"][:2]
+        seed = 0 if member is None else 100 + member
+        g = np.geomspace(10.0, 460.0, Nr)
+        drF = g * (6000.0 / g.sum())
+        zF = np.concatenate([[0.0], np.cumsum(drF)])
+        He = exch_scalar(self.member_depth(member), tsrc, tcomp)
+        hFacC = np.clip((He[:, None] - zF[None, :-1, None, None]) / drF[None, :, None, None], 0.0, 1.0)
+        Im, Jm = L.is_(0, L.sNx - 1), L.js(0, L.sNy - 1)
+        hW = np.zeros((T, Nr, ny, nx))
+        hS = np.zeros((T, Nr, ny, nx))
+        hW[:, :, J, I] = np.minimum(hFacC[:, :, J, I], hFacC[:, :, J, Im])
+        hS[:, :, J, I] = np.minimum(hFacC[:, :, J, I], hFacC[:, :, Jm, I])
+        hW, hS = (np.moveaxis(a, 1, 0) for a in exch_vector(np.moveaxis(hW, 1, 0), np.moveaxis(hS, 1, 0),
+                                                             maps["UVn_u"], maps["UVn_v"]))
+        z = np.zeros(L.shape2d)
+
+        def inner(a):
+            out = z.copy()
+            out[:, J, I] = a[:, J, I]
+            return out
+
+        dyG, dxG = exch_vector(inner(self.dy), inner(self.dx), maps["UVn_u"], maps["UVn_v"])
+        rdxC, rdyC = exch_vector(inner(1.0 / self.dx), inner(1.0 / self.dy), maps["UVn_u"], maps["UVn_v"])
+        rA = exch_scalar(inner(self.rA), tsrc, tcomp)
+        grid = self.topo.grid
+
+        def noise(k, scale, mask):
+            f = _to_tiles(self.topo, _facet_noise(grid, 5000 + 10 * seed + k, self.sigma))
+            f = f / max(np.abs(f).max(), 1e-300)
+            return exch_scalar(inner(scale * f * mask), tsrc, tcomp)
+
+        ocean = self.ocean
+        Bo = exch_scalar(inner(GRAVITY * (1.0 + 0.01 * noise(0, 1.0, np.ones(L.shape2d)))), tsrc, tcomp)
+        Bo = np.where(Bo == 0.0, GRAVITY, Bo)                            # unwritten halo points: plain g
+        recip_Bo = 1.0 / Bo
+        rng = np.random.default_rng(6000 + seed)
+        gU = np.zeros((T, Nr, ny, nx))
+        gV = np.zeros((T, Nr, ny, nx))
+        gU[:, :, J, I] = 1e-5 * rng.standard_normal((T, Nr, L.sNy, L.sNx)) * (hW[:, :, J, I] > 0)
+        gV[:, :, J, I] = 1e-5 * rng.standard_normal((T, Nr, L.sNy, L.sNx)) * (hS[:, :, J, I] > 0)
+        gU, gV = (np.moveaxis(a, 1, 0) for a in exch_vector(np.moveaxis(gU, 1, 0), np.moveaxis(gV, 1, 0),
+                                                             maps["UVn_u"], maps["UVn_v"]))
+        aW = np.zeros((T, L.sNy, L.sNx))
+        aS = np.zeros((T, L.sNy, L.sNx))
+        for k in range(Nr):
+            aW = aW + (dyG[:, J, I] * drF[k] * hW[:, k][:, J, I]) * rdxC[:, J, I]
+            aS = aS + (dxG[:, J, I] * drF[k] * hS[:, k][:, J, I]) * rdyC[:, J, I]
+        my = max(np.abs(aW).max(), np.abs(aS).max())
+        return dict(
+            Nr=Nr, drF=drF, hFacW=hW, hFacS=hS, dyG=dyG, dxG=dxG, recip_dxC=rdxC, recip_dyC=rdyC, rA=rA,
+            maskInC=inner(ocean), Bo_surf=Bo, recip_Bo=recip_Bo, gU=gU, gV=gV,
+            EmPmR=noise(1, 1e-5, ocean), etaN=noise(2, 0.5, ocean), etaH=noise(3, 0.5, ocean),
+            cg2dNorm=(1.0 / my) if my != 0.0 else 1.0, cg2dpcOffDFac=PC_OFFDIAG_FAC,
+            deltaTMom=DELTA_T, deltaTFreeSurf=DELTA_T, freeSurfFac=1.0, implicSurfPress=1.0, implicDiv2DFlow=1.0,
+            mass2rUnit=1.0 / 1029.0, useRealFreshWaterFlux=True)
+
 
 def make_batch(N=90, count=1, ts=None, with_cotangent=False, members=None):
     """Stacked inputs of `count` members (or of the listed ensemble members): dict of [count, T, ny, nx] arrays plus

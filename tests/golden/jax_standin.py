@@ -75,7 +75,7 @@ def install():
 
     for name in ("zeros", "ones", "zeros_like", "ones_like", "where", "sum", "max", "min", "abs", "sqrt", "maximum",
                  "minimum", "moveaxis", "logical_not", "logical_and", "vdot", "stack", "concatenate", "full",
-                 "arange", "isfinite", "all", "any"):
+                 "arange", "isfinite", "all", "any", "argmax"):
         setattr(jnp, name, _wrap(getattr(np, name)))
     jnp.asarray = _wrap(lambda a, dtype=None: np.array(a, dtype=dtype, copy=True))
     jnp.array = jnp.asarray
@@ -90,12 +90,20 @@ def install():
         return st
 
     def scan(f, init, xs, length=None, reverse=False, unroll=1):
+        # xs: an array, or a tuple / list of arrays sliced together along their first axis (a pytree of arrays)
         carry = init
         ys = []
-        n = len(xs) if xs is not None else length
+        multi = isinstance(xs, (tuple, list))
+        n = (len(xs[0]) if multi else len(xs)) if xs is not None else length
         order = range(n - 1, -1, -1) if reverse else range(n)
+
+        def item(i):
+            if xs is None:
+                return None
+            return type(xs)(_w(a[i]) for a in xs) if multi else _w(xs[i])
+
         for i in order:
-            carry, y = f(carry, None if xs is None else _w(xs[i]))
+            carry, y = f(carry, item(i))
             ys.append(y)
         if all(y is None for y in ys):
             return carry, None
@@ -133,6 +141,33 @@ def install():
     tu.register_pytree_node_class = lambda cls: cls
     tu.register_dataclass = lambda cls, data_fields=None, meta_fields=None: cls
     tree.map = lambda f, t: {k: f(v) for k, v in t.items()} if isinstance(t, dict) else f(t)
+
+    # pytrees of tuples, lists and dicts (keys in sorted order); anything else is a leaf
+    def flatten(t):
+        if isinstance(t, (tuple, list)):
+            parts = [flatten(x) for x in t]
+            return [leaf for ls, _ in parts for leaf in ls], (type(t), None, [d for _, d in parts])
+        if isinstance(t, dict):
+            keys = sorted(t)
+            parts = [flatten(t[k]) for k in keys]
+            return [leaf for ls, _ in parts for leaf in ls], (dict, keys, [d for _, d in parts])
+        return [t], None
+
+    def unflatten(treedef, leaves):
+        it = iter(leaves)
+
+        def build(d):
+            if d is None:
+                return next(it)
+            typ, keys, subs = d
+            if typ is dict:
+                return {k: build(s) for k, s in zip(keys, subs)}
+            return typ(build(s) for s in subs)
+
+        return build(treedef)
+
+    tree.flatten = flatten
+    tree.unflatten = unflatten
     dtypes.float0 = np.dtype([])
 
     class _Config:
