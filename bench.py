@@ -13,6 +13,9 @@ instance sharing its operator in ONE persistent mixed-precision launch, followed
 --impl reference times the reference's CPU path (the oracle restatement of cg2d_fortran, FP64, forward + tight
 adjoint solve + coefficient cotangents) on all host cores, one instance per process.
 
+--mode pressure times SOLVE_FOR_PRESSURE around the solve (update_cg2d, cg2d_rhs, the FP64 solve, the post-solve
+exchange; default batch 16, 50 levels), each step with its own device time and bandwidth.
+
 --mode exact times the exact-mode adjoint instead (cg2d_adjoint_exact: FP64 forward, then reverse mode through
 every CG iteration with checkpointed, recomputed segments; default batch 16) and reports adjoint solves/s and the
 peak device memory of the step. The reference has no exact mode (it differentiates cg2d implicitly), so
@@ -45,8 +48,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--mode", default="forward_adjoint", choices=("forward_adjoint", "exact"))
-    ap.add_argument("--batch", type=int, default=None, help="instances per GPU (64; 16 with --mode exact)")
+    ap.add_argument("--mode", default="forward_adjoint", choices=("forward_adjoint", "exact", "pressure"))
+    ap.add_argument("--batch", type=int, default=None, help="instances per GPU (64; 16 with --mode exact/pressure)")
+    ap.add_argument("--nr", type=int, default=50, help="--mode pressure: vertical levels")
     ap.add_argument("--checkpoint", type=int, default=30, help="--mode exact: iterations between checkpoints")
     ap.add_argument("--precision", default="mixed", choices=("mixed", "f64"))
     ap.add_argument("--tol", type=float, default=1e-12)
@@ -58,7 +62,7 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="eager launches instead of CUDA graph replay")
     a = ap.parse_args()
     if a.batch is None:
-        a.batch = 16 if a.mode == "exact" else 64
+        a.batch = 16 if a.mode in ("exact", "pressure") else 64
     return a
 
 
@@ -610,8 +614,136 @@ def run_exact(a):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------------------------
+# SOLVE_FOR_PRESSURE around the solve
+
+PRESSURE_METRIC = "SOLVE_FOR_PRESSURE steps/s (update_cg2d + cg2d_rhs + FP64 CG2D + post) on B200"
+
+
+def pressure_config(a):
+    return {"workload": f"batch {a.batch} LLC90 SOLVE_FOR_PRESSURE with {a.nr} levels: update_cg2d (operator and "
+                        f"preconditioner from the level sums), cg2d_rhs (g-hat divergence over the levels, fresh-water "
+                        f"and etaH terms), FP64 ROWBLOCK CG2D to {a.tol:g}, exchange and etaN",
+            "batch_per_gpu": a.batch, "levels": a.nr, "tolerance": a.tol, "max_iters": a.maxit,
+            "grid": "LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)", "parallelism": "1 GPU"}
+
+
+def pressure_bytes(B, Nr, n=90, T=13, npad=98):
+    """Algorithmic bytes per launch. update_cg2d: hFacW, hFacS and four face metrics read on the (n+1)^2 faces per
+    tile for every level, aW2d and aS2d written on the padded tile, then aW2d, aS2d, recip_Bo, rA read on the interior
+    and aC2d, pW, pS, pC written. cg2d_rhs: gU, gV, hFacW, hFacS read per interior point and level, EmPmR, etaN,
+    etaH, rA, maskInC, Bo_surf, dyG, dxG read and cg2d_b, cg2d_x written per point. Post: x, cg2d_x, recip_Bo read
+    and etaN written per padded point."""
+    f1, pts, pe = T * (n + 1) ** 2, T * n * n, T * npad * npad
+    upd = B * (8 * f1 * (2 * Nr + 4) + 8 * 2 * pe) + B * (8 * 4 * pts + 8 * pe + 8 * 3 * f1)
+    rhs = B * (8 * pts * (4 * Nr + 8) + 8 * 2 * pe)
+    post = B * 8 * 4 * pe
+    return upd, rhs, post
+
+
+def run_pressure(a):
+    import torch
+
+    from mit_jax_b200 import cg2d as cg
+    from mit_jax_b200 import pressure as pr
+    from mit_jax_b200.synthetic import LLCSynthetic
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    syn = LLCSynthetic(90)
+    distinct = [syn.model_fields(a.nr, m) for m in range(min(a.batch, 8))]
+    fs = [distinct[m % len(distinct)] for m in range(a.batch)]
+    f0 = fs[0]
+    import types
+    g = types.SimpleNamespace(layout=syn.L, **{k: f0[k] for k in ("drF", "dyG", "dxG", "recip_dxC", "recip_dyC",
+                                                                   "rA", "maskInC")})
+    p = pr.FreeSurfParams(deltaTMom=f0["deltaTMom"], deltaTFreeSurf=f0["deltaTFreeSurf"],
+                          freeSurfFac=f0["freeSurfFac"], implicSurfPress=f0["implicSurfPress"],
+                          implicDiv2DFlow=f0["implicDiv2DFlow"], mass2rUnit=f0["mass2rUnit"],
+                          rUnit2mass=1.0 / f0["mass2rUnit"], facEmP=1.0, hFacInf=0.2, hFacSup=2.0,
+                          rStarAreaWeight=True, pfFacMom=1.0, select_rStar=2, nonlinFreeSurf=4,
+                          useRealFreshWaterFlux=True, Nr=a.nr)
+    st = {k: torch.as_tensor(np.stack([f[k] for f in fs])).to(dev)
+          for k in ("hFacW", "hFacS", "gU", "gV", "EmPmR", "etaN", "etaH")}
+    del distinct, fs
+    norms = torch.full((a.batch,), float(f0["cg2dNorm"]), dtype=torch.float64, device=dev)
+    cp = cg.Cg2dParams(cg2dMaxIters=a.maxit, cg2dTolerance=a.tol, cg2dNorm=norms, sum_order="rowblock")
+    grid = {k: torch.as_tensor(f0[k]).to(dev) for k in ("recip_Bo", "Bo_surf")}
+    g = types.SimpleNamespace(layout=syn.L, **{k: torch.as_tensor(getattr(g, k)).to(dev)
+                                               for k in ("drF", "dyG", "dxG", "recip_dxC", "recip_dyC", "rA",
+                                                         "maskInC")})
+    ex = cg.default_exchanger(syn.L)
+    prev = [torch.zeros((a.batch,) + syn.L.shape2d, dtype=torch.float64, device=dev) for _ in range(3)]
+    stream = torch.cuda.current_stream(dev)
+
+    def step(ev=None):
+        rec = (lambda i: ev[i].record(stream)) if ev else (lambda i: None)
+        rec(0)
+        ops = pr.update_cg2d(p, cp, g, ex, st["hFacW"], st["hFacS"], grid["recip_Bo"], *prev)
+        rec(1)
+        b, x0 = pr.cg2d_rhs(p, g, st["gU"], st["gV"], st["hFacW"], st["hFacS"], st["EmPmR"], st["etaN"],
+                            st["etaH"], grid["Bo_surf"], ex=ex)
+        rec(2)
+        G = cg.GroupSpec(ex, ops, [b], [x0], [a.tol], [a.maxit], norms)
+        ((x, _, dg),), = cg.solve_groups([G], precision="f64", check_status=False)
+        rec(3)
+        eta = pr.pressure_post(ex, x, x0, grid["recip_Bo"])
+        rec(4)
+        return eta, dg
+
+    for _ in range(max(3, a.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(a.steps)]
+    with Clocks(_gpu_uuid(torch, dev)) as clk:
+        time.sleep(0.25)
+        torch.cuda.synchronize(dev)
+        for s in range(a.steps):
+            eta, dg = step(evs[s])
+        torch.cuda.synchronize(dev)
+    clocks = clk.summary()
+    parts = [[e[i].elapsed_time(e[i + 1]) for e in evs] for i in range(4)]
+    total = evs[0][0].elapsed_time(evs[-1][4]) / a.steps
+    recs = cg.diag_records(dg)
+    upd_b, rhs_b, post_b = pressure_bytes(a.batch, a.nr)
+    peak, peak_kind = measured_peak()
+    upd_ms, rhs_ms, solve_ms, post_ms = (statistics.mean(x) for x in parts)
+    solve_alg = sum(N_LLC90 * r["numIters"] * 96 for r in recs)
+
+    def gbs(nbytes, ms):
+        return nbytes / (ms / 1e3) / 1e9
+
+    line = {
+        "metric": PRESSURE_METRIC, "value": a.batch / (total / 1e3), "unit": "instances/s", "n_gpus": 1,
+        "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": total, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": pressure_config(a),
+        "roofline": {"bound": "hbm", "achieved": gbs(rhs_b, rhs_ms), "peak": peak, "unit": "GB/s",
+                     "frac": gbs(rhs_b, rhs_ms) / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "k_rhs (cg2d_rhs)", "kernel_ms": rhs_ms, "algorithmic_bytes_per_launch": rhs_b},
+        "steps_ms": {"update_cg2d": upd_ms, "cg2d_rhs": rhs_ms, "cg2d_solve": solve_ms, "post": post_ms},
+        "steps_gbs": {"update_cg2d": gbs(upd_b, upd_ms), "cg2d_rhs": gbs(rhs_b, rhs_ms),
+                      "cg2d_solve": gbs(solve_alg, solve_ms), "post": gbs(post_b, post_ms)},
+        "cpu_baseline": None, "e2e": None,
+        "gpu_launches": a.steps * 6,
+        "clocks": clocks,
+        "iterations": {"mean": statistics.mean(r["numIters"] for r in recs), "not_ok":
+                       sum(r["status"] != "ok" for r in recs)},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     a = parse()
+    if a.mode == "pressure":
+        if a.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "--mode pressure has no CPU reference arm; its "
+                                  "parity is checked against the reference's own outputs in the tests"}))
+            return 0
+        return run_pressure(a)
     if a.mode == "exact":
         if a.impl == "reference":
             if int(os.environ.get("RANK", "0")) == 0:

@@ -197,6 +197,46 @@ cg2d_status_t cg2d_solve_f64_noalloc(const cg2d_topology_t* topo, int batch, dou
                                      double* x_out, double* x_fortran, cg2d_diag_t* diag,
                                      const cg2d_params_t* params, cg2d_stream_t stream);
 
+/* ---- The steps either side of the solve in SOLVE_FOR_PRESSURE, batched. 3-D fields are [batch][T][Nr][ny][nx],
+ * per-instance 2-D fields [batch][T][ny][nx], grid fields [T][ny][nx] shared by the batch (all float64, device,
+ * the reference layout). Results are bit for bit those of the reference's functions. The vertical factors
+ * deepFacC, rhoFacC, deepFac2F of the reference are all 1 (free_surface.py:121-125) and are not taken. */
+
+/* The FreeSurfParams fields these steps read (mitgcm_jax/core/free_surface.py). */
+typedef struct {
+  double deltaTMom, deltaTFreeSurf, freeSurfFac, implicSurfPress, implicDiv2DFlow, mass2rUnit;
+  int useRealFreshWaterFlux;
+  int Nr;
+} cg2d_freesurf_t;
+
+/* update_cg2d (mitgcm_jax/core/solve_for_pressure.py:29-65): aW2d, aS2d from the level sums of the r* face areas
+ * (hFacW, hFacS after UPDATE_R_STAR, halos filled), scaled by cg2dNorm (per instance when cg2dNorm_per_instance
+ * is non-null), aC2d exchanged, and pW, pS, pC rewritten on i, j = 1..sNx+1, 1..sNy+1 (in place: the other points
+ * keep their values). Grid fields: drF [Nr], dyG, dxG, recip_dxC, recip_dyC, rA, recip_Bo. */
+cg2d_status_t cg2d_update_operator(const cg2d_topology_t* topo, int batch, const cg2d_freesurf_t* fs,
+                                   double cg2dNorm, const double* cg2dNorm_per_instance, double cg2dpcOffDFac,
+                                   const double* hFacW, const double* hFacS, const double* drF,
+                                   const double* dyG, const double* dxG, const double* recip_dxC,
+                                   const double* recip_dyC, const double* rA, const double* recip_Bo,
+                                   double* aW2d, double* aS2d, double* aC2d, double* pW, double* pS, double* pC,
+                                   cg2d_stream_t stream);
+
+/* cg2d_rhs (solve_for_pressure.py:68-106): cg2d_b on the interior (0 on halos) from the fresh-water flux EmPmR
+ * (when fs->useRealFreshWaterFlux), the divergence of the g-hat transports (gU, gV, hFacW, hFacS; levels Nr..1) and
+ * the exactConserv etaH term; cg2d_x = Bo_surf etaN on the full array. Grid fields: drF [Nr], dyG, dxG, rA,
+ * maskInC, Bo_surf. */
+cg2d_status_t cg2d_pressure_rhs(const cg2d_topology_t* topo, int batch, const cg2d_freesurf_t* fs,
+                                const double* gU, const double* gV, const double* hFacW, const double* hFacS,
+                                const double* EmPmR, const double* etaN, const double* etaH, const double* drF,
+                                const double* dyG, const double* dxG, const double* rA, const double* maskInC,
+                                const double* Bo_surf, double* cg2d_b, double* cg2d_x, cg2d_stream_t stream);
+
+/* After the solve (solve_for_pressure.py:116-121): etaN = recip_Bo x, x the solution on the interior and, on halo
+ * points, its exchanged value, or the first guess cg2d_x where the exchange writes nothing. recip_Bo is a grid
+ * field [T][ny][nx]. */
+cg2d_status_t cg2d_pressure_post(const cg2d_topology_t* topo, int batch, const double* x, const double* cg2d_x,
+                                 const double* recip_Bo, double* etaN, cg2d_stream_t stream);
+
 /* Host-side error word of the last solve that used this workspace (synchronises the stream). */
 cg2d_status_t cg2d_workspace_status(const void* workspace, cg2d_stream_t stream);
 

@@ -6,7 +6,8 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SOURCES = [HERE / "csrc" / "cg2d_solver.cu", HERE / "csrc" / "cg2d_capi.cu", HERE / "csrc" / "cg2d_adjoint.cu"]
+SOURCES = [HERE / "csrc" / "cg2d_solver.cu", HERE / "csrc" / "cg2d_capi.cu", HERE / "csrc" / "cg2d_adjoint.cu",
+           HERE / "csrc" / "cg2d_pressure.cu"]
 OUT = HERE / "libcg2d.so"
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]

@@ -33,7 +33,8 @@ STATUS_NAMES = {0: "ok", 1: "not_converged", 2: "nan", 3: "barrier_timeout", 4: 
 EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_params", "cg2d_workspace_size",
             "cg2d_solve_groups", "cg2d_solve_f64", "cg2d_workspace_status", "cg2d_apply_operator",
             "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string", "cg2d_workspace_profile",
-            "cg2d_solve_f64_noalloc", "cg2d_adjoint_exact", "cg2d_adjoint_exact_workspace_size")
+            "cg2d_solve_f64_noalloc", "cg2d_adjoint_exact", "cg2d_adjoint_exact_workspace_size",
+            "cg2d_update_operator", "cg2d_pressure_rhs", "cg2d_pressure_post")
 
 
 class Params(ctypes.Structure):
@@ -50,6 +51,14 @@ class Diag(ctypes.Structure):
 
 
 DIAG_BYTES = ctypes.sizeof(Diag)   # 48
+
+
+class FreeSurf(ctypes.Structure):
+    """cg2d_freesurf_t: the FreeSurfParams fields of update_cg2d / cg2d_rhs."""
+    _fields_ = [("deltaTMom", ctypes.c_double), ("deltaTFreeSurf", ctypes.c_double),
+                ("freeSurfFac", ctypes.c_double), ("implicSurfPress", ctypes.c_double),
+                ("implicDiv2DFlow", ctypes.c_double), ("mass2rUnit", ctypes.c_double),
+                ("useRealFreshWaterFlux", ctypes.c_int), ("Nr", ctypes.c_int)]
 
 _P = ctypes.c_void_p
 _D2 = ctypes.c_void_p * 2
@@ -107,6 +116,12 @@ def lib():
     L.cg2d_exchange_scalar.restype = i
     L.cg2d_workspace_profile.argtypes = [_P, ctypes.POINTER(Group), i, ctypes.POINTER(Params), _P, i, _P]
     L.cg2d_workspace_profile.restype = i
+    L.cg2d_update_operator.argtypes = [_P, i, ctypes.POINTER(FreeSurf), d, _P, d] + [_P] * 15 + [_P]
+    L.cg2d_update_operator.restype = i
+    L.cg2d_pressure_rhs.argtypes = [_P, i, ctypes.POINTER(FreeSurf)] + [_P] * 15 + [_P]
+    L.cg2d_pressure_rhs.restype = i
+    L.cg2d_pressure_post.argtypes = [_P, i, _P, _P, _P, _P, _P]
+    L.cg2d_pressure_post.restype = i
     L.cg2d_status_string.argtypes = [i]
     L.cg2d_status_string.restype = ctypes.c_char_p
     _LIB = L

@@ -470,7 +470,9 @@ def cg2d_solve(p: Cg2dParams, ex: Exchanger, ops, cg2d_b, cg2d_x):
     box = {}
     x, xf = Cg2dSolve.apply(p, ex, box, *args)
     if numpy_in:
-        return x.detach().cpu().numpy(), dict(box["diag"], x_fortran=xf.detach().cpu().numpy())
+        x, xf = x.detach().cpu().numpy(), xf.detach().cpu().numpy()
+    if isinstance(box["diag"], list):   # a batch: one record per instance, each with its own x_fortran
+        return x, [dict(d, x_fortran=xf[m]) for m, d in enumerate(box["diag"])]
     return x, dict(box["diag"], x_fortran=xf)
 
 

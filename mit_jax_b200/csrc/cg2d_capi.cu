@@ -543,6 +543,74 @@ cg2d_status_t cg2d_exchange_scalar(const cg2d_topology_t* topo, int batch, const
   return CG2D_OK;
 }
 
+cg2d_status_t cg2d_update_operator(const cg2d_topology_t* topo, int batch, const cg2d_freesurf_t* fs,
+                                   double cg2dNorm, const double* cg2dNorm_per_instance, double cg2dpcOffDFac,
+                                   const double* hFacW, const double* hFacS, const double* drF,
+                                   const double* dyG, const double* dxG, const double* recip_dxC,
+                                   const double* recip_dyC, const double* rA, const double* recip_Bo,
+                                   double* aW2d, double* aS2d, double* aC2d, double* pW, double* pS, double* pC,
+                                   cg2d_stream_t stream) {
+  if (!topo || !fs || batch < 1 || batch > 65535 || fs->Nr < 1) return CG2D_BAD_ARG;
+  for (const void* q : {(const void*)hFacW, (const void*)hFacS, (const void*)drF, (const void*)dyG,
+                        (const void*)dxG, (const void*)recip_dxC, (const void*)recip_dyC, (const void*)rA,
+                        (const void*)recip_Bo, (const void*)aW2d, (const void*)aS2d, (const void*)aC2d,
+                        (const void*)pW, (const void*)pS, (const void*)pC})
+    if (!q) return CG2D_BAD_ARG;
+  UpdateArgs U;
+  U.batch = batch;
+  U.Nr = fs->Nr;
+  U.hFacW = hFacW; U.hFacS = hFacS; U.drF = drF; U.dyG = dyG; U.dxG = dxG;
+  U.recip_dxC = recip_dxC; U.recip_dyC = recip_dyC; U.rA = rA; U.recip_Bo = recip_Bo;
+  U.norm = cg2dNorm;
+  U.norm_arr = cg2dNorm_per_instance;
+  U.offd = cg2dpcOffDFac;
+  U.implicSurfPress = fs->implicSurfPress;
+  U.implicDiv2DFlow = fs->implicDiv2DFlow;
+  U.freeSurfFac = fs->freeSurfFac;
+  U.deltaTMom = fs->deltaTMom;
+  U.deltaTFreeSurf = fs->deltaTFreeSurf;
+  U.aW2d = aW2d; U.aS2d = aS2d; U.aC2d = aC2d; U.pW = pW; U.pS = pS; U.pC = pC;
+  if (pressure_update(topo_dev(topo), U, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+cg2d_status_t cg2d_pressure_rhs(const cg2d_topology_t* topo, int batch, const cg2d_freesurf_t* fs,
+                                const double* gU, const double* gV, const double* hFacW, const double* hFacS,
+                                const double* EmPmR, const double* etaN, const double* etaH, const double* drF,
+                                const double* dyG, const double* dxG, const double* rA, const double* maskInC,
+                                const double* Bo_surf, double* cg2d_b, double* cg2d_x, cg2d_stream_t stream) {
+  if (!topo || !fs || batch < 1 || batch > 65535 || fs->Nr < 1) return CG2D_BAD_ARG;
+  for (const void* q : {(const void*)gU, (const void*)gV, (const void*)hFacW, (const void*)hFacS,
+                        (const void*)etaN, (const void*)etaH, (const void*)drF, (const void*)dyG, (const void*)dxG,
+                        (const void*)rA, (const void*)Bo_surf, (const void*)cg2d_b, (const void*)cg2d_x})
+    if (!q) return CG2D_BAD_ARG;
+  if (fs->useRealFreshWaterFlux && (!EmPmR || !maskInC)) return CG2D_BAD_ARG;
+  RhsIn R;
+  R.batch = batch;
+  R.Nr = fs->Nr;
+  R.useRealFreshWaterFlux = fs->useRealFreshWaterFlux ? 1 : 0;
+  R.gU = gU; R.gV = gV; R.hFacW = hFacW; R.hFacS = hFacS; R.EmPmR = EmPmR; R.etaN = etaN; R.etaH = etaH;
+  R.drF = drF; R.dyG = dyG; R.dxG = dxG; R.rA = rA; R.maskInC = maskInC; R.Bo_surf = Bo_surf;
+  R.freeSurfFac = fs->freeSurfFac;
+  R.mass2rUnit = fs->mass2rUnit;
+  R.implicDiv2DFlow = fs->implicDiv2DFlow;
+  R.deltaTMom = fs->deltaTMom;
+  R.deltaTFreeSurf = fs->deltaTFreeSurf;
+  R.cg2d_b = cg2d_b;
+  R.cg2d_x = cg2d_x;
+  if (pressure_rhs(topo_dev(topo), R, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+cg2d_status_t cg2d_pressure_post(const cg2d_topology_t* topo, int batch, const double* x, const double* cg2d_x,
+                                 const double* recip_Bo, double* etaN, cg2d_stream_t stream) {
+  if (!topo || batch < 1 || batch > 65535 || !x || !cg2d_x || !recip_Bo || !etaN || etaN == x || etaN == cg2d_x)
+    return CG2D_BAD_ARG;
+  if (pressure_post(topo_dev(topo), batch, x, cg2d_x, recip_Bo, etaN, reinterpret_cast<cudaStream_t>(stream)) !=
+      cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------------

@@ -183,4 +183,27 @@ cudaError_t launch_edge_products(const TopoDev& tp, int batch, double norm, cons
                                  cudaStream_t stream);
 cudaError_t launch_exchange(const TopoDev& tp, int batch, const double* a, double* out, cudaStream_t stream);
 
+// ---- the steps either side of the solve (cg2d_pressure.cu)
+struct UpdateArgs {
+  int batch, Nr;
+  const double *hFacW, *hFacS;                                  // [batch][T][Nr][ny][nx]
+  const double *drF, *dyG, *dxG, *recip_dxC, *recip_dyC, *rA, *recip_Bo;   // shared grid fields
+  double norm;                                                  // cg2dNorm when norm_arr is null
+  const double* norm_arr;                                       // [batch] or null
+  double offd, implicSurfPress, implicDiv2DFlow, freeSurfFac, deltaTMom, deltaTFreeSurf;
+  double *aW2d, *aS2d, *aC2d, *pW, *pS, *pC;                    // [batch][T][ny][nx]
+};
+struct RhsIn {
+  int batch, Nr, useRealFreshWaterFlux;
+  const double *gU, *gV, *hFacW, *hFacS;                        // [batch][T][Nr][ny][nx]
+  const double *EmPmR, *etaN, *etaH;                            // [batch][T][ny][nx]
+  const double *drF, *dyG, *dxG, *rA, *maskInC, *Bo_surf;       // shared grid fields
+  double freeSurfFac, mass2rUnit, implicDiv2DFlow, deltaTMom, deltaTFreeSurf;
+  double *cg2d_b, *cg2d_x;
+};
+cudaError_t pressure_update(const TopoDev& tp, const UpdateArgs& U, cudaStream_t st);
+cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st);
+cudaError_t pressure_post(const TopoDev& tp, int batch, const double* x, const double* cg2d_x,
+                          const double* recip_Bo, double* etaN, cudaStream_t st);
+
 }  // namespace cg2d

@@ -1,0 +1,230 @@
+// The steps either side of the CG2D solve in SOLVE_FOR_PRESSURE, on a batch of instances:
+//   update_cg2d  (mitgcm_jax/core/solve_for_pressure.py:29-65): the operator aW2d, aS2d, aC2d from the level sums of
+//                the face areas, its diagonal exchanged, and the preconditioner pW, pS, pC;
+//   cg2d_rhs     (solve_for_pressure.py:68-106): the right-hand side (fresh-water flux, the divergence of the g-hat
+//                transports summed from level Nr up to 1, the exactConserv etaH term) and the first guess;
+//   post-solve   (solve_for_pressure.py:116-121): the exchange of the solution and etaN = recip_Bo x.
+// Every operation is the reference's, in its order, without contraction (__dmul_rn / __dadd_rn / __ddiv_rn), so
+// results are bit for bit those of the reference. The vertical factors deepFacC, rhoFacC, deepFac2F are all 1 in
+// the reference (free_surface.py:121-125); the products with them are exact and are left out.
+//
+// Layout: 3-D fields [batch][T][Nr][ny][nx], 2-D per-instance fields [batch][T][ny][nx], grid fields [T][ny][nx]
+// shared by the batch (padded, the reference layout). One thread per padded point of an instance (blockIdx.y);
+// the level loops stream Nr planes with coalesced rows. All are HBM-bound.
+
+#include <cuda_runtime.h>
+
+#include "cg2d_internal.cuh"
+
+namespace cg2d {
+namespace {
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+
+struct Pt {
+  int t, j, i;   // tile; interior coordinates (Fortran index - 1): -OLy <= j < nj + OLy, -OLx <= i < ni + OLx
+};
+__device__ __forceinline__ Pt decode(const TopoDev& tp, int q) {
+  const int plane = tp.npy * tp.npx;
+  Pt p;
+  p.t = q / plane;
+  const int rem = q - p.t * plane;
+  const int jp = rem / tp.npx;
+  p.j = jp - tp.OLy;
+  p.i = rem - jp * tp.npx - tp.OLx;
+  return p;
+}
+__device__ __forceinline__ bool interior(const TopoDev& tp, const Pt& p) {
+  return p.j >= 0 && p.j < tp.nj && p.i >= 0 && p.i < tp.ni;
+}
+
+#define FOR_Q(tp)                                                                          \
+  const int pe_ = (tp).T * (tp).npy * (tp).npx;                                            \
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pe_; q += gridDim.x * blockDim.x)
+
+// aW2d, aS2d on j, i = 1..sNy+1, 1..sNx+1 (0 elsewhere): sum over k = 1..Nr in order of
+// ((dyG drF(k)) hFacW(k)) recip_dxC, then times cg2dNorm, implicSurfPress, implicDiv2DFlow (:41-47)
+__global__ void k_update_faces(TopoDev tp, int Nr, const double* hFacW, const double* hFacS, const double* drF,
+                               const double* dyG, const double* dxG, const double* rdxC, const double* rdyC,
+                               double norm, const double* norm_arr, double isp, double idf, double* aW2d,
+                               double* aS2d) {
+  const int in = blockIdx.y;
+  const int plane = tp.npy * tp.npx;
+  const long long o2 = (long long)in * tp.T * plane;
+  FOR_Q(tp) {
+    const Pt p = decode(tp, q);
+    double w = 0.0, s = 0.0;
+    if (p.j >= 0 && p.j <= tp.nj && p.i >= 0 && p.i <= tp.ni) {
+      const long long b3 = ((long long)in * tp.T + p.t) * Nr * plane + (q - p.t * plane);
+      const double dy = dyG[q], dx = dxG[q], rx = rdxC[q], ry = rdyC[q];
+      for (int k = 0; k < Nr; ++k) {
+        const double d = drF[k];
+        w = add(w, mul(mul(mul(dy, d), hFacW[b3 + (long long)k * plane]), rx));
+        s = add(s, mul(mul(mul(dx, d), hFacS[b3 + (long long)k * plane]), ry));
+      }
+      const double nrm = norm_arr ? norm_arr[in] : norm;
+      w = mul(mul(mul(w, nrm), isp), idf);
+      s = mul(mul(mul(s, nrm), isp), idf);
+    }
+    aW2d[o2 + q] = w;
+    aS2d[o2 + q] = s;
+  }
+}
+
+struct DiagArgs {
+  const double *aW2d, *aS2d, *recip_Bo, *rA;
+  double fn;      // freeSurfFac cg2dNorm (per instance when norm_arr is given)
+  const double* norm_arr;
+  double fsf, dTm, dTfs;
+};
+
+// aC2d at padded point q of instance in, as the exchange leaves it (:49-53): at an interior point
+// -(aW2d + aW2d(i+1) + aS2d + aS2d(j+1) + freeSurfFac cg2dNorm recip_Bo rA / deltaTMom / deltaTFreeSurf); at a halo
+// point the value at its exch2 source, or 0 where the map writes nothing
+__device__ double aC_at(const TopoDev& tp, const DiagArgs& A, int in, int q) {
+  Pt p = decode(tp, q);
+  if (!interior(tp, p)) {
+    if (tp.map_comp[q] != 1) return 0.0;
+    q = tp.map_src[q];
+    p = decode(tp, q);
+    if (!interior(tp, p)) return 0.0;
+  }
+  const long long o = (long long)in * tp.T * tp.npy * tp.npx;
+  const double f = A.norm_arr ? mul(A.fsf, A.norm_arr[in]) : A.fn;
+  const double sum = add(add(add(A.aW2d[o + q], A.aW2d[o + q + 1]), A.aS2d[o + q]), A.aS2d[o + q + tp.npx]);
+  const double ex = dvd(dvd(mul(mul(f, A.recip_Bo[q]), A.rA[q]), A.dTm), A.dTfs);
+  return -add(sum, ex);
+}
+
+// aC2d on every padded point; pW, pS, pC on j, i = 1..sNy+1, 1..sNx+1 (:55-65): pC = 1/a (1 where a = 0),
+// pW = -aW2d / (cg2dpcOffDFac (a + aC2d(i-1)))^2 (0 where the sum is 0), pS likewise with aC2d(j-1)
+__global__ void k_update_diag(TopoDev tp, DiagArgs A, double offd, double* aC2d, double* pW, double* pS,
+                              double* pC) {
+  const int in = blockIdx.y;
+  const long long o = (long long)in * tp.T * tp.npy * tp.npx;
+  FOR_Q(tp) {
+    const Pt p = decode(tp, q);
+    const double a = aC_at(tp, A, in, q);
+    aC2d[o + q] = a;
+    if (p.j >= 0 && p.j <= tp.nj && p.i >= 0 && p.i <= tp.ni) {
+      pC[o + q] = a == 0.0 ? 1.0 : dvd(1.0, a);
+      const double tw = add(a, aC_at(tp, A, in, q - 1));
+      const double ts = add(a, aC_at(tp, A, in, q - tp.npx));
+      const double cw = mul(offd, tw), cs = mul(offd, ts);
+      pW[o + q] = tw == 0.0 ? 0.0 : dvd(-A.aW2d[o + q], mul(cw, cw));
+      pS[o + q] = ts == 0.0 ? 0.0 : dvd(-A.aS2d[o + q], mul(cs, cs));
+    }
+  }
+}
+
+struct RhsArgs {
+  const double *gU, *gV, *hFacW, *hFacS, *EmPmR, *etaN, *etaH;   // per instance
+  const double *drF, *dyG, *dxG, *rA, *maskInC, *Bo_surf;         // shared
+  double tmpFac, fsf, dTm, dTfs;
+  int fresh_water, Nr;
+};
+
+// cg2d_x = Bo_surf etaN everywhere (:76); cg2d_b on the interior (:77-106), 0 on halos
+__global__ void k_rhs(TopoDev tp, RhsArgs A, double* cg2d_b, double* cg2d_x) {
+  const int in = blockIdx.y;
+  const int plane = tp.npy * tp.npx;
+  const long long o = (long long)in * tp.T * plane;
+  FOR_Q(tp) {
+    const Pt p = decode(tp, q);
+    cg2d_x[o + q] = mul(A.Bo_surf[q], A.etaN[o + q]);
+    double b = 0.0;
+    if (interior(tp, p)) {
+      if (A.fresh_water) b = mul(dvd(mul(mul(A.tmpFac, A.rA[q]), A.EmPmR[o + q]), A.dTm), A.maskInC[q]);
+      const long long b3 = ((long long)in * tp.T + p.t) * A.Nr * plane + (q - p.t * plane);
+      const double dyc = A.dyG[q], dye = A.dyG[q + 1], dxc = A.dxG[q], dxn = A.dxG[q + tp.npx];
+      for (int k = A.Nr - 1; k >= 0; --k) {                                     // :95-101, k = Nr..1
+        const long long c = b3 + (long long)k * plane;
+        const double d = A.drF[k];
+        const double pu0 = dvd(mul(mul(mul(dyc, d), A.hFacW[c]), A.gU[c]), A.dTm);             // :90, :92
+        const double pu1 = dvd(mul(mul(mul(dye, d), A.hFacW[c + 1]), A.gU[c + 1]), A.dTm);
+        b = sub(add(b, pu1), pu0);                                                                // :97
+        const double pv0 = dvd(mul(mul(mul(dxc, d), A.hFacS[c]), A.gV[c]), A.dTm);             // :91, :93
+        const double pv1 = dvd(mul(mul(mul(dxn, d), A.hFacS[c + tp.npx]), A.gV[c + tp.npx]), A.dTm);
+        b = sub(add(b, pv1), pv0);                                                                // :98
+      }
+      b = sub(b, mul(dvd(dvd(mul(A.fsf, A.rA[q]), A.dTm), A.dTfs), A.etaH[o + q]));          // :103-105
+    }
+    cg2d_b[o + q] = b;
+  }
+}
+
+// etaN = recip_Bo x with x the solution on the interior and, on halos, its exchanged value, or the first guess
+// where the map writes nothing (:116-121)
+__global__ void k_post(TopoDev tp, const double* x, const double* cg2d_x, const double* recip_Bo, double* etaN) {
+  const int in = blockIdx.y;
+  const long long o = (long long)in * tp.T * tp.npy * tp.npx;
+  FOR_Q(tp) {
+    const Pt p = decode(tp, q);
+    double v;
+    if (interior(tp, p)) {
+      v = x[o + q];
+    } else if (tp.map_comp[q] == 1) {
+      const int s = tp.map_src[q];
+      v = interior(tp, decode(tp, s)) ? x[o + s] : cg2d_x[o + s];
+    } else {
+      v = cg2d_x[o + q];
+    }
+    etaN[o + q] = mul(recip_Bo[q], v);
+  }
+}
+
+dim3 grid_of(const TopoDev& tp, int batch) {
+  const int pe = tp.T * tp.npy * tp.npx;
+  return dim3((unsigned)((pe + 255) / 256), (unsigned)batch);
+}
+
+}  // namespace
+
+cudaError_t pressure_update(const TopoDev& tp, const UpdateArgs& U, cudaStream_t st) {
+  if (U.batch < 1 || U.batch > 65535 || U.Nr < 1) return cudaErrorInvalidValue;
+  const dim3 g = grid_of(tp, U.batch);
+  k_update_faces<<<g, 256, 0, st>>>(tp, U.Nr, U.hFacW, U.hFacS, U.drF, U.dyG, U.dxG, U.recip_dxC, U.recip_dyC,
+                                    U.norm, U.norm_arr, U.implicSurfPress, U.implicDiv2DFlow, U.aW2d, U.aS2d);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  DiagArgs D;
+  D.aW2d = U.aW2d;
+  D.aS2d = U.aS2d;
+  D.recip_Bo = U.recip_Bo;
+  D.rA = U.rA;
+  D.fsf = U.freeSurfFac;
+  D.norm_arr = U.norm_arr;
+  D.fn = U.norm_arr ? 0.0 : U.freeSurfFac * U.norm;   // the scalar product the reference forms once (:51)
+  D.dTm = U.deltaTMom;
+  D.dTfs = U.deltaTFreeSurf;
+  k_update_diag<<<g, 256, 0, st>>>(tp, D, U.offd, U.aC2d, U.pW, U.pS, U.pC);
+  return cudaGetLastError();
+}
+
+cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st) {
+  if (R.batch < 1 || R.batch > 65535 || R.Nr < 1) return cudaErrorInvalidValue;
+  RhsArgs A;
+  A.gU = R.gU; A.gV = R.gV; A.hFacW = R.hFacW; A.hFacS = R.hFacS;
+  A.EmPmR = R.EmPmR; A.etaN = R.etaN; A.etaH = R.etaH;
+  A.drF = R.drF; A.dyG = R.dyG; A.dxG = R.dxG; A.rA = R.rA; A.maskInC = R.maskInC; A.Bo_surf = R.Bo_surf;
+  A.tmpFac = R.freeSurfFac * R.mass2rUnit * R.implicDiv2DFlow;     // :79, formed once as the reference does
+  A.fsf = R.freeSurfFac;
+  A.dTm = R.deltaTMom;
+  A.dTfs = R.deltaTFreeSurf;
+  A.fresh_water = R.useRealFreshWaterFlux;
+  A.Nr = R.Nr;
+  k_rhs<<<grid_of(tp, R.batch), 256, 0, st>>>(tp, A, R.cg2d_b, R.cg2d_x);
+  return cudaGetLastError();
+}
+
+cudaError_t pressure_post(const TopoDev& tp, int batch, const double* x, const double* cg2d_x,
+                          const double* recip_Bo, double* etaN, cudaStream_t st) {
+  if (batch < 1 || batch > 65535) return cudaErrorInvalidValue;
+  k_post<<<grid_of(tp, batch), 256, 0, st>>>(tp, x, cg2d_x, recip_Bo, etaN);
+  return cudaGetLastError();
+}
+
+}  // namespace cg2d
