@@ -59,11 +59,16 @@ __global__ void k_update_faces(TopoDev tp, int Nr, const double* hFacW, const do
     double w = 0.0, s = 0.0;
     if (p.j >= 0 && p.j <= tp.nj && p.i >= 0 && p.i <= tp.ni) {
       const long long b3 = ((long long)in * tp.T + p.t) * Nr * plane + (q - p.t * plane);
+      const double* __restrict__ hw = hFacW + b3;
+      const double* __restrict__ hs = hFacS + b3;
       const double dy = dyG[q], dx = dxG[q], rx = rdxC[q], ry = rdyC[q];
+      // unrolled so that several levels' loads are in flight while the ordered sums proceed
+#pragma unroll 5
       for (int k = 0; k < Nr; ++k) {
-        const double d = drF[k];
-        w = add(w, mul(mul(mul(dy, d), hFacW[b3 + (long long)k * plane]), rx));
-        s = add(s, mul(mul(mul(dx, d), hFacS[b3 + (long long)k * plane]), ry));
+        const double d = __ldg(drF + k);
+        const double hwk = __ldg(hw + (long long)k * plane), hsk = __ldg(hs + (long long)k * plane);
+        w = add(w, mul(mul(mul(dy, d), hwk), rx));
+        s = add(s, mul(mul(mul(dx, d), hsk), ry));
       }
       const double nrm = norm_arr ? norm_arr[in] : norm;
       w = mul(mul(mul(w, nrm), isp), idf);
@@ -139,15 +144,24 @@ __global__ void k_rhs(TopoDev tp, RhsArgs A, double* cg2d_b, double* cg2d_x) {
     if (interior(tp, p)) {
       if (A.fresh_water) b = mul(dvd(mul(mul(A.tmpFac, A.rA[q]), A.EmPmR[o + q]), A.dTm), A.maskInC[q]);
       const long long b3 = ((long long)in * tp.T + p.t) * A.Nr * plane + (q - p.t * plane);
-      const double dyc = A.dyG[q], dye = A.dyG[q + 1], dxc = A.dxG[q], dxn = A.dxG[q + tp.npx];
+      const double* __restrict__ hw = A.hFacW + b3;
+      const double* __restrict__ hs = A.hFacS + b3;
+      const double* __restrict__ gu = A.gU + b3;
+      const double* __restrict__ gv = A.gV + b3;
+      const int n = tp.npx;
+      const double dyc = A.dyG[q], dye = A.dyG[q + 1], dxc = A.dxG[q], dxn = A.dxG[q + n], dTm = A.dTm;
+      // unrolled so that several levels' loads are in flight while the ordered sum proceeds
+#pragma unroll 4
       for (int k = A.Nr - 1; k >= 0; --k) {                                     // :95-101, k = Nr..1
-        const long long c = b3 + (long long)k * plane;
-        const double d = A.drF[k];
-        const double pu0 = dvd(mul(mul(mul(dyc, d), A.hFacW[c]), A.gU[c]), A.dTm);             // :90, :92
-        const double pu1 = dvd(mul(mul(mul(dye, d), A.hFacW[c + 1]), A.gU[c + 1]), A.dTm);
+        const long long c = (long long)k * plane;
+        const double d = __ldg(A.drF + k);
+        const double hw0 = __ldg(hw + c), hw1 = __ldg(hw + c + 1), u0 = __ldg(gu + c), u1 = __ldg(gu + c + 1);
+        const double hs0 = __ldg(hs + c), hs1 = __ldg(hs + c + n), v0 = __ldg(gv + c), v1 = __ldg(gv + c + n);
+        const double pu0 = dvd(mul(mul(mul(dyc, d), hw0), u0), dTm);                                // :90, :92
+        const double pu1 = dvd(mul(mul(mul(dye, d), hw1), u1), dTm);
         b = sub(add(b, pu1), pu0);                                                                // :97
-        const double pv0 = dvd(mul(mul(mul(dxc, d), A.hFacS[c]), A.gV[c]), A.dTm);             // :91, :93
-        const double pv1 = dvd(mul(mul(mul(dxn, d), A.hFacS[c + tp.npx]), A.gV[c + tp.npx]), A.dTm);
+        const double pv0 = dvd(mul(mul(mul(dxc, d), hs0), v0), dTm);                                // :91, :93
+        const double pv1 = dvd(mul(mul(mul(dxn, d), hs1), v1), dTm);
         b = sub(add(b, pv1), pv0);                                                                // :98
       }
       b = sub(b, mul(dvd(dvd(mul(A.fsf, A.rA[q]), A.dTm), A.dTfs), A.etaH[o + q]));          // :103-105

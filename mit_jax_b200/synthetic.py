@@ -226,6 +226,7 @@ class LLCSynthetic:
             aW = aW + (dyG[:, J, I] * drF[k] * hW[:, k][:, J, I]) * rdxC[:, J, I]
             aS = aS + (dxG[:, J, I] * drF[k] * hS[:, k][:, J, I]) * rdyC[:, J, I]
         my = max(np.abs(aW).max(), np.abs(aS).max())
+        hW, hS, gU, gV = (np.ascontiguousarray(a) for a in (hW, hS, gU, gV))   # [T, Nr, ny, nx] in C order
         return dict(
             Nr=Nr, drF=drF, hFacW=hW, hFacS=hS, dyG=dyG, dxG=dxG, recip_dxC=rdxC, recip_dyC=rdyC, rA=rA,
             maskInC=inner(ocean), Bo_surf=Bo, recip_Bo=recip_Bo, gU=gU, gV=gV,
