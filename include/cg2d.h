@@ -155,6 +155,36 @@ cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2d
                              const cg2d_params_t* params,
                              void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
 
+/* cg2d_solve_f64 in mixed precision (FP32 vectors and matvec, FP64 dot products, solution and residual
+ * replacement; the params' precision field is ignored). Same arguments; the workspace is sized by
+ * cg2d_workspace_size with precision CG2D_PREC_MIXED. */
+cg2d_status_t cg2d_solve_mixed(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                               const double* aW2d, const double* aS2d, const double* aC2d,
+                               const double* pW, const double* pS, const double* pC,
+                               const double* cg2d_b, const double* cg2d_x,
+                               double tolerance, int max_iters,
+                               double* x_out, double* x_fortran, cg2d_diag_t* diag,
+                               const cg2d_params_t* params,
+                               void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
+
+/* The adjoint of cg2d_solve (_cg2d_implicit_jvp, cg2d.py:318-348, transposed) for J = <x_bar, x>:
+ * lam = A^-1 x_bar by a tight CG from a zero first guess (adj_tolerance, adj_max_iters; the reference's
+ * tight_transpose, cg2d.py:333-344), which is the cotangent of cg2d_b; with coeff_grad = 1 also the coefficient
+ * cotangents gW, gS, gC as edge products of lam and the forward solution x (cg2d_edge_products); with
+ * coeff_grad = 0 the operator is passive (the reference's ECCO mode, stop_coeff_grad, cg2d.py:370-371) and gW, gS,
+ * gC (nullable) are zeroed. x: the forward solution (interior; its halos are ignored). diag: the tight solve's.
+ * The workspace is cg2d_adjoint_ecco_workspace_size bytes (the solver's, plus the zero first guess). */
+size_t cg2d_adjoint_ecco_workspace_size(const cg2d_topology_t* topo, int batch, int adj_max_iters,
+                                        const cg2d_params_t* params);
+cg2d_status_t cg2d_adjoint_ecco(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                const double* cg2dNorm_per_instance,
+                                const double* aW2d, const double* aS2d, const double* aC2d,
+                                const double* pW, const double* pS, const double* pC,
+                                const double* x, const double* x_bar, double adj_tolerance, int adj_max_iters,
+                                int coeff_grad, double* lam, double* gW, double* gS, double* gC,
+                                cg2d_diag_t* diag, const cg2d_params_t* params,
+                                void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
+
 /* Exact-mode adjoint: the cotangents of x_out = cg2d_solve_f64(...) (its interior) with respect to cg2d_b and to
  * the six coefficient arrays, for J = <x_bar, x_out>, by reverse mode through the CG iterations that the forward
  * took (each instance's numIters, read from fwd_diag, the diag of the forward solve). The "exact mode" of the

@@ -451,6 +451,79 @@ cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2d
   return cg2d_solve_groups(&g, 1, params, workspace, workspace_bytes, stream);
 }
 
+cg2d_status_t cg2d_solve_mixed(const cg2d_topology_t* topo, int batch, double cg2dNorm, const double* aW2d,
+                               const double* aS2d, const double* aC2d, const double* pW, const double* pS,
+                               const double* pC, const double* cg2d_b, const double* cg2d_x, double tolerance,
+                               int max_iters, double* x_out, double* x_fortran, cg2d_diag_t* diag,
+                               const cg2d_params_t* params, void* workspace, size_t workspace_bytes,
+                               cg2d_stream_t stream) {
+  cg2d_params_t p;
+  if (params) p = *params; else cg2d_default_params(&p);
+  p.precision = CG2D_PREC_MIXED;
+  return cg2d_solve_f64(topo, batch, cg2dNorm, aW2d, aS2d, aC2d, pW, pS, pC, cg2d_b, cg2d_x, tolerance, max_iters,
+                        x_out, x_fortran, diag, &p, workspace, workspace_bytes, stream);
+}
+
+namespace {
+// one uniform group of `batch` single right-hand-side solves (the pointers are filled by the caller)
+cg2d_group_t one_group(const cg2d_topology_t* topo, int batch, double tol, int max_iters) {
+  cg2d_group_t g;
+  std::memset(&g, 0, sizeof(g));
+  g.topo = topo;
+  g.count = batch;
+  g.nrhs = 1;
+  g.tolerance[0] = tol;
+  g.max_iters[0] = max_iters;
+  return g;
+}
+size_t round256(size_t n) { return (n + 255) & ~size_t(255); }
+}  // namespace
+
+size_t cg2d_adjoint_ecco_workspace_size(const cg2d_topology_t* topo, int batch, int adj_max_iters,
+                                        const cg2d_params_t* params) {
+  if (!topo || batch < 1 || adj_max_iters < 0) return 0;
+  cg2d_group_t g = one_group(topo, batch, 0.0, adj_max_iters);
+  const size_t solver = cg2d_workspace_size(&g, 1, params);
+  if (solver == 0) return 0;
+  const TopoDev tp = topo_dev(topo);
+  return round256(solver) + sizeof(double) * (size_t)batch * tp.T * tp.npy * tp.npx;
+}
+
+cg2d_status_t cg2d_adjoint_ecco(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                                const double* cg2dNorm_per_instance, const double* aW2d, const double* aS2d,
+                                const double* aC2d, const double* pW, const double* pS, const double* pC,
+                                const double* x, const double* x_bar, double adj_tolerance, int adj_max_iters,
+                                int coeff_grad, double* lam, double* gW, double* gS, double* gC, cg2d_diag_t* diag,
+                                const cg2d_params_t* params, void* workspace, size_t workspace_bytes,
+                                cg2d_stream_t stream) {
+  if (!topo || batch < 1 || !x_bar || !lam || !diag || !workspace || (coeff_grad && (!x || !gW || !gS || !gC)) ||
+      coeff_grad < 0 || coeff_grad > 1)
+    return CG2D_BAD_ARG;
+  const size_t need = cg2d_adjoint_ecco_workspace_size(topo, batch, adj_max_iters, params);
+  if (need == 0) return CG2D_BAD_ARG;
+  if (workspace_bytes < need) return CG2D_WORKSPACE_TOO_SMALL;
+  cg2d_group_t g = one_group(topo, batch, adj_tolerance, adj_max_iters);
+  const size_t solver = round256(cg2d_workspace_size(&g, 1, params));
+  const TopoDev tp = topo_dev(topo);
+  const size_t vb = sizeof(double) * (size_t)batch * tp.T * tp.npy * tp.npx;
+  double* zero = reinterpret_cast<double*>(static_cast<char*>(workspace) + solver);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(zero, 0, vb, st) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  g.aW2d = aW2d; g.aS2d = aS2d; g.aC2d = aC2d; g.pW = pW; g.pS = pS; g.pC = pC;
+  g.cg2dNorm = cg2dNorm;
+  g.cg2dNorm_per_instance = cg2dNorm_per_instance;
+  g.b[0] = x_bar;
+  g.x0[0] = zero;
+  g.x_out[0] = lam;
+  g.diag[0] = diag;
+  cg2d_status_t s = cg2d_solve_groups(&g, 1, params, workspace, solver, stream);
+  if (s != CG2D_OK) return s;
+  if (coeff_grad) return cg2d_edge_products(topo, batch, cg2dNorm, cg2dNorm_per_instance, lam, x, gW, gS, gC, stream);
+  for (double* gg : {gW, gS, gC})
+    if (gg && cudaMemsetAsync(gg, 0, vb, st) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
 size_t cg2d_adjoint_exact_workspace_size(const cg2d_topology_t* topo, int batch, int max_iters,
                                          int checkpoint_every) {
   if (!topo || batch < 1 || max_iters < 0 || checkpoint_every < 0) return 0;
