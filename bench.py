@@ -641,6 +641,31 @@ def pressure_bytes(B, Nr, n=90, T=13, npad=98):
     return upd, rhs, post
 
 
+def _cpu_pressure(syn, f, a):
+    """The oracle port on one member, one host thread: update_cg2d, cg2d_rhs, the FP64 solve (ROWBLOCK sums, as
+    the GPU arm) and the post-solve step."""
+    from oracle import cg2d_oracle as O
+    from oracle import pressure_oracle as P
+    L, tmap = syn.L, syn.topo.maps["T"]
+    t0 = time.perf_counter()
+    z = np.zeros(L.shape2d)
+    ops = P.update_cg2d(L, tmap, hFacW=f["hFacW"], hFacS=f["hFacS"], pW=z, pS=z, pC=z,
+                        **{k: f[k] for k in ("drF", "dyG", "dxG", "recip_dxC", "recip_dyC", "rA", "recip_Bo",
+                                             "cg2dNorm", "cg2dpcOffDFac", "implicSurfPress", "implicDiv2DFlow",
+                                             "freeSurfFac", "deltaTMom", "deltaTFreeSurf")})
+    b, x0 = P.cg2d_rhs(L, **{k: f[k] for k in ("gU", "gV", "hFacW", "hFacS", "EmPmR", "etaN", "etaH", "Bo_surf",
+                                               "drF", "dyG", "dxG", "rA", "maskInC", "freeSurfFac", "mass2rUnit",
+                                               "implicDiv2DFlow", "deltaTMom", "deltaTFreeSurf",
+                                               "useRealFreshWaterFlux")})
+    x, d = O.cg2d_fortran(L, tmap, ops, b, x0, cg2dNorm=f["cg2dNorm"], tolerance=a.tol, max_iters=a.maxit,
+                          sum_order="rowblock")
+    P.solve_for_pressure_post(L, tmap, np.where(O.interior_mask(L), x, 0.0), x0, f["recip_Bo"])
+    secs = time.perf_counter() - t0
+    return {"value": 1.0 / secs, "unit": "instances/s", "cores": 1, "kind": "port",
+            "sample": f"member 0 ({d['numIters']} iterations): the oracle port of update_cg2d, cg2d_rhs, the FP64 "
+                      f"ROWBLOCK solve and the post-solve step on one host thread, {secs:.2f} s"}
+
+
 def run_pressure(a):
     import torch
 
@@ -667,6 +692,9 @@ def run_pressure(a):
                           useRealFreshWaterFlux=True, Nr=a.nr)
     st = {k: torch.as_tensor(np.stack([f[k] for f in fs])).to(dev)
           for k in ("hFacW", "hFacS", "gU", "gV", "EmPmR", "etaN", "etaH")}
+    cpu = None
+    if not a.no_cpu:
+        cpu = _cpu_pressure(syn, f0, a)
     del distinct, fs
     norms = torch.full((a.batch,), float(f0["cg2dNorm"]), dtype=torch.float64, device=dev)
     cp = cg.Cg2dParams(cg2dMaxIters=a.maxit, cg2dTolerance=a.tol, cg2dNorm=norms, sum_order="rowblock")
@@ -725,7 +753,7 @@ def run_pressure(a):
         "steps_ms": {"update_cg2d": upd_ms, "cg2d_rhs": rhs_ms, "cg2d_solve": solve_ms, "post": post_ms},
         "steps_gbs": {"update_cg2d": gbs(upd_b, upd_ms), "cg2d_rhs": gbs(rhs_b, rhs_ms),
                       "cg2d_solve": gbs(solve_alg, solve_ms), "post": gbs(post_b, post_ms)},
-        "cpu_baseline": None, "e2e": None,
+        "cpu_baseline": cpu, "e2e": None,
         "gpu_launches": a.steps * 6,
         "clocks": clocks,
         "iterations": {"mean": statistics.mean(r["numIters"] for r in recs), "not_ok":
