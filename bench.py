@@ -444,10 +444,10 @@ EXACT_METRIC = "CG2D exact-mode adjoint solves/s (FP64 forward + reverse through
 
 
 def exact_config(a):
-    return {"workload": f"batch {a.batch} LLC90 exact-mode adjoint: FP64 ROWBLOCK forward to {a.tol:g}, reverse "
-                        f"through every iteration, r and s_prev checkpointed every {a.checkpoint} iterations, "
-                        f"segments recomputed with the recorded alpha and beta; gradients of <w, x> w.r.t. b and "
-                        f"all six coefficient arrays",
+    return {"workload": f"batch {a.batch} LLC90 exact-mode adjoint: FP64 ROWBLOCK forward to {a.tol:g} storing r and "
+                        f"s_prev every {a.checkpoint} iterations, reverse through every iteration with segments "
+                        f"recomputed from the solve's alpha and beta; gradients of <w, x> w.r.t. b and all six "
+                        f"coefficient arrays",
             "batch_per_gpu": a.batch, "tolerance": a.tol, "max_iters": a.maxit, "checkpoint_every": a.checkpoint,
             "grid": "LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)",
             "parallelism": "1 GPU"}
@@ -527,7 +527,7 @@ def run_exact(a):
     clocks = clk.summary()
     ms = e0.elapsed_time(e1) / a.steps
     peak_alloc = torch.cuda.max_memory_allocated(dev)
-    ws_bytes = capi.lib().cg2d_adjoint_exact_workspace_size(ex.handle(dev), a.batch, a.maxit, a.checkpoint)
+    ws_bytes = capi.lib().cg2d_solve_exact_workspace_size(ex.handle(dev), a.batch, a.maxit, 8, a.checkpoint)
     iters = [r["numIters"] for r in d]
     bad = [r for r in d if r["status"] != "ok"]
     alg = exact_algorithmic_bytes(iters, a.checkpoint)

@@ -208,6 +208,23 @@ cg2d_status_t cg2d_adjoint_exact(const cg2d_topology_t* topo, int batch, double 
                                  double* gpW, double* gpS, double* gpC, double* x_check,
                                  void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
 
+/* The FP64 ROWBLOCK solve and the exact-mode adjoint in one call: the forward solve (x_out, diag, as
+ * cg2d_solve_f64) stores the checkpoints and keeps its sums, and the reverse sweep (as cg2d_adjoint_exact,
+ * outputs b_bar, gW/gS/gC, gpW/gpS/gpC) starts from them, with no second forward pass. The gradients equal
+ * cg2d_adjoint_exact's on the same inputs bit for bit. Synchronises the stream once (the iteration counts).
+ * Workspace: cg2d_solve_exact_workspace_size bytes, 256-byte aligned. */
+size_t cg2d_solve_exact_workspace_size(const cg2d_topology_t* topo, int batch, int max_iters, int rows_per_block,
+                                       int checkpoint_every);
+cg2d_status_t cg2d_solve_exact(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                               const double* cg2dNorm_per_instance,
+                               const double* aW2d, const double* aS2d, const double* aC2d,
+                               const double* pW, const double* pS, const double* pC,
+                               const double* cg2d_b, const double* cg2d_x, double tolerance, int max_iters,
+                               const double* x_bar, int rows_per_block, int checkpoint_every,
+                               double* x_out, cg2d_diag_t* diag, double* b_bar, double* gW, double* gS, double* gC,
+                               double* gpW, double* gpS, double* gpC,
+                               void* workspace, size_t workspace_bytes, cg2d_stream_t stream);
+
 /* cg2d_solve_f64 without a caller workspace and without any allocation (no counterpart in the reference, whose
  * JAX arrays are allocated by XLA). For callers that cannot allocate device memory where they solve: a step
  * inside a framework that owns the whole device pool and hands a custom call only its operands, or code that

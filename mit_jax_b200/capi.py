@@ -35,7 +35,8 @@ EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_param
             "cg2d_edge_products", "cg2d_exchange_scalar", "cg2d_status_string", "cg2d_workspace_profile",
             "cg2d_solve_f64_noalloc", "cg2d_adjoint_exact", "cg2d_adjoint_exact_workspace_size",
             "cg2d_update_operator", "cg2d_pressure_rhs", "cg2d_pressure_post", "cg2d_solve_mixed",
-            "cg2d_adjoint_ecco_workspace_size", "cg2d_adjoint_ecco")
+            "cg2d_adjoint_ecco_workspace_size", "cg2d_adjoint_ecco", "cg2d_solve_exact_workspace_size",
+            "cg2d_solve_exact")
 
 
 class Params(ctypes.Structure):
@@ -124,6 +125,10 @@ def lib():
     L.cg2d_adjoint_ecco.argtypes = [_P, i, d, _P] + [_P] * 8 + [d, i, i] + [_P] * 5 + [ctypes.POINTER(Params), _P,
                                                                                      ctypes.c_size_t, _P]
     L.cg2d_adjoint_ecco.restype = i
+    L.cg2d_solve_exact_workspace_size.argtypes = [_P, i, i, i, i]
+    L.cg2d_solve_exact_workspace_size.restype = ctypes.c_size_t
+    L.cg2d_solve_exact.argtypes = [_P, i, d, _P] + [_P] * 8 + [d, i, _P, i, i] + [_P] * 9 + [_P, ctypes.c_size_t, _P]
+    L.cg2d_solve_exact.restype = i
     L.cg2d_update_operator.argtypes = [_P, i, ctypes.POINTER(FreeSurf), d, _P, d] + [_P] * 15 + [_P]
     L.cg2d_update_operator.restype = i
     L.cg2d_pressure_rhs.argtypes = [_P, i, ctypes.POINTER(FreeSurf)] + [_P] * 15 + [_P]

@@ -367,13 +367,17 @@ def edge_products(ex, lam, x, cg2dNorm):
 
 
 def exact_adjoint(ex, ops, cg2d_b, cg2d_x, x_bar, *, cg2dNorm, tolerance, max_iters, rows_per_block=8,
-                  checkpoint_every=30, x_check=False):
-    """Exact-mode adjoint (cg2d_adjoint_exact): solve A x = b in FP64 (ROWBLOCK sums), then reverse through the
-    iterations that solve took. Returns (x, diag records, grads) with x the solution (interior, 0 on halos) and grads
-    a dict of the cotangents of J = <x_bar, x> with respect to cg2d_b ("b") and to the six coefficient arrays
-    (names of OPS); x0 is constant. checkpoint_every: iterations between checkpoints (0 = keep all). x_check=True
-    adds the recording forward's solution ("x_check"), which equals x bit for bit. Arrays [batch, T, ny, nx] or
-    [T, ny, nx]; cg2dNorm a float or a [batch] tensor."""
+                  checkpoint_every=30, x_check=False, one_pass=True):
+    """Exact-mode adjoint: solve A x = b in FP64 (ROWBLOCK sums), then reverse through the iterations that solve
+    took. Returns (x, diag records, grads) with x the solution (interior, 0 on halos) and grads a dict of the
+    cotangents of J = <x_bar, x> with respect to cg2d_b ("b") and to the six coefficient arrays (names of OPS); x0 is
+    constant. checkpoint_every: iterations between checkpoints (0 = one segment). Arrays [batch, T, ny, nx] or
+    [T, ny, nx]; cg2dNorm a float or a [batch] tensor.
+
+    one_pass (default): the solve itself stores the checkpoints and its sums, and the reverse sweep starts from them
+    (cg2d_solve_exact). one_pass=False or x_check=True: the solve, then cg2d_adjoint_exact, whose recording forward
+    repeats the iterations; x_check adds that recording forward's solution ("x_check"), equal to x bit for bit. Both
+    give the same gradients bit for bit."""
     b, back = _dev(cg2d_b)
     dev = b.device
     lead = b.shape[:-3]
@@ -386,6 +390,30 @@ def exact_adjoint(ex, ops, cg2d_b, cg2d_x, x_bar, *, cg2dNorm, tolerance, max_it
     norm = cg2dNorm
     if isinstance(norm, np.ndarray):
         norm = torch.as_tensor(norm)
+    norm_arr = norm.to(dev, torch.float64).contiguous() if isinstance(norm, torch.Tensor) else None
+    nval = 0.0 if norm_arr is not None else float(norm)
+    if one_pass and not x_check:
+        with torch.cuda.device(dev):
+            L = capi.lib()
+            topo = ex.handle(dev)
+            nbytes = L.cg2d_solve_exact_workspace_size(topo, batch, int(max_iters), int(rows_per_block),
+                                                       int(checkpoint_every))
+            if nbytes == 0:
+                raise capi.Cg2dError(capi.CG2D_BAD_ARG, "cg2d_solve_exact_workspace_size")
+            ws = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+            base = ws.data_ptr() + (-ws.data_ptr()) % 256
+            x = torch.empty_like(b)
+            dg = torch.zeros((batch, capi.DIAG_BYTES), dtype=torch.uint8, device=dev)
+            outs = {k: torch.empty_like(b) for k in ("b",) + OPS}
+            capi.check(L.cg2d_solve_exact(topo, batch, nval, _ptr(norm_arr), *(t.data_ptr() for t in ops_t),
+                                          b.data_ptr(), x0.data_ptr(), float(tolerance), int(max_iters),
+                                          xb.data_ptr(), int(rows_per_block), int(checkpoint_every), x.data_ptr(),
+                                          dg.data_ptr(), outs["b"].data_ptr(), *(outs[k].data_ptr() for k in OPS),
+                                          base, nbytes, _stream(dev)), "cg2d_solve_exact")
+        shape = lead + tuple(ex.L.shape2d)
+        grads = {k: back(v.reshape(shape)) for k, v in outs.items()}
+        recs = diag_records(dg)
+        return back(x.reshape(shape)), (recs[0] if not lead else recs), grads
     with torch.cuda.device(dev):
         G = GroupSpec(ex, ops_t, [b], [x0], [tolerance], [max_iters], norm)
         (res,), = solve_groups([G], precision="f64", sum_order="rowblock", rows_per_block=rows_per_block)
@@ -399,8 +427,6 @@ def exact_adjoint(ex, ops, cg2d_b, cg2d_x, x_bar, *, cg2dNorm, tolerance, max_it
         base = ws.data_ptr() + (-ws.data_ptr()) % 256
         outs = {k: torch.empty_like(b) for k in ("b",) + OPS}
         xc = torch.empty_like(b) if x_check else None
-        norm_arr = norm.to(dev, torch.float64).contiguous() if isinstance(norm, torch.Tensor) else None
-        nval = 0.0 if norm_arr is not None else float(norm)
         capi.check(L.cg2d_adjoint_exact(topo, batch, nval, _ptr(norm_arr), *(t.data_ptr() for t in ops_t),
                                         b.data_ptr(), x0.data_ptr(), dg.data_ptr(), xb.data_ptr(), int(max_iters),
                                         int(rows_per_block), int(checkpoint_every), outs["b"].data_ptr(),

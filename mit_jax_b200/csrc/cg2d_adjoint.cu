@@ -466,6 +466,26 @@ __global__ void k_xout(Geo G, const double* x, const double* rn, double* out) {
   POINT(G, in, t, j, i, p);
   out[p] = __ddiv_rn(x[p], rn[in]);
 }
+// alpha, beta, eta, sigma of every iteration from a forward solve's sum history (one group of one right-hand side:
+// solve index = instance): eta_0 = z.r of the first Z pass, eta_k (k >= 1) = z.r of pass X_{k-1}, sigma_k = s.q
+// of pass S_k; beta_k = eta_k / eta_{k-1} (eta_{-1} = 1) and alpha_k = eta_k / sigma_k with the solver's divisions
+__global__ void k_hist_scalars(Geo G, const double* hist, int hist_len, Scal S, const int* K) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= G.batch) return;
+  const double* h = hist + (size_t)in * H_NKIND * hist_len;
+  double eta_prev = 1.0;
+  for (int k = 0; k < K[in]; ++k) {
+    const double eta = k == 0 ? h[(size_t)H_ETAZ * hist_len] : h[(size_t)H_ETAX * hist_len + k];
+    const double sig = h[(size_t)H_SQ * hist_len + k];
+    const long long o = (long long)k * G.batch + in;
+    S.eta[o] = eta;
+    S.beta[o] = __ddiv_rn(eta, eta_prev);
+    S.sig[o] = sig;
+    S.alpha[o] = __ddiv_rn(eta, sig);
+    eta_prev = eta;
+  }
+}
+
 // per-instance rhsNorm from the forward's rhsMax (cg2d.py:225) and cg2dNorm, iteration counts
 __global__ void k_setup(int batch, const cg2d_diag_t* diag, double norm, const double* norm_arr, double* rn,
                         double* nrm, int* K) {
@@ -487,15 +507,28 @@ size_t exact_adjoint_workspace(const TopoDev& tp, int batch, int max_iters, int 
   const size_t rows = (size_t)tp.T * tp.nj;
   size_t b = 0;
   b += vec * 5;                                   // r, s, z, q, x of the recording forward
-  b += vec * 2 * (size_t)std::max(1, nseg);       // checkpoints: r_c, s_{c-1}
+  b += vec * 2 * (size_t)(std::max(1, nseg) + 1); // checkpoints r_c, s_{c-1}; one slot more for a forward that
+                                                  // records at its last iteration
   b += vec * 4 * (size_t)C;                       // a segment's r, z, s, q
   b += vec * 3;                                   // xbar, rbar, sbar
   b += sizeof(double) * batch * 2 * rows;         // row sums
   b += sizeof(double) * ((size_t)4 * std::max(1, max_iters) * batch + 5 * batch);   // scalars, rn, norm
   b += sizeof(int) * batch;
   b += sizeof(int) * 2 * (size_t)tp.T * (tp.nj + tp.ni);   // padded-offset neighbour table
-  b += 256 * (size_t)(31 + 2 * std::max(1, nseg) + 4 * C);   // each buffer starts 256-byte aligned
+  b += 256 * (size_t)(33 + 2 * std::max(1, nseg) + 4 * C);   // each buffer starts 256-byte aligned
   return b;
+}
+
+void exact_checkpoints(const TopoDev& tp, int batch, int max_iters, int checkpoint, void* ws, double** ck_r0,
+                       double** ck_s0, long long* stride) {
+  const size_t vecn = (size_t)tp.T * tp.npy * tp.npx * batch;
+  const size_t vstride = (vecn * sizeof(double) + 255) & ~size_t(255);
+  const int C = checkpoint > 0 ? checkpoint : std::max(1, max_iters);
+  const int nck = std::max(1, (max_iters + C - 1) / C) + 1;
+  char* base = static_cast<char*>(ws) + 5 * vstride;   // after r, s, z, q, x (exact_adjoint's carve)
+  *ck_r0 = reinterpret_cast<double*>(base);
+  *ck_s0 = reinterpret_cast<double*>(base + nck * vstride);
+  *stride = (long long)(vstride / sizeof(double));
 }
 
 cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaStream_t st) {
@@ -505,7 +538,8 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   G.pe = (long long)tp.T * tp.npy * tp.npx;
   G.pts = (long long)tp.T * tp.nj * tp.ni;
   const int Kmax = A.max_iters;
-  const int C = A.checkpoint > 0 ? A.checkpoint : std::max(1, Kmax);
+  if (A.recorded && (A.x_check || !A.hist)) return cudaErrorInvalidValue;
+  const int C = A.checkpoint > 0 ? A.checkpoint : std::max(1, A.recorded ? std::max(A.max_iters_cap, Kmax) : Kmax);
   const int nseg = (Kmax + C - 1) / C;
   const size_t vecn = (size_t)G.pe * A.batch;
   const int rows = tp.T * tp.nj;
@@ -513,8 +547,18 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   auto take = [&](size_t bytes) { char* p = w; w += (bytes + 255) & ~size_t(255); return p; };
   auto vec = [&]() { return reinterpret_cast<double*>(take(vecn * sizeof(double))); };
   double *r = vec(), *s = vec(), *z = vec(), *q = vec(), *x = vec();
-  std::vector<double*> ck_r(std::max(1, nseg)), ck_s(std::max(1, nseg));
-  for (int c = 0; c < std::max(1, nseg); ++c) { ck_r[c] = vec(); ck_s[c] = vec(); }
+  // checkpoint blocks: r_c and s_{c-1} for c = 0 .. cap / C, carved from the capacity (a recording forward stores
+  // into them before the iteration counts are known); exact_checkpoints gives the same addresses
+  const int cap = std::max(A.max_iters_cap, Kmax);
+  const int nck = std::max(1, (cap + C - 1) / C) + 1;
+  const size_t vstride = (vecn * sizeof(double) + 255) & ~size_t(255);
+  char* ckr0 = take(vstride * nck);
+  char* cks0 = take(vstride * nck);
+  std::vector<double*> ck_r(nck), ck_s(nck);
+  for (int c = 0; c < nck; ++c) {
+    ck_r[c] = reinterpret_cast<double*>(ckr0 + c * vstride);
+    ck_s[c] = reinterpret_cast<double*>(cks0 + c * vstride);
+  }
   std::vector<double*> sg_r(C), sg_z(C), sg_s(C), sg_q(C);
   for (int c = 0; c < C; ++c) { sg_r[c] = vec(); sg_z[c] = vec(); sg_s[c] = vec(); sg_q[c] = vec(); }
   double *xbar = vec(), *rbar = vec(), *sbar = vec();
@@ -563,15 +607,25 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   LK();
   k_nbp<<<(2 * tp.T * (tp.nj + tp.ni) + 255) / 256, 256, 0, st>>>(tp, nbp);
   LK();
-  k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
-  LK();
+  if (A.recorded) {
+    // the forward solve stored r_c and s_{c-1} for c >= 1 and kept its sums: r_0 and s_{-1} = 0 here, alpha and
+    // beta rebuilt from the sums with the solver's own divisions
+    CK(cudaMemsetAsync(ck_s[0], 0, vb, st));
+    k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, ck_r[0], x);
+    LK();
+    k_hist_scalars<<<gi, 128, 0, st>>>(G, A.hist, A.hist_len, S, K);
+    LK();
+  } else {
+    k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
+    LK();
+  }
 
   // ---- recording forward: scalars of every iteration, checkpoints of r_k and s_{k-1} every C iterations. r and s
   // alternate between two buffers (a stencil reads its neighbours' old values while every point writes its new
   // one); the second ones borrow the first segment buffers, which the reverse sweep fills later.
   double *rcur = r, *rnext = sg_r[0];
   double *sprev = s, *snew = sg_s[0];
-  for (int k = 0; k <= Kmax; ++k) {
+  for (int k = 0; k <= Kmax && !A.recorded; ++k) {
     const bool ck = k < Kmax && k % C == 0;
     if (k == Kmax && !A.x_check) break;   // the last updates only move x
     k_fa<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rcur, q, sprev, A.x_check ? x : nullptr, rnext, z,

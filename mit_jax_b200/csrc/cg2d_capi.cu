@@ -319,8 +319,19 @@ size_t cg2d_workspace_size(const cg2d_group_t* groups, int ngroups, const cg2d_p
   return L.total;
 }
 
-cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params,
-                                void* workspace, size_t workspace_bytes, cg2d_stream_t stream_) {
+// checkpoint recording for the exact-mode adjoint (see KParams::ck_r), and where the launch keeps its sums
+struct CkRec {
+  double* ck_r;
+  double* ck_s;
+  long long stride;
+  int every;
+  const double** hist;   // out: the launch's sum history [total_rhs][H_NKIND][hist_len]
+  int* hist_len;
+};
+
+static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params,
+                                       void* workspace, size_t workspace_bytes, cg2d_stream_t stream_,
+                                       const CkRec* ck) {
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   cg2d_params_t def;
   if (!params) { cg2d_default_params(&def); params = &def; }
@@ -365,6 +376,16 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
   kp.test_missing = params->test_missing_arrivals;
   kp.unit_deal = params->unit_deal;
   kp.prof = params->profile ? reinterpret_cast<unsigned long long*>(ws + L.prof) : nullptr;
+  if (ck) {
+    if (ngroups != 1 || groups[0].nrhs != 1 || params->precision != CG2D_PREC_F64 || ck->every < 1)
+      return CG2D_BAD_ARG;
+    kp.ck_r = ck->ck_r;
+    kp.ck_s = ck->ck_s;
+    kp.ck_stride = ck->stride;
+    kp.ck_every = ck->every;
+    if (ck->hist) *ck->hist = kp.hist;
+    if (ck->hist_len) *ck->hist_len = kp.hist_len;
+  }
   for (int g = 0; g < ngroups; ++g) {
     const cg2d_topology* tp = groups[g].topo;
     for (int pt = 0; pt < P_NPASS; ++pt)
@@ -426,6 +447,11 @@ cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const c
 
   if (launch_solver(kp, (int)grid, smem, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return CG2D_OK;
+}
+
+cg2d_status_t cg2d_solve_groups(const cg2d_group_t* groups, int ngroups, const cg2d_params_t* params,
+                                void* workspace, size_t workspace_bytes, cg2d_stream_t stream) {
+  return solve_groups_impl(groups, ngroups, params, workspace, workspace_bytes, stream, nullptr);
 }
 
 cg2d_status_t cg2d_solve_f64(const cg2d_topology_t* topo, int batch, double cg2dNorm, const double* aW2d,
@@ -557,9 +583,10 @@ cg2d_status_t cg2d_adjoint_exact(const cg2d_topology_t* topo, int batch, double 
     if (r.numIters < 0 || r.numIters > max_iters) return CG2D_BAD_ARG;
     kmax = r.numIters > kmax ? r.numIters : kmax;
   }
-  ExactArgs a;
+  ExactArgs a{};
   a.batch = batch;
   a.max_iters = kmax;
+  a.max_iters_cap = max_iters;
   a.checkpoint = checkpoint_every;
   a.rows_per_block = rows_per_block;
   a.norm = cg2dNorm;
@@ -568,6 +595,91 @@ cg2d_status_t cg2d_adjoint_exact(const cg2d_topology_t* topo, int batch, double 
   a.b = cg2d_b; a.x0 = cg2d_x; a.xbar = x_bar; a.fwd_diag = fwd_diag;
   a.b_bar = b_bar; a.gW = gW; a.gS = gS; a.gC = gC; a.gpW = gpW; a.gpS = gpS; a.gpC = gpC; a.x_check = x_check;
   if (exact_adjoint(topo_dev(topo), a, workspace, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  return CG2D_OK;
+}
+
+namespace {
+cg2d_params_t exact_params(int rows_per_block) {
+  cg2d_params_t p;
+  cg2d_default_params(&p);
+  p.precision = CG2D_PREC_F64;
+  p.sum_order = CG2D_SUM_ROWBLOCK;
+  p.rows_per_block = rows_per_block;
+  return p;
+}
+}  // namespace
+
+size_t cg2d_solve_exact_workspace_size(const cg2d_topology_t* topo, int batch, int max_iters, int rows_per_block,
+                                       int checkpoint_every) {
+  if (!topo || batch < 1 || max_iters < 0 || checkpoint_every < 0) return 0;
+  const cg2d_params_t p = exact_params(rows_per_block);
+  cg2d_group_t g = one_group(topo, batch, 0.0, max_iters);
+  const size_t solver = cg2d_workspace_size(&g, 1, &p);
+  if (solver == 0) return 0;
+  return round256(exact_adjoint_workspace(topo_dev(topo), batch, max_iters, checkpoint_every)) + solver;
+}
+
+cg2d_status_t cg2d_solve_exact(const cg2d_topology_t* topo, int batch, double cg2dNorm,
+                               const double* cg2dNorm_per_instance, const double* aW2d, const double* aS2d,
+                               const double* aC2d, const double* pW, const double* pS, const double* pC,
+                               const double* cg2d_b, const double* cg2d_x, double tolerance, int max_iters,
+                               const double* x_bar, int rows_per_block, int checkpoint_every, double* x_out,
+                               cg2d_diag_t* diag, double* b_bar, double* gW, double* gS, double* gC, double* gpW,
+                               double* gpS, double* gpC, void* workspace, size_t workspace_bytes,
+                               cg2d_stream_t stream_) {
+  if (!topo || batch < 1 || max_iters < 0 || checkpoint_every < 0 || rows_per_block < 8 || !x_bar || !x_out ||
+      !diag || !b_bar || !gW || !gS || !gC || !gpW || !gpS || !gpC || !workspace)
+    return CG2D_BAD_ARG;
+  const size_t need = cg2d_solve_exact_workspace_size(topo, batch, max_iters, rows_per_block, checkpoint_every);
+  if (need == 0) return CG2D_BAD_ARG;
+  if (workspace_bytes < need) return CG2D_WORKSPACE_TOO_SMALL;
+  if ((reinterpret_cast<uintptr_t>(workspace) % kAlign) != 0) return CG2D_BAD_ARG;
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  const TopoDev tp = topo_dev(topo);
+  // workspace: the adjoint's (its checkpoint blocks receive the forward's r_c, s_{c-1}), then the solver's
+  char* adj = static_cast<char*>(workspace);
+  const size_t adj_bytes = round256(exact_adjoint_workspace(tp, batch, max_iters, checkpoint_every));
+  CkRec ck;
+  exact_checkpoints(tp, batch, max_iters, checkpoint_every, adj, &ck.ck_r, &ck.ck_s, &ck.stride);
+  ck.every = checkpoint_every > 0 ? checkpoint_every : (max_iters > 0 ? max_iters : 1);
+  const double* hist = nullptr;
+  int hist_len = 0;
+  ck.hist = &hist;
+  ck.hist_len = &hist_len;
+  const cg2d_params_t p = exact_params(rows_per_block);
+  cg2d_group_t g = one_group(topo, batch, tolerance, max_iters);
+  g.aW2d = aW2d; g.aS2d = aS2d; g.aC2d = aC2d; g.pW = pW; g.pS = pS; g.pC = pC;
+  g.cg2dNorm = cg2dNorm;
+  g.cg2dNorm_per_instance = cg2dNorm_per_instance;
+  g.b[0] = cg2d_b;
+  g.x0[0] = cg2d_x;
+  g.x_out[0] = x_out;
+  g.diag[0] = diag;
+  cg2d_status_t s = solve_groups_impl(&g, 1, &p, adj + adj_bytes, workspace_bytes - adj_bytes, stream_, &ck);
+  if (s != CG2D_OK) return s;
+  std::vector<cg2d_diag_t> d((size_t)batch);
+  if (cudaMemcpyAsync(d.data(), diag, sizeof(cg2d_diag_t) * batch, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  int kmax = 0;
+  for (const cg2d_diag_t& r : d) {
+    if (r.status == CG2D_BARRIER_TIMEOUT || r.status == CG2D_INTERNAL_ERROR) return (cg2d_status_t)r.status;
+    kmax = r.numIters > kmax ? r.numIters : kmax;
+  }
+  ExactArgs a{};
+  a.batch = batch;
+  a.max_iters = kmax;
+  a.max_iters_cap = max_iters;
+  a.checkpoint = checkpoint_every;
+  a.rows_per_block = rows_per_block;
+  a.recorded = 1;
+  a.hist = hist;
+  a.hist_len = hist_len;
+  a.norm = cg2dNorm;
+  a.norm_arr = cg2dNorm_per_instance;
+  a.aW = aW2d; a.aS = aS2d; a.aC = aC2d; a.pW = pW; a.pS = pS; a.pC = pC;
+  a.b = cg2d_b; a.x0 = cg2d_x; a.xbar = x_bar; a.fwd_diag = diag;
+  a.b_bar = b_bar; a.gW = gW; a.gS = gS; a.gC = gC; a.gpW = gpW; a.gpS = gpS; a.gpC = gpC; a.x_check = nullptr;
+  if (exact_adjoint(tp, a, adj, stream) != cudaSuccess) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   return CG2D_OK;
 }
 

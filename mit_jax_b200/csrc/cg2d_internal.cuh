@@ -148,6 +148,13 @@ struct KParams {
   int unit_deal;            // 0: units dealt round-robin to the CTAs; 1: contiguous runs (cg2d_params_t)
   int test_missing;         // extra arrivals the first grid-wide wait expects (testing the time limit)
   unsigned long long* prof; // nullable: [1 + grid * kProfSlots] phase times (ns) per CTA
+  // FP64, one group of one right-hand side: checkpoints for the exact-mode adjoint (nullable). At every iteration
+  // k with (k + 1) % ck_every == 0 pass X_k stores r_{k+1} into ck_r + ((k + 1) / ck_every) ck_stride and pass S_k
+  // stores s_k into ck_s + ((k + 1) / ck_every) ck_stride, in the reference layout [count][T][ny][nx] (interior)
+  double* ck_r;
+  double* ck_s;
+  long long ck_stride;
+  int ck_every;
   StageLay lay[kMaxGroups][P_NPASS];  // shared-memory image of a chunk, per group and pipelined pass
 };
 
@@ -162,6 +169,12 @@ enum ProfPhase : int { PR_BAR = 0, PR_MBAR = 1, PR_ISSUE = 2, PR_COMP = 3, PR_FI
 // exact-mode adjoint (cg2d_adjoint.cu)
 struct ExactArgs {
   int batch, max_iters, checkpoint, rows_per_block;
+  int max_iters_cap;           // the max_iters the workspace was sized for (checkpoint slots are carved from it)
+  // recorded: the forward solve stored the checkpoints (cg2d_solve_exact) and its sums are in hist
+  // ([batch][H_NKIND][hist_len], one group of one right-hand side); no recording forward runs
+  int recorded;
+  const double* hist;
+  int hist_len;
   double norm;
   const double* norm_arr;
   const double *aW, *aS, *aC, *pW, *pS, *pC, *b, *x0, *xbar;
@@ -169,6 +182,10 @@ struct ExactArgs {
   double *b_bar, *gW, *gS, *gC, *gpW, *gpS, *gpC, *x_check;
 };
 size_t exact_adjoint_workspace(const TopoDev& tp, int batch, int max_iters, int checkpoint);
+// where the checkpoint blocks of an exact-adjoint workspace lie: r_c at ck_r0 + c stride, s_{c-1} at
+// ck_s0 + c stride (elements), c = 0 .. max_iters / checkpoint
+void exact_checkpoints(const TopoDev& tp, int batch, int max_iters, int checkpoint, void* ws, double** ck_r0,
+                       double** ck_s0, long long* stride);
 cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& args, void* workspace, cudaStream_t stream);
 
 // launchers (cg2d_solver.cu)

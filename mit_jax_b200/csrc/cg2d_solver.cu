@@ -969,6 +969,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       const double* xo;
       V *s_out, *q_out;
       double* x_out;
+      double* ck;     // checkpoint of s_k for the exact-mode adjoint, or null
       V beta;
       double alpha_prev;
       bool upd;
@@ -984,6 +985,8 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       q.beta = (V)si.c1(s);
       q.alpha_prev = si.c2(s);
       q.upd = si.has_alpha(s) != 0;
+      q.ck = (!MIXED && kp.ck_s && ((k + 1) % kp.ck_every) == 0) ? kp.ck_s + ((k + 1) / kp.ck_every) * kp.ck_stride
+                                                                 : nullptr;
       return q;
     };
     const SlotS q0 = slot(0), q1 = slot(g.nrhs > 1 ? 1 : 0);
@@ -997,6 +1000,9 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       const V qv = (V)op_A<C>(aw, ae, as, an, ac, (C)vw, (C)ve, (C)vs, (C)vn, (C)vc);
       stcg(q.s_out + i, vc);
       stcg(q.q_out + i, qv);
+      if constexpr (!MIXED) {
+        if (q.ck) q.ck[prow + i] = (double)vc;                                   // checkpoint s_k
+      }
       double xn = 0.0;
       if (q.upd) {
         xn = add(q.xo[w * P + i + 1], mul(q.alpha_prev, (double)q.so[rc]));
@@ -1024,6 +1030,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
     struct SlotX {
       const V *ro, *qv;
       V *r_out, *z_out;
+      double* ck;     // checkpoint of r_{k+1} for the exact-mode adjoint, or null
       V alpha;
     };
     const bool xp = pt == P_X;
@@ -1034,6 +1041,8 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       q.r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0) + grow;
       q.z_out = vec_ptr<V>(g, c.inst, s, V_Z) + grow;
       q.alpha = (V)si.c1(s);
+      q.ck = (!MIXED && xp && kp.ck_r && ((k + 1) % kp.ck_every) == 0)
+                 ? kp.ck_r + ((k + 1) / kp.ck_every) * kp.ck_stride : nullptr;
       return q;
     };
     const SlotX q0 = slot(0), q1 = slot(g.nrhs > 1 ? 1 : 0);
@@ -1051,6 +1060,9 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       }
       const V z = (V)op_M<C>(pc, pw, pe_, ps, pn, (C)vc, (C)vw, (C)ve, (C)vs, (C)vn);
       if (xp) stcg(q.r_out + i, vc);
+      if constexpr (!MIXED) {
+        if (q.ck) q.ck[prow + i] = (double)vc;                                   // checkpoint r_{k+1}
+      }
       stcg(q.z_out + i, z);
       if (edge) {
         if (xp) push_s(ptab, q.r_out - grow, j, w, i, vc);

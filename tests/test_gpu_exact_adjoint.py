@@ -1,7 +1,8 @@
-"""Exact-mode adjoint on the GPU (cg2d_adjoint_exact, reverse mode through the CG iterations the forward took):
-its recording forward equals the FP64 solve bit for bit; its gradients equal torch autograd through the same
-iterations (oracle/cg2d_exact_oracle.py) to rounding, for single and batched solves, whatever the checkpoint
-interval; and at a tight tolerance they approach the implicit derivative (measured here, not assumed)."""
+"""Exact-mode adjoint on the GPU (reverse mode through the CG iterations the forward took: cg2d_solve_exact, and
+the two-call cg2d_adjoint_exact): the recording forward equals the FP64 solve bit for bit, and both paths give the
+same gradients bit for bit; the gradients equal torch autograd through the same iterations
+(oracle/cg2d_exact_oracle.py) to rounding, for single and batched solves, whatever the checkpoint interval, and
+central differences; at a tight tolerance they approach the implicit derivative (measured here, not assumed)."""
 
 import numpy as np
 import pytest
@@ -146,3 +147,28 @@ def test_exact_adjoint_finite_differences(small):
             fd = (moved(1.0) - moved(-1.0)) / (2 * h)
             an = float((g[name] * dvec).sum())
             assert abs(fd - an) <= 1e-6 * abs(an), (name, fd, an)
+
+
+def test_exact_adjoint_one_pass_equals_recording_forward():
+    """The solve storing its own checkpoints and sums (cg2d_solve_exact) gives the two-call path's solution and
+    gradients bit for bit: three members with 37, 39 and 36 iterations, checkpoint intervals 0, 7 and 30, and a run
+    stopped by the iteration cap at a multiple of the interval (its last checkpoint lands in the spare slot)."""
+    from mit_jax_b200.synthetic import make_batch
+    syn, B = make_batch(16, ts=8, members=[0, 1, 2])
+    ex = cg.default_exchanger(syn.L)
+    B["b"][1] = O.interior_mask(syn.L).astype(np.float64)
+    B["b"][2] = B["b"][2] ** 2 * np.sign(B["b"][2])
+    w = np.random.default_rng(8).standard_normal((3,) + syn.L.shape2d) * O.interior_mask(syn.L)
+    ops = tuple(torch.as_tensor(B[k]).cuda() for k in cg.OPS)
+    args = (ex, ops, torch.as_tensor(B["b"]).cuda(), torch.as_tensor(B["x0"]).cuda(), torch.as_tensor(w).cuda())
+    norm = torch.as_tensor(B["cg2dNorm"])
+    for tol, maxit, c in ((1e-12, 300, 0), (1e-12, 300, 7), (1e-12, 300, 30), (0.0, 28, 7)):
+        x1, d1, g1 = cg.exact_adjoint(*args, cg2dNorm=norm, tolerance=tol, max_iters=maxit, checkpoint_every=c)
+        x2, d2, g2 = cg.exact_adjoint(*args, cg2dNorm=norm, tolerance=tol, max_iters=maxit, checkpoint_every=c,
+                                      one_pass=False)
+        assert [r["numIters"] for r in d1] == [r["numIters"] for r in d2]
+        if tol == 0.0:
+            assert [r["numIters"] for r in d1] == [maxit] * 3
+        torch.testing.assert_close(x1, x2, rtol=0, atol=0)
+        for k in NAMES:
+            torch.testing.assert_close(g1[k], g2[k], rtol=0, atol=0, msg=f"{k} checkpoint {c}")
