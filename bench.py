@@ -336,39 +336,72 @@ def run_gpu(a):
         except Exception:
             traffic = None
 
-    # ---- end to end through the public API from pinned host buffers
+    # ---- end to end through the public API from pinned host buffers. Every step uploads its inputs and
+    #      downloads its solutions, gradients and diagnostics; the steps are pipelined over three streams (step s+1's
+    #      inputs upload and step s-1's results download while step s computes), with two device input buffers.
     e2e = None
     if not a.no_e2e:
         host_in = {k: torch.as_tensor(B[k]).pin_memory() for k in (*cg.OPS, "b", "w", "x0")}
-        host_norm = torch.as_tensor(B["cg2dNorm"])
-        outs = {k: torch.empty((a.batch, *syn.L.shape2d), dtype=torch.float64).pin_memory()
-                for k in ("x", "lam", "gW", "gS", "gC")}
-        h2d = sum(v.numel() * v.element_size() for v in host_in.values()) + host_norm.numel() * 8
-        d2h = sum(v.numel() * v.element_size() for v in outs.values()) + 2 * a.batch * cg.capi.DIAG_BYTES
+        host_in["norm"] = torch.as_tensor(B["cg2dNorm"]).pin_memory()
+        keys = ("x", "lam", "gW", "gS", "gC")
+        outs = [{k: torch.empty((a.batch, *syn.L.shape2d), dtype=torch.float64).pin_memory() for k in keys}
+                for _ in range(2)]
+        dgs = [[torch.empty((a.batch, cg.capi.DIAG_BYTES), dtype=torch.uint8).pin_memory() for _ in range(2)]
+               for _ in range(2)]
+        h2d = sum(v.numel() * v.element_size() for v in host_in.values())
+        d2h = sum(v.numel() * v.element_size() for v in outs[0].values()) + 2 * a.batch * cg.capi.DIAG_BYTES
+        dbuf = [{k: torch.empty_like(v, device=dev) for k, v in host_in.items()} for _ in range(2)]
+        up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        ev = {n: [torch.cuda.Event() for _ in range(2)] for n in ("in", "comp")}
 
-        def e2e_step():
-            din = {k: v.to(dev, non_blocking=True) for k, v in host_in.items()}
-            r = cg.solve_with_adjoint(ex, tuple(din[k] for k in cg.OPS), din["b"], din["w"], din["x0"],
-                                      cg2dNorm=host_norm.to(dev, non_blocking=True), tolerance=a.tol,
-                                      max_iters=a.maxit, adj_tolerance=a.tol, adj_max_iters=a.maxit,
-                                      precision=a.precision)
-            for k in outs:
-                outs[k].copy_(r[k], non_blocking=True)
-            return r["diag_fwd"].cpu(), r["diag_adj"].cpu()
+        def upload(s):
+            i = s % 2
+            with torch.cuda.stream(up):
+                if s >= 2:
+                    up.wait_event(ev["comp"][i])            # step s-2 has finished reading buffer i
+                for k, v in host_in.items():
+                    dbuf[i][k].copy_(v, non_blocking=True)
+                ev["in"][i].record(up)
 
-        for _ in range(max(1, a.warmup)):
-            e2e_step()
+        def compute_and_download(s):
+            i = s % 2
+            d = dbuf[i]
+            with torch.cuda.stream(stream):
+                stream.wait_event(ev["in"][i])
+                r = cg.solve_with_adjoint(ex, tuple(d[k] for k in cg.OPS), d["b"], d["w"], d["x0"],
+                                          cg2dNorm=d["norm"], tolerance=a.tol, max_iters=a.maxit,
+                                          adj_tolerance=a.tol, adj_max_iters=a.maxit, precision=a.precision)
+                ev["comp"][i].record(stream)
+            with torch.cuda.stream(down):                    # downloads into a host buffer stay in stream order
+                down.wait_event(ev["comp"][i])
+                for k in keys:
+                    r[k].record_stream(down)
+                    outs[i][k].copy_(r[k], non_blocking=True)
+                for j, name in enumerate(("diag_fwd", "diag_adj")):
+                    r[name].record_stream(down)
+                    dgs[i][j].copy_(r[name], non_blocking=True)
+
+        def run(n):
+            upload(0)
+            for s in range(n):
+                if s + 1 < n:
+                    upload(s + 1)
+                compute_and_download(s)
+
+        run(max(2, a.warmup))
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(a.steps):
-            e2e_step()
-        e1.record(stream)
+        e0.record(up)
+        run(a.steps)
+        e1.record(down)
         barrier()
         et = max_over_ranks(e0.elapsed_time(e1), dev)
+        last = [cg.diag_records(t) for t in dgs[(a.steps - 1) % 2]]
         e2e = {"value": world * a.batch * a.steps / (et / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "pipelined": "uploads of step s+1 and downloads of step s-1 overlap step s (three streams)",
+               "not_ok": sum(r["status"] != "ok" for recs in last for r in recs)}
 
     # ---- the plain FP64 one-solve-per-launch kernel: one instance, forward launch then adjoint launch
     plain = None
