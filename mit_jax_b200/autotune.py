@@ -4,7 +4,8 @@ A schedule says where the work runs, not what it computes:
 - grid_ctas: how many CTAs the cooperative launch has;
 - ctas_per_sm: how many of them share an SM (1, or the occupancy maximum);
 - unit_deal: how the work units (instance, tile, row block) are dealt to them, round-robin (0) or in contiguous
-  runs (1).
+  runs (1);
+- stages: the depth of each CTA's copy pipeline (2 to 4 stage buffers; deeper takes more shared memory).
 No schedule changes a result bit: every sum is formed from per-unit partials in one fixed order, whichever CTA
 computed a unit (the GPU tests solve every candidate and compare them bit for bit).
 
@@ -45,14 +46,17 @@ def signature(groups, *, precision, sum_order, rows_per_block, replace_every=25,
 
 def candidates(sm_count, max_ctas_per_sm=2):
     """Schedules to try: 1 and up to max_ctas_per_sm CTAs per SM, the full co-resident grid and three quarters
-    and half of it, each with both unit deals. The library clamps ctas_per_sm to the occupancy maximum and the
-    grid to the co-resident CTAs and to the work units, so every candidate is a valid launch."""
+    and half of it, each with both unit deals and a two-stage pipeline; and one CTA per SM on every SM with three
+    and four stages. The library clamps ctas_per_sm to the occupancy maximum and the grid to the co-resident CTAs
+    and to the work units, so every candidate is a valid launch."""
     out = []
     for cps in range(1, max_ctas_per_sm + 1):
         full = cps * sm_count
         for grid in sorted({full, (3 * full) // 4, full // 2}, reverse=True):
             for deal in (0, 1):
-                out.append({"grid_ctas": int(max(1, grid)), "ctas_per_sm": cps, "unit_deal": deal})
+                out.append({"grid_ctas": int(max(1, grid)), "ctas_per_sm": cps, "unit_deal": deal, "stages": 2})
+    for ns in (3, 4):
+        out.append({"grid_ctas": int(sm_count), "ctas_per_sm": 1, "unit_deal": 0, "stages": ns})
     return out
 
 
@@ -67,7 +71,7 @@ def _load(path):
         return
     if isinstance(data, dict):
         for k, v in data.items():
-            if isinstance(v, dict) and {"grid_ctas", "ctas_per_sm", "unit_deal"} <= set(v):
+            if isinstance(v, dict) and {"grid_ctas", "ctas_per_sm", "unit_deal", "stages"} <= set(v):
                 _CACHE.setdefault(k, v)
 
 
@@ -93,7 +97,7 @@ def cached(key):
 
 def tune(groups, *, precision="f64", sum_order="rowblock", rows_per_block=8, replace_every=25,
          replace_above=100.0, iters=20, reps=3, force=False, report=None):
-    """The fastest schedule for these groups (a dict of grid_ctas, ctas_per_sm, unit_deal), from the cache or by
+    """The fastest schedule for these groups (a dict of grid_ctas, ctas_per_sm, unit_deal, stages), from the cache or by
     timing every candidate. report, if a list, receives one (schedule, milliseconds or None) per candidate."""
     from mit_jax_b200 import capi
     from mit_jax_b200.cg2d import GroupSpec, solve_groups

@@ -43,7 +43,8 @@ class Params(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("sum_order", ctypes.c_int), ("rows_per_block", ctypes.c_int),
                 ("replace_every", ctypes.c_int), ("replace_above", ctypes.c_double), ("grid_ctas", ctypes.c_int),
                 ("ctas_per_sm", ctypes.c_int), ("timeout_s", ctypes.c_double),
-                ("test_missing_arrivals", ctypes.c_int), ("profile", ctypes.c_int), ("unit_deal", ctypes.c_int)]
+                ("test_missing_arrivals", ctypes.c_int), ("profile", ctypes.c_int), ("unit_deal", ctypes.c_int),
+                ("stages", ctypes.c_int)]
 
 
 class Diag(ctypes.Structure):

@@ -59,7 +59,8 @@ class Cg2dParams:
 
 
 def _params_struct(precision="f64", sum_order="rowblock", rows_per_block=8, replace_every=25, replace_above=100.0,
-                   timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, test_missing_arrivals=0, profile=False, unit_deal=0):
+                   timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, test_missing_arrivals=0, profile=False, unit_deal=0,
+                   stages=0):
     p = capi.default_params()
     p.precision = capi.PREC_MIXED if precision == "mixed" else capi.PREC_F64
     p.sum_order = capi.SUM_FORTRAN if sum_order == "fortran" else capi.SUM_ROWBLOCK
@@ -72,6 +73,7 @@ def _params_struct(precision="f64", sum_order="rowblock", rows_per_block=8, repl
     p.test_missing_arrivals = test_missing_arrivals
     p.profile = 1 if profile else 0
     p.unit_deal = unit_deal
+    p.stages = stages
     return p
 
 
@@ -200,13 +202,13 @@ PROF_SLOTS = len(PROF_NAMES)
 
 def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8, replace_every=25,
                  replace_above=100.0, timeout_s=10.0, grid_ctas=0, ctas_per_sm=0, check_status=True,
-                 test_missing_arrivals=0, profile=False, unit_deal=0, schedule=None):
+                 test_missing_arrivals=0, profile=False, unit_deal=0, stages=0, schedule=None):
     """Run every right-hand side of every group in one persistent launch (cg2d_solve_groups).
 
     Returns per group a list (one entry per slot) of (x_out, x_fortran or None, diag ndarray of cg2d_diag_t).
     profile=True records per-CTA phase times; they are left in `solve_groups.last_profile` as an array
     [ctas, PROF_SLOTS] of nanoseconds, columns PROF_NAMES (include/cg2d.h, cg2d_workspace_profile).
-    The launch schedule is grid_ctas, ctas_per_sm and unit_deal, or schedule: a dict of those three, or "auto"
+    The launch schedule is grid_ctas, ctas_per_sm, unit_deal and stages, or schedule: a dict of those, or "auto"
     for the autotuner's choice for this workload (mit_jax_b200.autotune; tuned once, then cached). No schedule
     changes a result bit."""
     if not 1 <= len(groups) <= 4:
@@ -222,8 +224,9 @@ def solve_groups(groups, precision="f64", sum_order="rowblock", rows_per_block=8
         grid_ctas = int(schedule.get("grid_ctas", grid_ctas))
         ctas_per_sm = int(schedule.get("ctas_per_sm", ctas_per_sm))
         unit_deal = int(schedule.get("unit_deal", unit_deal))
+        stages = int(schedule.get("stages", stages))
     params = _params_struct(precision, sum_order, rows_per_block, replace_every, replace_above, timeout_s,
-                            grid_ctas, ctas_per_sm, test_missing_arrivals, profile, unit_deal)
+                            grid_ctas, ctas_per_sm, test_missing_arrivals, profile, unit_deal, stages)
     arr = (capi.Group * len(groups))()
     keep, outs = [], []
     for gi, G in enumerate(groups):

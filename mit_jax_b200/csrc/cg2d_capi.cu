@@ -70,11 +70,12 @@ cg2d_status_t check_params(const cg2d_params_t* p) {
   if (!(p->timeout_s > 0.0) || p->timeout_s > 3600.0) return CG2D_BAD_ARG;
   if (p->test_missing_arrivals < 0 || p->test_missing_arrivals > 1024) return CG2D_BAD_ARG;
   if (p->unit_deal != 0 && p->unit_deal != 1) return CG2D_BAD_ARG;
+  if (p->stages != 0 && (p->stages < 2 || p->stages > kMaxStages)) return CG2D_BAD_ARG;
   return CG2D_OK;
 }
 
-// chunk height and stage buffers: the largest chunk (8, else 4 rows) whose two stage buffers fit
-cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial, WsLayout* L) {
+// chunk height and stage buffers: the largest chunk (8, else 4 rows) whose `ns` stage buffers fit
+cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial, int ns, WsLayout* L) {
   const size_t fixed = fixed_smem_bytes(L->max_ni, serial);
   for (int ch : {8, 4}) {
     unsigned hot = 0, rep = 0;
@@ -94,19 +95,21 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
     const unsigned direct = (unsigned)(2 * (kWarps + 2) * (L->max_ni + 2) * sizeof(double));
     // the sums of a pass are formed with a tile-sum buffer per warp in the same area
     const unsigned sums = (unsigned)(kAllWarps * kMaxTiles * sizeof(double));
+    // the stage area (ns buffers) also holds a replacement pass's single stage, the direct passes' staging and the
+    // tile-sum buffers
     unsigned sb = hot;
-    if (2 * sb < sums) sb = (sums + 1) / 2;
-    if (2 * sb < rep) sb = (rep + 1) / 2;
-    if (2 * sb < direct) sb = (direct + 1) / 2;
+    if (ns * sb < sums) sb = (sums + ns - 1) / ns;
+    if (ns * sb < rep) sb = (rep + ns - 1) / ns;
+    if (ns * sb < direct) sb = (direct + ns - 1) / ns;
     sb = al128(sb);
-    const size_t smem = fixed + 2 * (size_t)sb;
+    const size_t smem = fixed + (size_t)ns * sb;
     if (smem <= (size_t)kSmemLimit) {
       L->ch = ch;
       L->stage_bytes = sb;
       L->smem = smem;
       // FORTRAN order keeps every element product of a chunk in one buffer: one stage
-      for (int i = 0; i < P_NPASS; ++i) L->nstage[i] = serial ? 1 : 2;
-      L->nstage[P_R] = (!serial && rep <= sb) ? 2 : 1;
+      for (int i = 0; i < P_NPASS; ++i) L->nstage[i] = serial ? 1 : ns;
+      L->nstage[P_R] = (!serial && rep <= sb) ? ns : 1;
       return CG2D_OK;
     }
   }
@@ -142,7 +145,7 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     L->total_units = (int)tu;
   }
   if (L->total_rhs > kMaxSolves || L->total_ops > kMaxOps) return CG2D_UNSUPPORTED;
-  cg2d_status_t st = size_stages(gr, ng, mixed, serial, L);
+  cg2d_status_t st = size_stages(gr, ng, mixed, serial, p->stages ? p->stages : 2, L);
   if (st != CG2D_OK) return st;
   L->hist_len = max_iters + 2;
   size_t o = 0;
@@ -187,6 +190,7 @@ void cg2d_default_params(cg2d_params_t* p) {
   p->test_missing_arrivals = 0;
   p->profile = 0;
   p->unit_deal = 0;
+  p->stages = 0;
 }
 
 const char* cg2d_status_string(cg2d_status_t s) {

@@ -12,7 +12,7 @@ constexpr int kWarps = 8;                  // compute warps per CTA; a chunk has
 constexpr int kProducer = kWarps;          // index of the warp that issues the bulk copies and folds the row sums
 constexpr int kThreads = (kWarps + 1) * 32;
 constexpr int kAllWarps = kThreads / 32;
-constexpr int kMaxStages = 2;              // stage buffers of the copy pipeline
+constexpr int kMaxStages = 4;              // stage buffers of the copy pipeline (cg2d_params_t.stages)
 constexpr int kMaxUnitsPerCta = 512;       // work units one CTA owns in a launch (its unit table)
 constexpr int kMaxGroups = CG2D_MAX_GROUPS;
 constexpr int kMaxSolves = CG2D_MAX_SOLVES; // right-hand sides per launch (one thread owns each)

@@ -29,6 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layouts():
     assert ctypes.sizeof(capi.Params) == 56
+    assert capi.Params.stages.offset == 52
     assert capi.Params.unit_deal.offset == 48
     assert ctypes.sizeof(capi.Diag) == 48
     assert ctypes.sizeof(capi.Group) == 8 + 4 + 4 + 6 * 8 + 8 + 8 + 5 * 16 + 16 + 8

@@ -41,8 +41,16 @@ def test_every_candidate_schedule_is_bitwise_equal(workload, precision):
     ref = cg.solve_groups([G], precision=precision)
     recs = cg.diag_records(ref[0][0][2])
     assert all(r["status"] == "ok" for r in recs)
+    ran = 0
     for cand in autotune.candidates(torch.cuda.get_device_properties(0).multi_processor_count):
-        _same(ref, cg.solve_groups([G], precision=precision, **cand))
+        try:
+            res = cg.solve_groups([G], precision=precision, **cand)
+        except cg.capi.Cg2dError as e:           # a pipeline too deep for the shared memory is refused, not run
+            assert e.status == cg.capi.CG2D_UNSUPPORTED, e
+            continue
+        _same(ref, res)
+        ran += 1
+    assert ran >= 12
 
 
 def test_tune_picks_a_candidate_and_caches_it(workload, monkeypatch):
