@@ -16,6 +16,9 @@ adjoint solve + coefficient cotangents) on all host cores, one instance per proc
 --mode pressure times SOLVE_FOR_PRESSURE around the solve (update_cg2d, cg2d_rhs, the FP64 solve, the post-solve
 exchange; default batch 16, 50 levels), each step with its own device time and bandwidth.
 
+--mode mixed_sizes times one mixed-precision launch over 8 LLC270 and 32 LLC90 instances and reports every
+solution's error against the FP64 solve of the same instance.
+
 --mode exact times the exact-mode adjoint instead (cg2d_adjoint_exact: FP64 forward, then reverse mode through
 every CG iteration with checkpointed, recomputed segments; default batch 16) and reports adjoint solves/s and the
 peak device memory of the step. The reference has no exact mode (it differentiates cg2d implicitly), so
@@ -48,7 +51,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--mode", default="forward_adjoint", choices=("forward_adjoint", "exact", "pressure"))
+    ap.add_argument("--mode", default="forward_adjoint", choices=("forward_adjoint", "exact", "pressure",
+                                                                  "mixed_sizes"))
     ap.add_argument("--batch", type=int, default=None, help="instances per GPU (64; 16 with --mode exact/pressure)")
     ap.add_argument("--nr", type=int, default=50, help="--mode pressure: vertical levels")
     ap.add_argument("--checkpoint", type=int, default=30, help="--mode exact: iterations between checkpoints")
@@ -796,8 +800,97 @@ def run_pressure(a):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------------------------
+# mixed sizes: LLC270 and LLC90 instances in one mixed-precision launch
+
+MIXED_SIZES_METRIC = "CG2D mixed-precision solves/s, 8 LLC270 + 32 LLC90 instances in one launch, on B200"
+
+
+def run_mixed_sizes(a):
+    import torch
+
+    from mit_jax_b200 import autotune
+    from mit_jax_b200 import cg2d as cg
+    from mit_jax_b200.graph import GraphedSolve
+    from mit_jax_b200.synthetic import make_batch
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    sizes = ((270, 8, 1000), (90, 32, a.maxit))
+    groups, npts = [], []
+    for N, count, maxit in sizes:
+        syn, B = make_batch(N, count)
+        ex = cg.default_exchanger(syn.L)
+        ops = tuple(torch.as_tensor(B[k]).to(dev) for k in cg.OPS)
+        b = torch.as_tensor(B["b"]).to(dev)
+        norms = torch.as_tensor(B["cg2dNorm"]).to(dev)
+        groups.append(cg.GroupSpec(ex, ops, [b], [torch.zeros_like(b)], [a.tol], [maxit], norms))
+        npts.append(13 * N * N)
+    stream = torch.cuda.current_stream(dev)
+    report = []
+    sched = autotune.tune(groups, precision="mixed", report=report)
+    graphed = GraphedSolve(groups, precision="mixed", schedule=sched)
+    for _ in range(max(3, a.warmup)):
+        graphed.replay()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(_gpu_uuid(torch, dev)) as clk:
+        time.sleep(0.25)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(a.steps):
+            res, _ = graphed.replay()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    clocks = clk.summary()
+    ms = e0.elapsed_time(e1) / a.steps
+    nsolve = sum(c for _, c, _ in sizes)
+    # every solution against the FP64 solve of the same instance (FP64 ROWBLOCK equals the FP64 oracle bit for bit)
+    ref = cg.solve_groups(groups, precision="f64")
+    errs, iters, alg, bad = {}, {}, 0, 0
+    for (N, _, _), r_m, r_f, n in zip(sizes, res, ref, npts):
+        xm, xf = r_m[0][0], r_f[0][0]
+        num = (xm - xf).abs().flatten(1).amax(1)
+        den = xf.abs().flatten(1).amax(1).clamp_min(1e-300)
+        e = (num / den).cpu().numpy()
+        recs, recs_f = cg.diag_records(r_m[0][2]), cg.diag_records(r_f[0][2])
+        errs[f"llc{N}"] = {"max": float(e.max()), "median": float(np.median(e))}
+        iters[f"llc{N}"] = {"mixed_mean": statistics.mean(r["numIters"] for r in recs),
+                            "f64_mean": statistics.mean(r["numIters"] for r in recs_f),
+                            "mixed_max": max(r["numIters"] for r in recs)}
+        bad += sum(r["status"] != "ok" for r in recs)
+        alg += sum(n * (r["numIters"] * 56 + r["replacements"] * 96) for r in recs)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (ms / 1e3) / 1e9
+    line = {
+        "metric": MIXED_SIZES_METRIC, "value": nsolve / (ms / 1e3), "unit": "solves/s", "n_gpus": 1,
+        "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "8 LLC270 + 32 LLC90 instances (two groups) in one mixed-precision persistent launch, "
+                               f"to {a.tol:g} (LLC270 cap 1000 iterations, LLC90 {a.maxit})",
+                   "grid": "LLC270 13x270x270 and LLC90 13x90x90, halo 4", "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": "1 GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "kernel": "cg2d_persistent (mixed, two groups)",
+                     "kernel_ms": ms, "algorithmic_bytes_per_launch": alg},
+        "error_vs_f64": errs, "iterations": iters, "not_ok": bad,
+        "cpu_baseline": None, "e2e": None, "gpu_launches": 3 * a.steps, "clocks": clocks,
+        "schedule": {"chosen": sched, "launch": "CUDA graph replay"},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     a = parse()
+    if a.mode == "mixed_sizes":
+        if a.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "--mode mixed_sizes has no CPU reference arm"}))
+            return 0
+        return run_mixed_sizes(a)
     if a.mode == "pressure":
         if a.impl == "reference":
             if int(os.environ.get("RANK", "0")) == 0:
