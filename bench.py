@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default launch schedule instead of the autotuner's")
     ap.add_argument("--no-graph", action="store_true", help="eager launches instead of CUDA graph replay")
+    ap.add_argument("--phases", action="store_true",
+                    help="after the timed region, one more launch with the kernel's phase timers (phases_ms)")
     a = ap.parse_args()
     if a.batch is None:
         a.batch = 16 if a.mode in ("exact", "pressure") else 64
@@ -340,6 +342,17 @@ def run_gpu(a):
         except Exception:
             traffic = None
 
+    # ---- the kernel's own phase timers: one more launch, outside the timed region
+    phases = None
+    if a.phases:
+        cg.solve_groups([G], precision=a.precision, schedule=sched, profile=True)
+        prof = cg.solve_groups.last_profile.astype(np.float64) / 1e6
+        phases = {"per_cta_mean": {n: float(prof[:, i].mean()) for i, n in enumerate(cg.PROF_NAMES)},
+                  "ctas": int(prof.shape[0]),
+                  "note": "ms per CTA over one launch: bar grid-wide waits, mbar waits for stage data, comp chunk "
+                          "compute, fin/direct/drain/other the rest of thread 0's time; issue and pwait the copy "
+                          "warp's busy and waiting time"}
+
     # ---- end to end through the public API from pinned host buffers. Every step uploads its inputs and
     #      downloads its solutions, gradients and diagnostics; the steps are pipelined over three streams (step s+1's
     #      inputs upload and step s-1's results download while step s computes), with two device input buffers.
@@ -462,6 +475,7 @@ def run_gpu(a):
                            "replacements_mean": statistics.mean(d["replacements"] for d in diag_f + diag_a),
                            "not_ok": len(bad)},
             "edge_products_ms": statistics.mean(edge_ms),
+            "phases_ms": phases,
             "schedule": {"chosen": sched or "library default", "launch": "eager" if a.no_graph else "CUDA graph replay",
                          "candidates_ms": [[c, ms] for c, ms in tune_report]},
             "plain_f64_one_solve_per_launch": plain,
