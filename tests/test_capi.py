@@ -52,6 +52,24 @@ def test_bad_arguments_are_rejected_without_a_gpu():
     assert lib.cg2d_solve_groups(g, 0, None, None, 0, None) == capi.CG2D_BAD_ARG
 
 
+def test_newer_entry_points_reject_bad_arguments_without_a_gpu():
+    """Null topologies, empty batches and missing outputs are refused before any device work."""
+    lib = capi.lib()
+    fs = capi.FreeSurf()
+    fs.Nr = 5
+    p15 = [None] * 15
+    assert lib.cg2d_update_operator(None, 1, ctypes.byref(fs), 1.0, None, 0.51, *p15, None) == capi.CG2D_BAD_ARG
+    assert lib.cg2d_pressure_rhs(None, 1, ctypes.byref(fs), *p15, None) == capi.CG2D_BAD_ARG
+    assert lib.cg2d_pressure_post(None, 1, None, None, None, None, None) == capi.CG2D_BAD_ARG
+    assert lib.cg2d_solve_exact_workspace_size(None, 1, 300, 8, 30) == 0
+    assert lib.cg2d_solve_exact(None, 1, 1.0, None, *([None] * 8), 1e-12, 300, None, 8, 30, *([None] * 9), None, 0,
+                                None) == capi.CG2D_BAD_ARG
+    assert lib.cg2d_adjoint_ecco_workspace_size(None, 1, 300, None) == 0
+    assert lib.cg2d_adjoint_ecco(None, 1, 1.0, None, *([None] * 8), 1e-13, 2000, 1, *([None] * 5), None, None, 0,
+                                 None) == capi.CG2D_BAD_ARG
+    assert lib.cg2d_adjoint_exact_workspace_size(None, 1, 300, 30) == 0
+
+
 def test_struct_layouts_match_the_c_compiler(tmp_path):
     """sizeof and every field offset of cg2d_params_t and cg2d_diag_t as gcc lays out include/cg2d.h."""
     import shutil

@@ -128,6 +128,32 @@ def test_batched_members_one_launch():
     assert len(iters) >= 2                      # uneven counts exercised the per-instance retirement
 
 
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_nan_instance_is_reported_and_isolated(precision):
+    """A NaN in one instance's right-hand side: that solve runs to its iteration cap and reports status "nan" (the
+    reference lets NaNs through silently), the launch itself succeeds, and the other instance of the same launch is
+    bit for bit its solo solve."""
+    from mit_jax_b200.synthetic import make_batch
+    syn, B = make_batch(16, ts=8, members=[0, 1])
+    ex = cg.default_exchanger(syn.L)
+    dev = torch.device("cuda")
+    ops = tuple(torch.as_tensor(B[k]).to(dev) for k in cg.OPS)
+    b = torch.as_tensor(B["b"]).to(dev)
+    J, I = syn.L.interior
+    b_nan = b.clone()
+    b_nan[1, 3, J.start + 2, I.start + 5] = float("nan")
+    x0 = torch.zeros_like(b)
+    G = cg.GroupSpec(ex, ops, [b_nan], [x0], [1e-12], [60], torch.as_tensor(B["cg2dNorm"]))
+    ((x, _, dg),), = cg.solve_groups([G], precision=precision)
+    d = cg.diag_records(dg)
+    assert d[1]["status"] == "nan" and d[1]["numIters"] == 60
+    G1 = cg.GroupSpec(ex, tuple(o[:1].contiguous() for o in ops), [b[:1].contiguous()], [x0[:1].contiguous()],
+                      [1e-12], [60], torch.as_tensor(B["cg2dNorm"][:1]))
+    ((x1, _, dg1),), = cg.solve_groups([G1], precision=precision)
+    torch.testing.assert_close(x[0], x1[0], rtol=0, atol=0)
+    assert d[0] == cg.diag_records(dg1)[0]
+
+
 def test_mixed_precision_matches_mixed_oracle_and_fp64(llc90):
     syn, ex_ref, tmap = llc90
     ex = cg.default_exchanger(syn.L)
