@@ -341,26 +341,13 @@ __global__ void k_fb(Geo G, const double* aW, const double* aS, const double* aC
   if (rs) row_sums(G, in, row, inb, prod, 0.0, 1, rs);
 }
 
-// Edge products of one point's faces for a stencil out = C v with out's cotangent u: the west and south faces of
-// the point, its own diagonal entry, and the east / north halo face when the point is the last of its row /
-// column (the faces edge_products_kernel writes). uc, uw, us: u at the point and its west / south neighbours
-// (interior only); vc, vw, ve, vs, vn: v at the point and its neighbours as the stencil reads it.
-__device__ __forceinline__ void point_edges(const TopoDev& tp, int j, int i, long long p, double uc, double uw,
-                                            double us, double vc, double vw, double ve, double vs, double vn,
-                                            double* gW, double* gS, double* gC) {
-  gW[p] += add(mul(uc, vw), i >= 1 ? mul(uw, vc) : 0.0);
-  gS[p] += add(mul(uc, vs), j >= 1 ? mul(us, vc) : 0.0);
-  gC[p] += mul(uc, vc);
-  if (i == tp.ni - 1) gW[p + 1] += mul(uc, ve);
-  if (j == tp.nj - 1) gS[p + tp.npx] += mul(uc, vn);
-}
-
 // Reverse of iteration k, first half. With qbar = sigbar s_k - alpha_k rbar (formed at each stencil point):
 //   sbar = bs sbar + alpha_k xbar + sigbar q_k + A qbar, bs = beta_{k+1} (the scaling of sbar left from the
-//   reverse of iteration k+1; none when k + 1 = K), gA += qbar (x) s_k, and the row sums of sbar s_{k-1}.
+//   reverse of iteration k+1; none when k + 1 = K), and the row sums of sbar s_{k-1}. qbar is stored (qb) for the
+//   segment's edge products (k_seg_edges).
 __global__ void k_rq(Geo G, const double* aW, const double* aS, const double* aC, const double* s, const double* q,
-                     const double* xbar, const double* rbar, double* sbar, const double* sp, double* gW, double* gS,
-                     double* gC, double* rs, Scal S, const int* K, int k) {
+                     const double* xbar, const double* rbar, double* sbar, const double* sp, double* qb, double* rs,
+                     Scal S, const int* K, int k) {
   const int Kin = K[blockIdx.y];
   if (k >= Kin) return;
   POINT_IN(G);
@@ -380,19 +367,20 @@ __global__ void k_rq(Geo G, const double* aW, const double* aS, const double* aC
     sb = add(add(sb, mul(a, xbar[p])), mul(sg, q[p]));
     sb = add(sb, opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], qw, qe, qs, qn, qc));
     sbar[p] = sb;
-    point_edges(tp, j, i, p, qc, qw, qs, sc, sw, se, ss, sn, gW, gS, gC);
+    qb[p] = qc;
     prod = mul(sb, sp[p]);
   }
   row_sums(G, in, row, inb, prod, 0.0, 1, rs);
 }
 
 // Reverse of iteration k, second half. With zbar = sbar + etabar r_k (formed at each stencil point):
-//   rbar += etabar z_k + M zbar, gM += zbar (x) r_k; and, when s1 / q1 (s_{k-1}, q_{k-1}) are given, the row sums
+//   rbar += etabar z_k + M zbar, zbar stored (zb) for the segment's edge products; and, when s1 / q1 (s_{k-1},
+//   q_{k-1}) are given, the row sums
 //   of xbar s_{k-1} and rbar q_{k-1} for the reverse of iteration k-1. Those row sums are also formed for the
 //   instances whose last iteration is k-1 (K = k): their reverse starts there, with rbar still 0.
 __global__ void k_rz(Geo G, const double* pW, const double* pS, const double* pC, const double* r, const double* z,
-                     const double* sbar, double* rbar, double* gpW, double* gpS, double* gpC, const double* xbar,
-                     const double* s1, const double* q1, double* rs, Scal S, const int* K, int k) {
+                     const double* sbar, double* rbar, double* zb, const double* xbar, const double* s1,
+                     const double* q1, double* rs, Scal S, const int* K, int k) {
   const int Kin = K[blockIdx.y];
   const bool live = k < Kin, next = s1 != nullptr && k - 1 < Kin;
   if (!live && !next) return;
@@ -411,7 +399,7 @@ __global__ void k_rz(Geo G, const double* pW, const double* pS, const double* pC
       rb = add(rb, mul(e, z[p]));
       rb = add(rb, opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], zc, zw, ze, zs, zn));
       rbar[p] = rb;
-      point_edges(tp, j, i, p, zc, zw, zs, rc, rw, re, rs_, rn_, gpW, gpS, gpC);
+      zb[p] = zc;
     }
     if (next) {
       p0 = mul(xbar[p], s1[p]);
@@ -419,6 +407,54 @@ __global__ void k_rz(Geo G, const double* pW, const double* pS, const double* pC
     }
   }
   if (next) row_sums(G, in, row, inb, p0, p1, 2, rs);
+}
+
+// The edge products of one segment (iterations c0 .. c0 + len - 1), added to the coefficient cotangents once per
+// point: gA += qbar_k (x) s_k and gM += zbar_k (x) r_k for k from the last iteration down, the same terms in the
+// same order as adding them one iteration at a time: the west and south faces of the point, its diagonal entry, and
+// the east / north halo face when the point is the last of its row / column (the faces edge_products_kernel
+// writes). qbar_m at qb0 + m vstr, zbar_m at zb0 + m vstr,
+// s_m at s0 + m sstr, r_m at r1 + m sstr (m >= 1) and at r0 (m = 0, the checkpoint).
+__global__ void k_seg_edges(Geo G, int c0, int len, const double* qb0, const double* zb0, long long vstr,
+                            const double* s0, const double* r0, const double* r1, long long sstr, double* gW,
+                            double* gS, double* gC, double* gpW, double* gpS, double* gpC, const int* K) {
+  const int Kin = K[blockIdx.y];
+  if (c0 >= Kin) return;
+  POINT_IN(G);
+  if (!inb) return;
+  const bool ie = i == tp.ni - 1, jn = j == tp.nj - 1;
+  const long long pe_ = p + 1, pn_ = p + tp.npx;
+  double aw = gW[p], as = gS[p], ac = gC[p], ae = ie ? gW[pe_] : 0.0, an = jn ? gS[pn_] : 0.0;
+  double bw = gpW[p], bs = gpS[p], bc = gpC[p], be = ie ? gpW[pe_] : 0.0, bn = jn ? gpS[pn_] : 0.0;
+  for (int m = len - 1; m >= 0; --m) {
+    if (c0 + m >= Kin) continue;
+    {
+      const double* u = qb0 + m * vstr + base;
+      const double* v = s0 + m * sstr + base;
+      auto V = [&](int o) -> double { return o < 0 ? 0.0 : v[o]; };
+      const double uc = u[off], vc = v[off];
+      aw = aw + add(mul(uc, V(ow)), i >= 1 ? mul(u[off - 1], vc) : 0.0);
+      as = as + add(mul(uc, V(os)), j >= 1 ? mul(u[off - tp.npx], vc) : 0.0);
+      ac = ac + mul(uc, vc);
+      if (ie) ae = ae + mul(uc, V(oe));
+      if (jn) an = an + mul(uc, V(on));
+    }
+    {
+      const double* u = zb0 + m * vstr + base;
+      const double* v = (m == 0 ? r0 : r1 + m * sstr) + base;
+      auto V = [&](int o) -> double { return o < 0 ? 0.0 : v[o]; };
+      const double uc = u[off], vc = v[off];
+      bw = bw + add(mul(uc, V(ow)), i >= 1 ? mul(u[off - 1], vc) : 0.0);
+      bs = bs + add(mul(uc, V(os)), j >= 1 ? mul(u[off - tp.npx], vc) : 0.0);
+      bc = bc + mul(uc, vc);
+      if (ie) be = be + mul(uc, V(oe));
+      if (jn) bn = bn + mul(uc, V(on));
+    }
+  }
+  gW[p] = aw; gS[p] = as; gC[p] = ac;
+  gpW[p] = bw; gpS[p] = bs; gpC[p] = bc;
+  if (ie) { gW[pe_] = ae; gpW[pe_] = be; }
+  if (jn) { gS[pn_] = an; gpS[pn_] = bn; }
 }
 
 // coefficient cotangents of a stencil application out = C v: gW/gS/gC += sign (u (x) v) on the faces and points
@@ -509,13 +545,13 @@ size_t exact_adjoint_workspace(const TopoDev& tp, int batch, int max_iters, int 
   b += vec * 5;                                   // r, s, z, q, x of the recording forward
   b += vec * 2 * (size_t)(std::max(1, nseg) + 1); // checkpoints r_c, s_{c-1}; one slot more for a forward that
                                                   // records at its last iteration
-  b += vec * 4 * (size_t)C;                       // a segment's r, z, s, q
+  b += vec * 6 * (size_t)C;                       // a segment's r, z, s, q, qbar, zbar
   b += vec * 3;                                   // xbar, rbar, sbar
   b += sizeof(double) * batch * 2 * rows;         // row sums
   b += sizeof(double) * ((size_t)4 * std::max(1, max_iters) * batch + 5 * batch);   // scalars, rn, norm
   b += sizeof(int) * batch;
   b += sizeof(int) * 2 * (size_t)tp.T * (tp.nj + tp.ni);   // padded-offset neighbour table
-  b += 256 * (size_t)(33 + 2 * std::max(1, nseg) + 4 * C);   // each buffer starts 256-byte aligned
+  b += 256 * (size_t)(35 + 2 * std::max(1, nseg) + 6 * C);   // each buffer starts 256-byte aligned
   return b;
 }
 
@@ -561,6 +597,10 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   }
   std::vector<double*> sg_r(C), sg_z(C), sg_s(C), sg_q(C);
   for (int c = 0; c < C; ++c) { sg_r[c] = vec(); sg_z[c] = vec(); sg_s[c] = vec(); sg_q[c] = vec(); }
+  // qbar_m, zbar_m of the segment being reversed (edge products added once per segment)
+  double* qb0 = reinterpret_cast<double*>(take(vstride * C));
+  double* zb0 = reinterpret_cast<double*>(take(vstride * C));
+  const long long vstr = (long long)(vstride / sizeof(double)), sstr = 4 * vstr;
   double *xbar = vec(), *rbar = vec(), *sbar = vec();
   double* rs = reinterpret_cast<double*>(take(sizeof(double) * A.batch * 2 * rows));
   Scal S;
@@ -671,15 +711,18 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
       const int k = c0 + m;
       k_rev_alpha<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rq<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_s[m], sg_q[m], xbar, rbar, sbar, sp(m), A.gW, A.gS, A.gC,
+      k_rq<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_s[m], sg_q[m], xbar, rbar, sbar, sp(m), qb0 + m * vstr,
                                    rs, S, K, k);
       LK();
       k_rev_beta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rz<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rr(m), sg_z[m], sbar, rbar, A.gpW, A.gpS, A.gpC, xbar,
+      k_rz<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rr(m), sg_z[m], sbar, rbar, zb0 + m * vstr, xbar,
                                    m > 0 ? sg_s[m - 1] : nullptr, m > 0 ? sg_q[m - 1] : nullptr, rs, S, K, k);
       LK();
     }
+    k_seg_edges<<<gp, bp, 0, st>>>(G, c0, len, qb0, zb0, vstr, sg_s[0], ck_r[seg], sg_r[0], sstr, A.gW, A.gS, A.gC,
+                                   A.gpW, A.gpS, A.gpC, K);
+    LK();
   }
   // r_0 = b_n - A x0_n: the cotangents of b and, through x0_n, of A
   k_scale<<<gp, bp, 0, st>>>(G, rbar, nrm, rn, A.b_bar, 1);
