@@ -452,11 +452,15 @@ __device__ __forceinline__ double butterfly(double v) {
   for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-__device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, const Smem& sm, int st) {
+// (two: the pass forms two sums per solve; otherwise the second kind is not read and not reduced)
+__device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, const Smem& sm, int st, bool two) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double r0 = butterfly(lp.v[0]), r1 = butterfly(lp.v[1]);
+  const double r0 = butterfly(lp.v[0]), r1 = two ? butterfly(lp.v[1]) : 0.0;
   double r2 = 0.0, r3 = 0.0;
-  if (g.nrhs > 1) { r2 = butterfly(lp.v[2]); r3 = butterfly(lp.v[3]); }
+  if (g.nrhs > 1) {
+    r2 = butterfly(lp.v[2]);
+    if (two) r3 = butterfly(lp.v[3]);
+  }
   if (lane == 0) {
     double* rs = sm.rowsum() + st * 4 * kWarps;
     rs[0 * kWarps + warp] = r0;
@@ -636,7 +640,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
           vmax1 = y1 > vmax1 ? y1 : vmax1;
         }
       } else if (!kp.serial) {
-        row_sums(g, lp, sm, 0);
+        row_sums(g, lp, sm, 0, true);
       }
     }
     if (pt == P_MAX) {
@@ -947,6 +951,12 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       lp.v[3] = add(lp.v[3], p1);
     }
   };
+  // the same for passes that form one sum per solve (the second kind is never read there)
+  auto emit1 = [&](int s, int i, double p0) {
+    if (kp.serial) sm.prod()[((s * 2) * kWarps + w) * kp.max_ni + i] = p0;
+    else if (s == 0) lp.v[0] = add(lp.v[0], p0);
+    else lp.v[2] = add(lp.v[2], p0);
+  };
   // runs f(i) for this lane's columns
   auto columns = [&](auto&& f) {
     if (MAXM > 0) {
@@ -1013,7 +1023,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
         push_s(ptab, q.q_out - grow, j, w, i, qv);
         if (MIXED && q.upd) push_s(ptab, q.x_out - grow, j, w, i, xn);   // x's neighbours: replacement pass only
       }
-      emit(s, i, mul((double)vc, (double)qv), 0.0);
+      emit1(s, i, mul((double)vc, (double)qv));
     };
     columns([&](int i) {
       const int rc = (w + 1) * P + i + 1;
@@ -1069,7 +1079,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
         push_s(ptab, q.z_out - grow, j, w, i, z);
       }
       if (xp) emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));
-      else emit(s, i, mul((double)z, (double)vc), 0.0);
+      else emit1(s, i, mul((double)z, (double)vc));
     };
     columns([&](int i) {
       const int rc = (w + 1) * P + i + 1;
@@ -1103,7 +1113,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
         const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + NP], ac[cr], vw, ve, vs, vn, vc));
         stcg(r_out + grow + i, r);
         if (er | (i == 0) | (i == ni - 1)) push_s(ptab, r_out, j, w, i, r);
-        emit(s, i, mul((double)r, (double)r), 0.0);
+        emit1(s, i, mul((double)r, (double)r));
       }
     }
   }
@@ -1206,7 +1216,7 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
     const GroupDev& g = kp.g[c.gi];
     const Slots si = slots_of(g, c.inst, sm);
     const Lanes lp = compute_chunk<MIXED, MAXM>(kp, c, pt, k, si, st, sm);
-    if (warp < c.nr && !kp.serial) row_sums(g, lp, sm, st);
+    if (warp < c.nr && !kp.serial) row_sums(g, lp, sm, st, pt == P_X);
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty()[st]);
     PROF_ADD(kp, sm, PR_COMP, t0);
