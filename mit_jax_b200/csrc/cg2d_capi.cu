@@ -434,7 +434,7 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
 
   const size_t smem = L.smem;
   int bps = 0;
-  if (solver_occupancy(kp.mixed, kp.max_ni, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  if (solver_occupancy(kp, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
   if (params->ctas_per_sm > 0 && params->ctas_per_sm < bps) bps = params->ctas_per_sm;
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);

@@ -191,7 +191,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& args, void* worksp
 // launchers (cg2d_solver.cu)
 size_t fixed_smem_bytes(int max_ni, int serial);
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream);
-cudaError_t solver_occupancy(int mixed, int max_ni, size_t smem, int* blocks_per_sm);
+cudaError_t solver_occupancy(const KParams& kp, size_t smem, int* blocks_per_sm);
 cudaError_t launch_pack_coef(const GroupDev& g, int mixed, cudaStream_t stream);
 cudaError_t launch_apply_operator(const TopoDev& tp, int batch, double norm, const double* aW, const double* aS,
                                   const double* aC, const double* v, double* out, cudaStream_t stream);

@@ -801,6 +801,21 @@ __device__ __forceinline__ bool cursor_next(const KParams& kp, const Smem& sm, C
 struct Chunk {
   int gi, inst, lu, t, j0u, j1u, jc, nr;
 };
+
+// The group and stage layout of a chunk. ONE: the launch has one group, so both are read at addresses fixed at
+// compile time (the parameter loads fold into the instructions that use them instead of loads by index).
+template <bool ONE>
+__device__ __forceinline__ const GroupDev& group_of(const KParams& kp, int gi) { return kp.g[ONE ? 0 : gi]; }
+template <bool ONE>
+__device__ __forceinline__ const StageLay& stage_lay(const KParams& kp, int gi, int pt) {
+  if (!ONE) return kp.lay[gi][pt];
+  switch (pt) {
+    case P_S: return kp.lay[0][P_S];
+    case P_X: return kp.lay[0][P_X];
+    case P_Z: return kp.lay[0][P_Z];
+    default: return kp.lay[0][P_R];
+  }
+}
 __device__ __forceinline__ Chunk chunk_at(const KParams& kp, const Smem& sm, int ui, int jc) {
   const Unit u = unit_at(sm, ui);
   Chunk c;
@@ -893,17 +908,17 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
 // w 3 ldc + i (columns: W/pW, +ldc S/pS, +2 ldc C/pC; east face +1, north face +3 ldc). A point pushes its new
 // values to the rings of the tiles that read it when it lies on the tile's edge (every point of the first and
 // last row, the first and last point of the others).
-template <bool MIXED, int MAXM>
+template <bool MIXED, int MAXM, bool ONE>
 __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si, int st,
                                const Smem& sm) {
   Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
   using V = typename Prec<MIXED>::V;
   using C = typename Prec<MIXED>::C;
-  const GroupDev& g = kp.g[c.gi];
+  const GroupDev& g = group_of<ONE>(kp, c.gi);
   const TopoDev& tp = g.tp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp >= c.nr) return lp;
-  const StageLay& L = kp.lay[c.gi][pt];
+  const StageLay& L = stage_lay<ONE>(kp, c.gi, pt);
   const unsigned char* sb = smem_raw + sm.stage + st * kp.stage_bytes;
   const int ni = tp.ni, nj = tp.nj, t = c.t, w = warp, j = c.jc + w;
   const int P = tp.P, CL = g.ldc, CR = 3 * g.ldc;
@@ -1195,7 +1210,7 @@ __device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const S
   return ok;
 }
 
-template <bool MIXED, int MAXM>
+template <bool MIXED, int MAXM, bool ONE>
 __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, Pipe& pp) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ns = kp.nstage[pt];
@@ -1213,9 +1228,9 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
     }
     t0 = PROF_T0(kp);
     const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
-    const GroupDev& g = kp.g[c.gi];
+    const GroupDev& g = group_of<ONE>(kp, c.gi);
     const Slots si = slots_of(g, c.inst, sm);
-    const Lanes lp = compute_chunk<MIXED, MAXM>(kp, c, pt, k, si, st, sm);
+    const Lanes lp = compute_chunk<MIXED, MAXM, ONE>(kp, c, pt, k, si, st, sm);
     if (warp < c.nr && !kp.serial) row_sums(g, lp, sm, st, pt == P_X);
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty()[st]);
@@ -1226,11 +1241,11 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
   return true;
 }
 
-template <bool MIXED, int MAXM>
+template <bool MIXED, int MAXM, bool ONE>
 __device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const Smem& sm, Pipe& pp) {
   bool ok;
   if ((threadIdx.x >> 5) == kProducer) ok = produce_pass(kp, pt, k, hidx, sm, pp);
-  else ok = consume_pass<MIXED, MAXM>(kp, pt, k, sm, pp);
+  else ok = consume_pass<MIXED, MAXM, ONE>(kp, pt, k, sm, pp);
   const unsigned long long td = PROF_T0(kp);
   const int bad = __syncthreads_or(!ok);
   PROF_ADD(kp, sm, PR_DRAIN, td);
@@ -1280,7 +1295,7 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
   PROF_ADD(kp, sm, PR_CTRL, t0);
 }
 
-template <bool MIXED, int MAXM>
+template <bool MIXED, int MAXM, bool ONE>
 __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const __grid_constant__ KParams kp) {
   const Smem sm = carve(kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
@@ -1337,7 +1352,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
   if (own) S->rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, 0, 0, sm, pp);
+  ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_Z, 0, 0, sm, pp);
   ok = grid_sync(kp, target, P_Z, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
@@ -1361,7 +1376,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
-    ok = run_pass_pipe<MIXED, MAXM>(kp, P_S, k, k, sm, pp);
+    ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_S, k, k, sm, pp);
     ok = grid_sync(kp, target, P_S, k, sm) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
@@ -1379,7 +1394,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     }
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, own ? S->alpha : 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM>(kp, P_X, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_X, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_X, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
@@ -1389,7 +1404,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
     }
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, own ? S->alpha : 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM>(kp, P_R, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_R, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_R, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
@@ -1397,7 +1412,7 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const
         ++S->nrep;
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM>(kp, P_Z, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_Z, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_Z, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
@@ -1607,28 +1622,32 @@ static int grid_for(long long work) {
   return (int)b;
 }
 
-// the kernel instantiation for a launch: precision and the column steps per row (ceil(max_ni / 32), unrolled for
-// tiles up to 96 and 288 points wide)
-static const void* solver_fn(int mixed, int max_ni) {
+// the kernel instantiation for a launch: precision, the column steps per row (ceil(max_ni / 32), unrolled for
+// tiles up to 96 and 288 points wide) and whether the launch has a single group
+template <bool ONE>
+static const void* solver_fn_of(int mixed, int max_ni) {
   if (mixed) {
-    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3>;
-    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9>;
-    return (const void*)cg2d_persistent<true, 0>;
+    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE>;
+    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE>;
+    return (const void*)cg2d_persistent<true, 0, ONE>;
   }
-  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3>;
-  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9>;
-  return (const void*)cg2d_persistent<false, 0>;
+  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE>;
+  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE>;
+  return (const void*)cg2d_persistent<false, 0, ONE>;
+}
+static const void* solver_fn(const KParams& kp) {
+  return kp.ngroups == 1 ? solver_fn_of<true>(kp.mixed, kp.max_ni) : solver_fn_of<false>(kp.mixed, kp.max_ni);
 }
 
-cudaError_t solver_occupancy(int mixed, int max_ni, size_t smem, int* blocks_per_sm) {
-  const void* fn = solver_fn(mixed, max_ni);
+cudaError_t solver_occupancy(const KParams& kp, size_t smem, int* blocks_per_sm) {
+  const void* fn = solver_fn(kp);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, smem);
 }
 
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream) {
-  const void* fn = solver_fn(kp.mixed, kp.max_ni);
+  const void* fn = solver_fn(kp);
   void* args[] = {const_cast<KParams*>(&kp)};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream);
 }
