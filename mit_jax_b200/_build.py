@@ -10,7 +10,7 @@ SOURCES = [HERE / "csrc" / "cg2d_solver.cu", HERE / "csrc" / "cg2d_capi.cu", HER
            HERE / "csrc" / "cg2d_pressure.cu"]
 OUT = HERE / "libcg2d.so"
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC"]
 
 
 def nvcc():
@@ -19,14 +19,24 @@ def nvcc():
 
 
 def build(force=False, verbose=False):
+    """Compile the translation units side by side into objects next to the library, then link libcg2d.so."""
     deps = SOURCES + [HERE / "csrc" / "cg2d_internal.cuh", HERE.parent / "include" / "cg2d.h"]
     if not force and OUT.exists() and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", str(OUT) + ".tmp", *map(str, SOURCES)]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    objs = [HERE / "csrc" / (src.stem + ".o") for src in SOURCES]
+    procs = []
+    for src, obj in zip(SOURCES, objs):
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", str(obj), str(src)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, pr in procs if pr.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
+    subprocess.run([nvcc(), *NVCC_FLAGS, "-shared", "-o", str(OUT) + ".tmp", *map(str, objs)], check=True)
     os.replace(str(OUT) + ".tmp", OUT)
+    for obj in objs:
+        obj.unlink()
     return OUT
 
 

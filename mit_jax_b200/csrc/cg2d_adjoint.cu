@@ -266,25 +266,55 @@ __device__ __forceinline__ void neighbours(const Geo& G, int t, int j, int i, in
   on = j < nj - 1 ? off + tp.npx : G.nbp[2 * T * nj + T * ni + t * ni + i];
 }
 
-// Row sums of up to two per-point products (v0, v1; points outside the tile pass inb = false) for the row of
-// threadIdx.y, in k_rowdot's order: lane partials over i = lane + 32 m in order, then the xor butterfly. The
-// products go through shared memory ([2][blockDim.y][blockDim.x] doubles). Every thread of the block calls it.
-__device__ void row_sums(const Geo& G, int in, int row, bool inb, double v0, double v1, int nq, double* rs) {
+// Iteration kernels march over rows: thread (x, y) of a block takes point i = x of the rows
+// row0 + h blockDim.y + y, h = 0 .. kRows - 1, row0 = blockIdx.x blockDim.y kRows, so that the instance check, the
+// iteration's scalars and the block's row-sum tail are paid once per kRows rows.
+constexpr int kRows = 4;
+
+// one row of the march: the point (t, j, i) and its neighbours' padded offsets in the instance
+#define ROW_POINT(G, row)                                                                 \
+  const bool inb = i < tp.ni && (row) < tp.T * tp.nj;                                     \
+  const int t = inb ? (row) / tp.nj : 0, j = inb ? (row) - t * tp.nj : 0;                 \
+  const int off = ((t * tp.npy + j + tp.OLy) * tp.npx) + i + tp.OLx;                      \
+  const long long p = base + off;                                                         \
+  int ow = -1, oe = -1, os = -1, on = -1;                                                 \
+  if (inb) neighbours(G, t, j, i, off, ow, oe, os, on)
+
+// The row products of march step h (q: which product) go through shared memory, [2][kRows][blockDim.y][blockDim.x]
+// doubles; points outside the tile store 0
+__device__ __forceinline__ void put_prod(int q, int h, double v) {
   extern __shared__ double shp[];
-  const int bx = blockDim.x, by = blockDim.y, x = threadIdx.x, y = threadIdx.y;
-  shp[y * bx + x] = inb ? v0 : 0.0;
-  if (nq > 1) shp[(by + y) * bx + x] = inb ? v1 : 0.0;
+  shp[((q * kRows + h) * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x] = v;
+}
+// Row sums of the block's rows, in k_rowdot's order: lane partials over i = lane + 32 m in order, then the xor
+// butterfly; the first warp of thread row y sums the rows it marched over. Every thread of the block calls it.
+__device__ void row_sums(const Geo& G, int in, int row0, int nq, double* rs) {
+  extern __shared__ double shp[];
   __syncthreads();
+  const int bx = blockDim.x, by = blockDim.y, x = threadIdx.x, y = threadIdx.y;
   const int rows = G.tp.T * G.tp.nj;
-  if (x < 32 && row < rows) {
+  if (x >= 32) return;
+  for (int h = 0; h < kRows; ++h) {
+    const int row = row0 + h * by + y;
+    if (row >= rows) break;
     for (int q = 0; q < nq; ++q) {
+      const double* sp_ = shp + ((q * kRows + h) * by + y) * bx;
       double v = 0.0;
-      for (int ii = x; ii < G.tp.ni; ii += 32) v = add(v, shp[(q * by + y) * bx + ii]);
+      for (int ii = x; ii < G.tp.ni; ii += 32) v = add(v, sp_[ii]);
       for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
       if (x == 0) rs[((long long)in * 2 + q) * rows + row] = v;
     }
   }
 }
+
+#define MARCH_BEGIN                                                                       \
+  const TopoDev& tp = G.tp;                                                               \
+  const int i = threadIdx.x, in = blockIdx.y;                                             \
+  const long long base = (long long)in * G.pe;                                            \
+  const int row0 = blockIdx.x * blockDim.y * kRows;                                       \
+  for (int h = 0; h < kRows; ++h) {                                                       \
+    const int row = row0 + h * blockDim.y + threadIdx.y;                                  \
+    ROW_POINT(G, row);
 
 // Iteration k, first half, with the updates of iteration k-1 (upd, k >= 1):
 //   r_k = r_{k-1} - alpha_{k-1} q_{k-1}  (cg2d.py:255; written to rout when non-null),
@@ -294,83 +324,95 @@ __device__ void row_sums(const Geo& G, int in, int row, bool inb, double v0, dou
 // Without upd, r_k is rp itself. r_k at a neighbour is formed from that neighbour's r_{k-1} and q_{k-1}: the
 // value its owner computes, as the exchange of r gives it (cg2d.py:260). The updates of iteration k-1 run for
 // instances that took it (k - 1 < K), the rest for instances that take iteration k.
-__global__ void k_fa(Geo G, const double* pW, const double* pS, const double* pC, const double* rp, const double* qp,
-                     const double* sp, double* x, double* rout, double* z, double* ckr, double* cks, double* rs,
-                     Scal S, const int* K, int k, int upd) {
+__global__ void k_fa(Geo G, const double* __restrict__ pW, const double* __restrict__ pS,
+                     const double* __restrict__ pC, const double* __restrict__ rp, const double* __restrict__ qp,
+                     const double* __restrict__ sp, double* __restrict__ x, double* __restrict__ rout,
+                     double* __restrict__ z, double* __restrict__ ckr, double* __restrict__ cks,
+                     double* __restrict__ rs, Scal S, const int* __restrict__ K, int k, int upd) {
   const int Kin = K[blockIdx.y];
   const bool zl = k < Kin, ul = upd && k - 1 < Kin;
   if (!zl && !ul) return;
-  POINT_IN(G);
-  const double a = ul ? S.alpha[(long long)(k - 1) * G.batch + in] : 0.0;
-  auto R = [&](int o) -> double {
-    if (o < 0) return 0.0;
-    return upd ? sub(rp[base + o], mul(a, qp[base + o])) : rp[base + o];
-  };
-  double prod = 0.0;
-  if (inb) {
-    const double rc = R(off);
-    if (ul && rout) rout[p] = rc;
-    if (ul && x) x[p] = add(x[p], mul(a, sp[p]));
-    if (zl) {
-      if (ckr) ckr[p] = rc;
-      if (cks) cks[p] = sp[p];
-      const double zc = opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], rc, R(ow), R(oe), R(os), R(on));
-      z[p] = zc;
-      prod = mul(zc, rc);
+  const double a = ul ? S.alpha[(long long)(k - 1) * G.batch + blockIdx.y] : 0.0;
+  MARCH_BEGIN
+    auto R = [&](int o) -> double {
+      if (o < 0) return 0.0;
+      return upd ? sub(rp[base + o], mul(a, qp[base + o])) : rp[base + o];
+    };
+    double prod = 0.0;
+    if (inb) {
+      const double rc = R(off);
+      if (ul && rout) rout[p] = rc;
+      if (ul && x) x[p] = add(x[p], mul(a, sp[p]));
+      if (zl) {
+        if (ckr) ckr[p] = rc;
+        if (cks) cks[p] = sp[p];
+        const double zc = opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], rc, R(ow), R(oe), R(os), R(on));
+        z[p] = zc;
+        prod = mul(zc, rc);
+      }
     }
+    if (rs && zl) put_prod(0, h, prod);
   }
-  if (rs && zl) row_sums(G, in, row, inb, prod, 0.0, 1, rs);
+  if (rs && zl) row_sums(G, in, row0, 1, rs);
 }
 
 // Iteration k, second half: s_k = z_k + beta_k s_{k-1} (cg2d.py:249), q_k = A s_k (cg2d.py:251), the row sums of
 // s_k q_k (cg2d.py:252; when rs is non-null). s_k at a neighbour is formed from that neighbour's z_k and s_{k-1}.
-__global__ void k_fb(Geo G, const double* aW, const double* aS, const double* aC, const double* z, const double* sp,
-                     double* s, double* q, double* rs, Scal S, const int* K, int k) {
+__global__ void k_fb(Geo G, const double* __restrict__ aW, const double* __restrict__ aS,
+                     const double* __restrict__ aC, const double* __restrict__ z, const double* __restrict__ sp,
+                     double* __restrict__ s, double* __restrict__ q, double* __restrict__ rs, Scal S,
+                     const int* __restrict__ K, int k) {
   if (k >= K[blockIdx.y]) return;
-  POINT_IN(G);
-  const double beta = S.beta[(long long)k * G.batch + in];
-  auto Sv = [&](int o) -> double { return o < 0 ? 0.0 : add(z[base + o], mul(beta, sp[base + o])); };
-  double prod = 0.0;
-  if (inb) {
-    const double sc = Sv(off);
-    const double qc = opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], Sv(ow), Sv(oe), Sv(os), Sv(on), sc);
-    s[p] = sc;
-    q[p] = qc;
-    prod = mul(sc, qc);
+  const double beta = S.beta[(long long)k * G.batch + blockIdx.y];
+  MARCH_BEGIN
+    auto Sv = [&](int o) -> double { return o < 0 ? 0.0 : add(z[base + o], mul(beta, sp[base + o])); };
+    double prod = 0.0;
+    if (inb) {
+      const double sc = Sv(off);
+      const double qc = opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], Sv(ow), Sv(oe), Sv(os), Sv(on), sc);
+      s[p] = sc;
+      q[p] = qc;
+      prod = mul(sc, qc);
+    }
+    if (rs) put_prod(0, h, prod);
   }
-  if (rs) row_sums(G, in, row, inb, prod, 0.0, 1, rs);
+  if (rs) row_sums(G, in, row0, 1, rs);
 }
 
 // Reverse of iteration k, first half. With qbar = sigbar s_k - alpha_k rbar (formed at each stencil point):
 //   sbar = bs sbar + alpha_k xbar + sigbar q_k + A qbar, bs = beta_{k+1} (the scaling of sbar left from the
 //   reverse of iteration k+1; none when k + 1 = K), and the row sums of sbar s_{k-1}. qbar is stored (qb) for the
 //   segment's edge products (k_seg_edges).
-__global__ void k_rq(Geo G, const double* aW, const double* aS, const double* aC, const double* s, const double* q,
-                     const double* xbar, const double* rbar, double* sbar, const double* sp, double* qb, double* rs,
-                     Scal S, const int* K, int k) {
+__global__ void k_rq(Geo G, const double* __restrict__ aW, const double* __restrict__ aS,
+                     const double* __restrict__ aC, const double* __restrict__ s, const double* __restrict__ q,
+                     const double* __restrict__ xbar, const double* __restrict__ rbar, double* __restrict__ sbar,
+                     const double* __restrict__ sp, double* __restrict__ qb, double* __restrict__ rs, Scal S,
+                     const int* __restrict__ K, int k) {
   const int Kin = K[blockIdx.y];
   if (k >= Kin) return;
-  POINT_IN(G);
-  const long long o = (long long)k * G.batch + in;
-  const double a = S.alpha[o], sg = S.sigbar[in];
+  const long long o_ = (long long)k * G.batch + blockIdx.y;
+  const double a = S.alpha[o_], sg = S.sigbar[blockIdx.y];
   const bool scale = k + 1 < Kin;
-  const double bs = scale ? S.beta[o + G.batch] : 0.0;
-  auto SV = [&](int o) -> double { return o < 0 ? 0.0 : s[base + o]; };
-  auto RB = [&](int o) -> double { return o < 0 ? 0.0 : rbar[base + o]; };
-  double prod = 0.0;
-  if (inb) {
-    const double sc = SV(off), sw = SV(ow), se = SV(oe), ss = SV(os), sn = SV(on);
-    auto QB = [&](double sv, double rv) -> double { return sub(mul(sg, sv), mul(a, rv)); };
-    const double qc = QB(sc, RB(off)), qw = QB(sw, RB(ow)), qe = QB(se, RB(oe)), qs = QB(ss, RB(os)),
-                 qn = QB(sn, RB(on));
-    double sb = scale ? mul(bs, sbar[p]) : sbar[p];
-    sb = add(add(sb, mul(a, xbar[p])), mul(sg, q[p]));
-    sb = add(sb, opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], qw, qe, qs, qn, qc));
-    sbar[p] = sb;
-    qb[p] = qc;
-    prod = mul(sb, sp[p]);
+  const double bs = scale ? S.beta[o_ + G.batch] : 0.0;
+  MARCH_BEGIN
+    auto SV = [&](int o) -> double { return o < 0 ? 0.0 : s[base + o]; };
+    auto RB = [&](int o) -> double { return o < 0 ? 0.0 : rbar[base + o]; };
+    double prod = 0.0;
+    if (inb) {
+      const double sc = SV(off), sw = SV(ow), se = SV(oe), ss = SV(os), sn = SV(on);
+      auto QB = [&](double sv, double rv) -> double { return sub(mul(sg, sv), mul(a, rv)); };
+      const double qc = QB(sc, RB(off)), qw = QB(sw, RB(ow)), qe = QB(se, RB(oe)), qs = QB(ss, RB(os)),
+                   qn = QB(sn, RB(on));
+      double sb = scale ? mul(bs, sbar[p]) : sbar[p];
+      sb = add(add(sb, mul(a, xbar[p])), mul(sg, q[p]));
+      sb = add(sb, opA(aW[p], aW[p + 1], aS[p], aS[p + tp.npx], aC[p], qw, qe, qs, qn, qc));
+      sbar[p] = sb;
+      qb[p] = qc;
+      prod = mul(sb, sp[p]);
+    }
+    put_prod(0, h, prod);
   }
-  row_sums(G, in, row, inb, prod, 0.0, 1, rs);
+  row_sums(G, in, row0, 1, rs);
 }
 
 // Reverse of iteration k, second half. With zbar = sbar + etabar r_k (formed at each stencil point):
@@ -378,35 +420,42 @@ __global__ void k_rq(Geo G, const double* aW, const double* aS, const double* aC
 //   q_{k-1}) are given, the row sums
 //   of xbar s_{k-1} and rbar q_{k-1} for the reverse of iteration k-1. Those row sums are also formed for the
 //   instances whose last iteration is k-1 (K = k): their reverse starts there, with rbar still 0.
-__global__ void k_rz(Geo G, const double* pW, const double* pS, const double* pC, const double* r, const double* z,
-                     const double* sbar, double* rbar, double* zb, const double* xbar, const double* s1,
-                     const double* q1, double* rs, Scal S, const int* K, int k) {
+__global__ void k_rz(Geo G, const double* __restrict__ pW, const double* __restrict__ pS,
+                     const double* __restrict__ pC, const double* __restrict__ r, const double* __restrict__ z,
+                     const double* __restrict__ sbar, double* __restrict__ rbar, double* __restrict__ zb,
+                     const double* __restrict__ xbar, const double* __restrict__ s1, const double* __restrict__ q1,
+                     double* __restrict__ rs, Scal S, const int* __restrict__ K, int k) {
   const int Kin = K[blockIdx.y];
   const bool live = k < Kin, next = s1 != nullptr && k - 1 < Kin;
   if (!live && !next) return;
-  POINT_IN(G);
-  const double e = live ? S.etabar[in] : 0.0;
-  auto RV = [&](int o) -> double { return o < 0 ? 0.0 : r[base + o]; };
-  auto SB = [&](int o) -> double { return o < 0 ? 0.0 : sbar[base + o]; };
-  double p0 = 0.0, p1 = 0.0;
-  if (inb) {
-    double rb = rbar[p];
-    if (live) {
-      const double rc = RV(off), rw = RV(ow), re = RV(oe), rs_ = RV(os), rn_ = RV(on);
-      auto ZB = [&](double sv, double rv) -> double { return add(sv, mul(e, rv)); };
-      const double zc = ZB(SB(off), rc), zw = ZB(SB(ow), rw), ze = ZB(SB(oe), re), zs = ZB(SB(os), rs_),
-                   zn = ZB(SB(on), rn_);
-      rb = add(rb, mul(e, z[p]));
-      rb = add(rb, opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], zc, zw, ze, zs, zn));
-      rbar[p] = rb;
-      zb[p] = zc;
+  const double e = live ? S.etabar[blockIdx.y] : 0.0;
+  MARCH_BEGIN
+    auto RV = [&](int o) -> double { return o < 0 ? 0.0 : r[base + o]; };
+    auto SB = [&](int o) -> double { return o < 0 ? 0.0 : sbar[base + o]; };
+    double p0 = 0.0, p1 = 0.0;
+    if (inb) {
+      double rb = rbar[p];
+      if (live) {
+        const double rc = RV(off), rw = RV(ow), re = RV(oe), rs_ = RV(os), rn_ = RV(on);
+        auto ZB = [&](double sv, double rv) -> double { return add(sv, mul(e, rv)); };
+        const double zc = ZB(SB(off), rc), zw = ZB(SB(ow), rw), ze = ZB(SB(oe), re), zs = ZB(SB(os), rs_),
+                     zn = ZB(SB(on), rn_);
+        rb = add(rb, mul(e, z[p]));
+        rb = add(rb, opM(pC[p], pW[p], pW[p + 1], pS[p], pS[p + tp.npx], zc, zw, ze, zs, zn));
+        rbar[p] = rb;
+        zb[p] = zc;
+      }
+      if (next) {
+        p0 = mul(xbar[p], s1[p]);
+        p1 = mul(rb, q1[p]);
+      }
     }
     if (next) {
-      p0 = mul(xbar[p], s1[p]);
-      p1 = mul(rb, q1[p]);
+      put_prod(0, h, p0);
+      put_prod(1, h, p1);
     }
   }
-  if (next) row_sums(G, in, row, inb, p0, p1, 2, rs);
+  if (next) row_sums(G, in, row0, 2, rs);
 }
 
 // The edge products of one segment (iterations c0 .. c0 + len - 1), added to the coefficient cotangents once per
@@ -415,9 +464,11 @@ __global__ void k_rz(Geo G, const double* pW, const double* pS, const double* pC
 // the east / north halo face when the point is the last of its row / column (the faces edge_products_kernel
 // writes). qbar_m at qb0 + m vstr, zbar_m at zb0 + m vstr,
 // s_m at s0 + m sstr, r_m at r1 + m sstr (m >= 1) and at r0 (m = 0, the checkpoint).
-__global__ void k_seg_edges(Geo G, int c0, int len, const double* qb0, const double* zb0, long long vstr,
-                            const double* s0, const double* r0, const double* r1, long long sstr, double* gW,
-                            double* gS, double* gC, double* gpW, double* gpS, double* gpC, const int* K) {
+__global__ void k_seg_edges(Geo G, int c0, int len, const double* __restrict__ qb0, const double* __restrict__ zb0,
+                            long long vstr, const double* __restrict__ s0, const double* __restrict__ r0,
+                            const double* __restrict__ r1, long long sstr, double* __restrict__ gW,
+                            double* __restrict__ gS, double* __restrict__ gC, double* __restrict__ gpW,
+                            double* __restrict__ gpS, double* __restrict__ gpC, const int* __restrict__ K) {
   const int Kin = K[blockIdx.y];
   if (c0 >= Kin) return;
   POINT_IN(G);
@@ -426,8 +477,10 @@ __global__ void k_seg_edges(Geo G, int c0, int len, const double* qb0, const dou
   const long long pe_ = p + 1, pn_ = p + tp.npx;
   double aw = gW[p], as = gS[p], ac = gC[p], ae = ie ? gW[pe_] : 0.0, an = jn ? gS[pn_] : 0.0;
   double bw = gpW[p], bs = gpS[p], bc = gpC[p], be = ie ? gpW[pe_] : 0.0, bn = jn ? gpS[pn_] : 0.0;
-  for (int m = len - 1; m >= 0; --m) {
-    if (c0 + m >= Kin) continue;
+  // iterations c0 + m < K only: m runs from min(len, K - c0) - 1 down, with no test inside, so that the loads of
+  // the next iterations are issued ahead of the additions (which stay in order)
+#pragma unroll 2
+  for (int m = min(len, Kin - c0) - 1; m >= 0; --m) {
     {
       const double* u = qb0 + m * vstr + base;
       const double* v = s0 + m * sstr + base;
@@ -624,10 +677,11 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   if (bxe > 1024 || A.batch > 65535) return cudaErrorInvalidValue;
   const dim3 bp(bxp, std::max(1, 384 / bxp)), be(bxe, std::max(1, 384 / bxe));
   const dim3 gp((rows + bp.y - 1) / bp.y, A.batch), ge((tp.T * (tp.nj + 1) + be.y - 1) / be.y, A.batch);
+  const dim3 gm((rows + bp.y * kRows - 1) / (bp.y * kRows), A.batch);   // the marching iteration kernels
   const dim3 gw((rows + 7) / 8, A.batch);
   const int gi = (A.batch + 127) / 128, nbk = (tp.nj + A.rows_per_block - 1) / A.rows_per_block;
   const size_t fold_sh = sizeof(double) * (size_t)tp.T * (nbk + 1);
-  const size_t row_sh = sizeof(double) * 2 * bp.x * bp.y;   // row_sums: two products per thread
+  const size_t row_sh = sizeof(double) * 2 * kRows * bp.x * bp.y;   // row_sums: two products per point
   if (fold_sh > 48 * 1024) return cudaErrorInvalidValue;
   const size_t vb = vecn * sizeof(double);
   cudaError_t e;
@@ -668,7 +722,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   for (int k = 0; k <= Kmax && !A.recorded; ++k) {
     const bool ck = k < Kmax && k % C == 0;
     if (k == Kmax && !A.x_check) break;   // the last updates only move x
-    k_fa<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rcur, q, sprev, A.x_check ? x : nullptr, rnext, z,
+    k_fa<<<gm, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rcur, q, sprev, A.x_check ? x : nullptr, rnext, z,
                                  ck ? ck_r[k / C] : nullptr, ck ? ck_s[k / C] : nullptr, k < Kmax ? rs : nullptr,
                                  S, K, k, k > 0);
     LK();
@@ -676,7 +730,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
     if (k == Kmax) break;
     k_fwd_eta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
     LK();
-    k_fb<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, z, sprev, snew, q, rs, S, K, k);
+    k_fb<<<gm, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, z, sprev, snew, q, rs, S, K, k);
     LK();
     k_fwd_sigma<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
     LK();
@@ -697,11 +751,11 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
     // recompute the segment's r, z, s, q with the recorded alpha and beta (the recording forward's operations)
     for (int m = 0; m < len; ++m) {
       const int k = c0 + m;
-      k_fa<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, m == 0 ? ck_r[seg] : rr(m - 1), m == 0 ? nullptr : sg_q[m - 1],
+      k_fa<<<gm, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, m == 0 ? ck_r[seg] : rr(m - 1), m == 0 ? nullptr : sg_q[m - 1],
                                    nullptr, nullptr, m == 0 ? nullptr : sg_r[m], sg_z[m], nullptr, nullptr, nullptr,
                                    S, K, k, m > 0);
       LK();
-      k_fb<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_z[m], sp(m), sg_s[m], sg_q[m], nullptr, S, K, k);
+      k_fb<<<gm, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_z[m], sp(m), sg_s[m], sg_q[m], nullptr, S, K, k);
       LK();
     }
     // the row sums of alphabar for the segment's last iteration (inside a segment k_rz forms them)
@@ -711,12 +765,12 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
       const int k = c0 + m;
       k_rev_alpha<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rq<<<gp, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_s[m], sg_q[m], xbar, rbar, sbar, sp(m), qb0 + m * vstr,
+      k_rq<<<gm, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_s[m], sg_q[m], xbar, rbar, sbar, sp(m), qb0 + m * vstr,
                                    rs, S, K, k);
       LK();
       k_rev_beta<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
-      k_rz<<<gp, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rr(m), sg_z[m], sbar, rbar, zb0 + m * vstr, xbar,
+      k_rz<<<gm, bp, row_sh, st>>>(G, A.pW, A.pS, A.pC, rr(m), sg_z[m], sbar, rbar, zb0 + m * vstr, xbar,
                                    m > 0 ? sg_s[m - 1] : nullptr, m > 0 ? sg_q[m - 1] : nullptr, rs, S, K, k);
       LK();
     }

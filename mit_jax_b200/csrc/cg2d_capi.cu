@@ -433,12 +433,22 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
   }
 
   const size_t smem = L.smem;
-  int bps = 0;
-  if (solver_occupancy(kp, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
-  if (params->ctas_per_sm > 0 && params->ctas_per_sm < bps) bps = params->ctas_per_sm;
   int dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // FP64 has a kernel built for 1 CTA per SM (no register limit below the SM's) and one for 2 (96 registers a
+  // thread). ctas_per_sm 2 takes the second; 0 takes it when every group has one right-hand side and there are at
+  // least 8 units per SM, where its doubled warps pay for the spills (exact-mode forward solves); otherwise the first.
+  kp.fp64_cps = 1;
+  if (!kp.mixed) {
+    bool one_rhs = true;
+    for (int g = 0; g < ngroups; ++g) one_rhs = one_rhs && groups[g].nrhs == 1;
+    if (params->ctas_per_sm == 2 || (params->ctas_per_sm == 0 && one_rhs && kp.total_units >= 8 * nsm))
+      kp.fp64_cps = 2;
+  }
+  int bps = 0;
+  if (solver_occupancy(kp, smem, &bps) != cudaSuccess || bps < 1) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  if (params->ctas_per_sm > 0 && params->ctas_per_sm < bps) bps = params->ctas_per_sm;
   long long grid = (long long)bps * nsm;
   if (params->grid_ctas > 0 && params->grid_ctas < grid) grid = params->grid_ctas;
   if (grid > kp.total_units) grid = kp.total_units;

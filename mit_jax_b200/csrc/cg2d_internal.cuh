@@ -134,6 +134,7 @@ struct KParams {
   int mixed, serial, rows_per_block, replace_every;
   double replace_above;
   int max_ni;
+  int fp64_cps;             // FP64: the kernel built for 1 or 2 CTAs per SM (96 registers a thread at 2)
   int ch;                   // rows per chunk (<= kWarps)
   int nstage[P_NPASS];      // pipeline depth of each pass kind (1 or 2)
   unsigned stage_bytes;     // bytes of one stage buffer

@@ -1295,8 +1295,8 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
   PROF_ADD(kp, sm, PR_CTRL, t0);
 }
 
-template <bool MIXED, int MAXM, bool ONE>
-__global__ void __launch_bounds__(kThreads, MIXED ? 2 : 1) cg2d_persistent(const __grid_constant__ KParams kp) {
+template <bool MIXED, int MAXM, bool ONE, int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_constant__ KParams kp) {
   const Smem sm = carve(kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
   unsigned target = (unsigned)kp.test_missing;
@@ -1623,20 +1623,23 @@ static int grid_for(long long work) {
 }
 
 // the kernel instantiation for a launch: precision, the column steps per row (ceil(max_ni / 32), unrolled for
-// tiles up to 96 and 288 points wide) and whether the launch has a single group
-template <bool ONE>
+// tiles up to 96 and 288 points wide), whether the launch has a single group and, FP64, the CTAs per SM it is
+// built for (MIXED: always 2)
+template <bool ONE, int CPS>
 static const void* solver_fn_of(int mixed, int max_ni) {
   if (mixed) {
-    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE>;
-    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE>;
-    return (const void*)cg2d_persistent<true, 0, ONE>;
+    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE, 2>;
+    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE, 2>;
+    return (const void*)cg2d_persistent<true, 0, ONE, 2>;
   }
-  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE>;
-  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE>;
-  return (const void*)cg2d_persistent<false, 0, ONE>;
+  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE, CPS>;
+  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE, CPS>;
+  return (const void*)cg2d_persistent<false, 0, ONE, CPS>;
 }
 static const void* solver_fn(const KParams& kp) {
-  return kp.ngroups == 1 ? solver_fn_of<true>(kp.mixed, kp.max_ni) : solver_fn_of<false>(kp.mixed, kp.max_ni);
+  const bool two = !kp.mixed && kp.fp64_cps == 2;
+  if (kp.ngroups == 1) return two ? solver_fn_of<true, 2>(kp.mixed, kp.max_ni) : solver_fn_of<true, 1>(kp.mixed, kp.max_ni);
+  return two ? solver_fn_of<false, 2>(kp.mixed, kp.max_ni) : solver_fn_of<false, 1>(kp.mixed, kp.max_ni);
 }
 
 cudaError_t solver_occupancy(const KParams& kp, size_t smem, int* blocks_per_sm) {
