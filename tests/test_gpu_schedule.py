@@ -53,6 +53,22 @@ def test_every_candidate_schedule_is_bitwise_equal(workload, precision):
     assert ran >= 12
 
 
+def test_fp64_builds_for_one_and_two_ctas_per_sm_are_bitwise_equal():
+    """One right-hand side, batch 8 LLC90 (1248 work units, at least 8 per SM): the default launch takes the FP64
+    build for 2 CTAs per SM (96 registers a thread), ctas_per_sm 1 the build for one CTA per SM and ctas_per_sm 2
+    the first again. Solutions and diagnostics are the same bit for bit."""
+    syn, B = make_batch(90, 8)
+    dev = torch.device("cuda")
+    ex = cg.default_exchanger(syn.L)
+    ops = tuple(torch.as_tensor(B[k]).to(dev) for k in cg.OPS)
+    b = torch.as_tensor(B["b"]).to(dev)
+    G = cg.GroupSpec(ex, ops, [b], [torch.zeros_like(b)], [1e-12], [300], torch.as_tensor(B["cg2dNorm"]).to(dev))
+    ref = cg.solve_groups([G], precision="f64")
+    assert all(r["status"] == "ok" for r in cg.diag_records(ref[0][0][2]))
+    for cps in (1, 2):
+        _same(ref, cg.solve_groups([G], precision="f64", ctas_per_sm=cps))
+
+
 def test_tune_picks_a_candidate_and_caches_it(workload, monkeypatch):
     _, G = workload
     monkeypatch.delenv("MIT_JAX_B200_TUNE_CACHE", raising=False)
