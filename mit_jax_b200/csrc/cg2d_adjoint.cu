@@ -458,17 +458,18 @@ __global__ void k_rz(Geo G, const double* __restrict__ pW, const double* __restr
   if (next) row_sums(G, in, row0, 2, rs);
 }
 
-// The edge products of one segment (iterations c0 .. c0 + len - 1), added to the coefficient cotangents once per
-// point: gA += qbar_k (x) s_k and gM += zbar_k (x) r_k for k from the last iteration down, the same terms in the
-// same order as adding them one iteration at a time: the west and south faces of the point, its diagonal entry, and
-// the east / north halo face when the point is the last of its row / column (the faces edge_products_kernel
-// writes). qbar_m at qb0 + m vstr, zbar_m at zb0 + m vstr,
-// s_m at s0 + m sstr, r_m at r1 + m sstr (m >= 1) and at r0 (m = 0, the checkpoint).
-__global__ void k_seg_edges(Geo G, int c0, int len, const double* __restrict__ qb0, const double* __restrict__ zb0,
-                            long long vstr, const double* __restrict__ s0, const double* __restrict__ r0,
-                            const double* __restrict__ r1, long long sstr, double* __restrict__ gW,
-                            double* __restrict__ gS, double* __restrict__ gC, double* __restrict__ gpW,
-                            double* __restrict__ gpS, double* __restrict__ gpC, const int* __restrict__ K) {
+// The edge products of one segment (iterations c0 .. c0 + len - 1) for one operator, added to its coefficient
+// cotangents once per point: gA += qbar_k (x) s_k (M false) or gM += zbar_k (x) r_k (M true) for k from the last
+// iteration down, the same terms in the same order as adding them one iteration at a time: the west and south faces
+// of the point, its diagonal entry, and the east / north halo face when the point is the last of its row / column
+// (the faces edge_products_kernel writes). The cotangent u_m (qbar_m or zbar_m) is at u0 + m vstr; the stencil
+// input (s_m or r_m) at v0 + m sstr for s, and for r at v0 (m = 0, the checkpoint) and v1 + m sstr (m >= 1).
+// The two operators run as two launches, so that each thread holds one set of accumulators (more CTAs per SM).
+template <bool M>
+__global__ void k_seg_edges(Geo G, int c0, int len, const double* __restrict__ u0, long long vstr,
+                            const double* __restrict__ v0, const double* __restrict__ v1, long long sstr,
+                            double* __restrict__ gW, double* __restrict__ gS, double* __restrict__ gC,
+                            const int* __restrict__ K) {
   const int Kin = K[blockIdx.y];
   if (c0 >= Kin) return;
   POINT_IN(G);
@@ -476,38 +477,23 @@ __global__ void k_seg_edges(Geo G, int c0, int len, const double* __restrict__ q
   const bool ie = i == tp.ni - 1, jn = j == tp.nj - 1;
   const long long pe_ = p + 1, pn_ = p + tp.npx;
   double aw = gW[p], as = gS[p], ac = gC[p], ae = ie ? gW[pe_] : 0.0, an = jn ? gS[pn_] : 0.0;
-  double bw = gpW[p], bs = gpS[p], bc = gpC[p], be = ie ? gpW[pe_] : 0.0, bn = jn ? gpS[pn_] : 0.0;
   // iterations c0 + m < K only: m runs from min(len, K - c0) - 1 down, with no test inside, so that the loads of
   // the next iterations are issued ahead of the additions (which stay in order)
 #pragma unroll 2
   for (int m = min(len, Kin - c0) - 1; m >= 0; --m) {
-    {
-      const double* u = qb0 + m * vstr + base;
-      const double* v = s0 + m * sstr + base;
-      auto V = [&](int o) -> double { return o < 0 ? 0.0 : v[o]; };
-      const double uc = u[off], vc = v[off];
-      aw = aw + add(mul(uc, V(ow)), i >= 1 ? mul(u[off - 1], vc) : 0.0);
-      as = as + add(mul(uc, V(os)), j >= 1 ? mul(u[off - tp.npx], vc) : 0.0);
-      ac = ac + mul(uc, vc);
-      if (ie) ae = ae + mul(uc, V(oe));
-      if (jn) an = an + mul(uc, V(on));
-    }
-    {
-      const double* u = zb0 + m * vstr + base;
-      const double* v = (m == 0 ? r0 : r1 + m * sstr) + base;
-      auto V = [&](int o) -> double { return o < 0 ? 0.0 : v[o]; };
-      const double uc = u[off], vc = v[off];
-      bw = bw + add(mul(uc, V(ow)), i >= 1 ? mul(u[off - 1], vc) : 0.0);
-      bs = bs + add(mul(uc, V(os)), j >= 1 ? mul(u[off - tp.npx], vc) : 0.0);
-      bc = bc + mul(uc, vc);
-      if (ie) be = be + mul(uc, V(oe));
-      if (jn) bn = bn + mul(uc, V(on));
-    }
+    const double* u = u0 + m * vstr + base;
+    const double* v = (M ? (m == 0 ? v0 : v1 + m * sstr) : v0 + m * sstr) + base;
+    auto V = [&](int o) -> double { return o < 0 ? 0.0 : v[o]; };
+    const double uc = u[off], vc = v[off];
+    aw = aw + add(mul(uc, V(ow)), i >= 1 ? mul(u[off - 1], vc) : 0.0);
+    as = as + add(mul(uc, V(os)), j >= 1 ? mul(u[off - tp.npx], vc) : 0.0);
+    ac = ac + mul(uc, vc);
+    if (ie) ae = ae + mul(uc, V(oe));
+    if (jn) an = an + mul(uc, V(on));
   }
   gW[p] = aw; gS[p] = as; gC[p] = ac;
-  gpW[p] = bw; gpS[p] = bs; gpC[p] = bc;
-  if (ie) { gW[pe_] = ae; gpW[pe_] = be; }
-  if (jn) { gS[pn_] = an; gpS[pn_] = bn; }
+  if (ie) gW[pe_] = ae;
+  if (jn) gS[pn_] = an;
 }
 
 // coefficient cotangents of a stencil application out = C v: gW/gS/gC += sign (u (x) v) on the faces and points
@@ -774,8 +760,9 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
                                    m > 0 ? sg_s[m - 1] : nullptr, m > 0 ? sg_q[m - 1] : nullptr, rs, S, K, k);
       LK();
     }
-    k_seg_edges<<<gp, bp, 0, st>>>(G, c0, len, qb0, zb0, vstr, sg_s[0], ck_r[seg], sg_r[0], sstr, A.gW, A.gS, A.gC,
-                                   A.gpW, A.gpS, A.gpC, K);
+    k_seg_edges<false><<<gp, bp, 0, st>>>(G, c0, len, qb0, vstr, sg_s[0], nullptr, sstr, A.gW, A.gS, A.gC, K);
+    LK();
+    k_seg_edges<true><<<gp, bp, 0, st>>>(G, c0, len, zb0, vstr, ck_r[seg], sg_r[0], sstr, A.gpW, A.gpS, A.gpC, K);
     LK();
   }
   // r_0 = b_n - A x0_n: the cotangents of b and, through x0_n, of A
