@@ -67,7 +67,9 @@ typedef struct {
   int replace_every;   /* MIXED: FP64 true-residual replacement period in iterations (default 25) */
   double replace_above;/* MIXED: replace only while the residual is above replace_above * tolerance (default 100) */
   int grid_ctas;       /* 0 = as many as can be co-resident (capped by the work units) */
-  int ctas_per_sm;     /* 0 = occupancy maximum */
+  int ctas_per_sm;     /* 0 = occupancy maximum. FP64 has two kernel builds: for 1 CTA per SM and for 2 (fewer
+                          registers a thread). 2 takes the second; 0 takes it when every group has one right-hand
+                          side and there are at least 8 work units per SM, otherwise the first. Results-neutral */
   double timeout_s;    /* bound on every grid-wide wait (default 10 s) */
   int test_missing_arrivals; /* testing only (default 0): the first grid-wide wait expects this many
                                 arrivals more than there are CTAs, so it runs out after timeout_s and
