@@ -516,13 +516,14 @@ def exact_algorithmic_bytes(iters, checkpoint):
 
 
 def exact_launches(kmax, checkpoint):
-    """Kernels cg2d_adjoint_exact launches for a batch whose largest iteration count is kmax (memsets and
-    device-to-device copies excluded): setup and init, 8 per recorded iteration, the cotangent scaling, 3 or 4 per
-    recomputed iteration (the last of a segment needs no new residual), 10 per reversed iteration, and the two
-    closing kernels."""
+    """Kernels one cg2d_solve_exact call launches for a batch whose largest iteration count is kmax (memsets
+    excluded): the coefficient pack and the solve; set-up, neighbour table, r_0 and the scalars from the solve's
+    sums; the cotangent scaling; per iteration two recompute kernels (k_fa, k_fb) and four reverse kernels
+    (k_rev_alpha, k_rq, k_rev_beta, k_rz); per segment the alphabar row dots and the two edge-product launches; and
+    the two closing kernels."""
     C = checkpoint if checkpoint > 0 else max(1, kmax)
     nseg = -(-kmax // C) if kmax else 0
-    return 2 + 8 * kmax + 1 + (4 * kmax - nseg) + 10 * kmax + 2
+    return 2 + 4 + 1 + 6 * kmax + 3 * nseg + 2
 
 
 def _cpu_exact(B, syn, member, iters):
@@ -654,7 +655,7 @@ def run_exact(a):
                      "kernel_ms": ms, "algorithmic_bytes_per_launch": alg},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "gpu_launches": a.steps * (1 + exact_launches(max(iters), a.checkpoint)),
+        "gpu_launches": a.steps * exact_launches(max(iters), a.checkpoint),
         "clocks": clocks,
         "memory": {"peak_allocated_bytes": int(peak_alloc), "resident_inputs_bytes": int(resident),
                    "workspace_bytes": int(ws_bytes)},
