@@ -233,11 +233,16 @@ cg2d_status_t cg2d_solve_exact(const cg2d_topology_t* topo, int batch, double cg
  * JAX arrays are allocated by XLA). For callers that cannot allocate device memory where they solve: a step
  * inside a framework that owns the whole device pool and hands a custom call only its operands, or code that
  * must not let a cudaMalloc synchronise the device. The workspace is a fixed array of
- * CG2D_NOALLOC_SCRATCH_BYTES in the library's device memory, held by every GPU that loads the library until the
- * process exits (enough for two LLC90 solves in FP64). A solve needing more returns CG2D_WORKSPACE_TOO_SMALL.
- * The topology is created beforehand (cg2d_topology_create allocates); inputs and outputs are the caller's, as
- * for cg2d_solve_f64. The first call on a device looks up the array's device address (with that device
- * current); make it before any stream capture. All calls on a device share the array: calls that overlap on
+ * CG2D_NOALLOC_SCRATCH_BYTES in the library's device memory (enough for two LLC90 solves in FP64). A solve needing
+ * more returns CG2D_WORKSPACE_TOO_SMALL. The array is reserved on a device when the library's device code is
+ * loaded there; under CUDA's lazy module loading (the default) that happens in the FIRST call of this entry point
+ * on the device, which also looks up the array's device address (with that device current). So make the first
+ * call at start-up: before a framework reserves its memory pool (or it may fail with CG2D_CUDA_ERROR, out of
+ * memory) and before any stream capture. Later calls reserve nothing; the device holds the array until the
+ * process exits. The address is looked up again in a new context (after cudaDeviceReset). params->profile must
+ * be 0 (CG2D_BAD_ARG otherwise: the profile would land in the hidden array); other invalid arguments give the
+ * status cg2d_solve_f64 gives. The topology is created beforehand (cg2d_topology_create allocates); inputs and
+ * outputs are the caller's, as for cg2d_solve_f64. All calls on a device share the array: calls that overlap on
  * the GPU (other streams, other threads) race and give wrong results; serialise them. */
 #define CG2D_NOALLOC_SCRATCH_BYTES (32u << 20)
 cg2d_status_t cg2d_solve_f64_noalloc(const cg2d_topology_t* topo, int batch, double cg2dNorm,

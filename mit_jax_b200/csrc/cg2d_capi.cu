@@ -817,27 +817,67 @@ cg2d_status_t cg2d_pressure_post(const cg2d_topology_t* topo, int batch, const d
 // solver step running inside a framework that owns the whole device pool (an XLA custom call handed only its
 // operands, a model step under a memory-capped allocator), or code where a cudaMalloc would synchronise the
 // device and stall its other streams. They use this entry point, whose workspace is a fixed array in the
-// library's device memory. Every GPU that loads the library holds CG2D_NOALLOC_SCRATCH_BYTES for it until the
-// process exits; all calls on a device share it.
+// library's device memory. The array is reserved on a device when the module holding it is loaded there: with
+// CUDA's lazy module loading (the default) that is the first call of this entry point on the device, which may
+// fail with an out-of-memory error if a framework has taken the whole pool by then, so make that first call at
+// start-up. From then on the device holds CG2D_NOALLOC_SCRATCH_BYTES for it until the process exits, and calls
+// reserve nothing more; all calls on a device share it.
 namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CG2D_NOALLOC_SCRATCH_BYTES];
 
-// device address of g_noalloc_scratch, looked up once per device (with that device current)
+// Device address of g_noalloc_scratch, looked up with the device current and kept per device together with the
+// unique ID of the context it was looked up in (cuCtxGetId, reached through the runtime's driver entry points so
+// that the library needs no link to libcuda). A context created after a cudaDeviceReset has a new ID, so the
+// address is looked up again there instead of reusing one from the destroyed context. The first lookup in a
+// context loads the library's device module under lazy loading, which reserves the array.
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_ptr[kMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {};
+
+using CtxGetCurrentFn = int (*)(void**);
+using CtxGetIdFn = int (*)(void*, unsigned long long*);
+
+// ID of the current context, 0 when there is none or the driver does not report IDs (then every call looks the
+// address up again, which allocates nothing once the module is loaded)
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_cur || !get_id || get_cur(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 
 cg2d_status_t noalloc_scratch(void** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  unsigned long long id = current_ctx_id();
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
-    g_noalloc_ptr[dev] = p;
+  if (id != 0 && g_noalloc_ptr[dev] && g_noalloc_ctx[dev] == id) {
+    *out = g_noalloc_ptr[dev];
+    return CG2D_OK;
   }
-  *out = g_noalloc_ptr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) { cudaGetLastError(); return CG2D_CUDA_ERROR; }
+  if (id == 0) id = current_ctx_id();   // the lookup made the device's primary context current
+  g_noalloc_ptr[dev] = p;
+  g_noalloc_ctx[dev] = id;
+  *out = p;
   return CG2D_OK;
 }
 
@@ -865,8 +905,11 @@ cg2d_status_t cg2d_solve_f64_noalloc(const cg2d_topology_t* topo, int batch, dou
   g.tolerance[0] = tolerance;
   g.max_iters[0] = max_iters;
   // the workspace this solve needs must fit the fixed array
+  // phase profiles would be written into the hidden array, where no caller can read them back
+  if (params && params->profile) return CG2D_BAD_ARG;
   const size_t need = cg2d_workspace_size(&g, 1, params);
-  if (need == 0) return CG2D_BAD_ARG;
+  // arguments the solver rejects: the same status as cg2d_solve_f64 (the checks run before the workspace is used)
+  if (need == 0) return cg2d_solve_groups(&g, 1, params, nullptr, 0, stream);
   if (need > (size_t)CG2D_NOALLOC_SCRATCH_BYTES) return CG2D_WORKSPACE_TOO_SMALL;
   void* ws = nullptr;
   const cg2d_status_t st = noalloc_scratch(&ws);
