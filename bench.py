@@ -239,6 +239,22 @@ def algorithmic_bytes(diag_f, diag_a, precision):
     return tot
 
 
+def error_vs_fp64(cg, G, slots, L, a):
+    """Every member's error against FP64: the same group solved once more in FP64 (ROWBLOCK order, which the tests
+    tie to the reference's own solution), outside the timed region; per right-hand side the relative max-norm error
+    over the interior, max |x - x64| / max |x64|, for every member (forward x and adjoint lam)."""
+    (ref,) = cg.solve_groups([G], precision="f64", check_status=False)
+    J, I = L.interior
+    out = {}
+    for name, (got, want) in zip(("x", "lam"), ((slots[0][0], ref[0][0]), (slots[1][0], ref[1][0]))):
+        g, r = got[:, :, J, I], want[:, :, J, I]
+        err = ((g - r).abs().amax(dim=(1, 2, 3)) / r.abs().amax(dim=(1, 2, 3))).cpu().numpy()
+        out[f"{name}_max"] = float(err.max())
+        out[f"{name}_per_member"] = [float(f"{e:.2e}") for e in err]
+    out["reference"] = "FP64 ROWBLOCK solve of every member, same tolerance (tests tie it to the reference's x)"
+    return out
+
+
 def _gpu_uuid(torch, dev):
     """The device's UUID as nvidia-smi -i accepts it (falls back to the ordinal)."""
     u = getattr(torch.cuda.get_device_properties(dev), "uuid", None)
@@ -328,6 +344,7 @@ def run_gpu(a):
     diag_f = cg.diag_records(slots[0][2])
     diag_a = cg.diag_records(slots[1][2])
     bad = [d for d in diag_f + diag_a if d["status"] != "ok"]
+    err_fp64 = error_vs_fp64(cg, G, slots, syn.L, a) if a.precision == "mixed" else None
     alg = algorithmic_bytes(diag_f, diag_a, a.precision)
     peak, peak_kind = measured_peak()
     solver_mean = statistics.mean(solver_ms)
@@ -474,6 +491,7 @@ def run_gpu(a):
                            "fwd_min": min(d["numIters"] for d in diag_f), "fwd_max": max(d["numIters"] for d in diag_f),
                            "replacements_mean": statistics.mean(d["replacements"] for d in diag_f + diag_a),
                            "not_ok": len(bad)},
+            "err_vs_fp64": err_fp64,
             "edge_products_ms": statistics.mean(edge_ms),
             "phases_ms": phases,
             "schedule": {"chosen": sched or "library default", "launch": "eager" if a.no_graph else "CUDA graph replay",

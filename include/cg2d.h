@@ -287,6 +287,16 @@ cg2d_status_t cg2d_pressure_rhs(const cg2d_topology_t* topo, int batch, const cg
                                 const double* dyG, const double* dxG, const double* rA, const double* maskInC,
                                 const double* Bo_surf, double* cg2d_b, double* cg2d_x, cg2d_stream_t stream);
 
+/* ini_cg2d_norm (mitgcm_jax/core/cg2d.py:108-134, ini_cg2d.F:90-135), once at set-up: per instance cg2dNorm =
+ * 1 / max over the interior faces of |aW|, |aS| of the un-normalised operator, aW = the sum over k = 1..Nr in order
+ * of implicSurfPress implicDiv2DFlow dyG drF(k) hFacW(k) recip_dxC (aS likewise with dxG, hFacS, recip_dyC), 1 where
+ * the maximum is 0. hFacW, hFacS: the initial face fractions [batch][T][Nr][ny][nx]; grid fields drF [Nr] and dyG,
+ * dxG, recip_dxC, recip_dyC [T][ny][nx]; cg2dNorm: device [batch], written. Bit for bit the reference's value. */
+cg2d_status_t cg2d_ini_norm(const cg2d_topology_t* topo, int batch, int Nr, double implicSurfPress,
+                            double implicDiv2DFlow, const double* hFacW, const double* hFacS, const double* drF,
+                            const double* dyG, const double* dxG, const double* recip_dxC, const double* recip_dyC,
+                            double* cg2dNorm, cg2d_stream_t stream);
+
 /* After the solve (solve_for_pressure.py:116-121): etaN = recip_Bo x, x the solution on the interior and, on halo
  * points, its exchanged value, or the first guess cg2d_x where the exchange writes nothing. recip_Bo is a grid
  * field [T][ny][nx]. */

@@ -36,7 +36,7 @@ EXPORTED = ("cg2d_topology_create", "cg2d_topology_destroy", "cg2d_default_param
             "cg2d_solve_f64_noalloc", "cg2d_adjoint_exact", "cg2d_adjoint_exact_workspace_size",
             "cg2d_update_operator", "cg2d_pressure_rhs", "cg2d_pressure_post", "cg2d_solve_mixed",
             "cg2d_adjoint_ecco_workspace_size", "cg2d_adjoint_ecco", "cg2d_solve_exact_workspace_size",
-            "cg2d_solve_exact")
+            "cg2d_solve_exact", "cg2d_ini_norm")
 
 
 class Params(ctypes.Structure):
@@ -136,6 +136,8 @@ def lib():
     L.cg2d_pressure_rhs.restype = i
     L.cg2d_pressure_post.argtypes = [_P, i, _P, _P, _P, _P, _P]
     L.cg2d_pressure_post.restype = i
+    L.cg2d_ini_norm.argtypes = [_P, i, i, d, d] + [_P] * 8 + [_P]
+    L.cg2d_ini_norm.restype = i
     L.cg2d_status_string.argtypes = [i]
     L.cg2d_status_string.restype = ctypes.c_char_p
     _LIB = L

@@ -801,6 +801,22 @@ cg2d_status_t cg2d_pressure_rhs(const cg2d_topology_t* topo, int batch, const cg
   return CG2D_OK;
 }
 
+cg2d_status_t cg2d_ini_norm(const cg2d_topology_t* topo, int batch, int Nr, double implicSurfPress,
+                             double implicDiv2DFlow, const double* hFacW, const double* hFacS, const double* drF,
+                             const double* dyG, const double* dxG, const double* recip_dxC, const double* recip_dyC,
+                             double* cg2dNorm, cg2d_stream_t stream) {
+  if (!topo || batch < 1 || batch > 65535 || Nr < 1) return CG2D_BAD_ARG;
+  for (const void* q : {(const void*)hFacW, (const void*)hFacS, (const void*)drF, (const void*)dyG, (const void*)dxG,
+                        (const void*)recip_dxC, (const void*)recip_dyC, (const void*)cg2dNorm})
+    if (!q) return CG2D_BAD_ARG;
+  if (pressure_ini_norm(topo_dev(topo), batch, Nr, implicSurfPress, implicDiv2DFlow, hFacW, hFacS, drF, dyG, dxG,
+                        recip_dxC, recip_dyC, cg2dNorm, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) {
+    cudaGetLastError();
+    return CG2D_CUDA_ERROR;
+  }
+  return CG2D_OK;
+}
+
 cg2d_status_t cg2d_pressure_post(const cg2d_topology_t* topo, int batch, const double* x, const double* cg2d_x,
                                  const double* recip_Bo, double* etaN, cg2d_stream_t stream) {
   if (!topo || batch < 1 || batch > 65535 || !x || !cg2d_x || !recip_Bo || !etaN || etaN == x || etaN == cg2d_x)

@@ -223,5 +223,9 @@ cudaError_t pressure_update(const TopoDev& tp, const UpdateArgs& U, cudaStream_t
 cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st);
 cudaError_t pressure_post(const TopoDev& tp, int batch, const double* x, const double* cg2d_x,
                           const double* recip_Bo, double* etaN, cudaStream_t st);
+cudaError_t pressure_ini_norm(const TopoDev& tp, int batch, int Nr, double implicSurfPress, double implicDiv2DFlow,
+                              const double* hFacW, const double* hFacS, const double* drF, const double* dyG,
+                              const double* dxG, const double* recip_dxC, const double* recip_dyC, double* norm,
+                              cudaStream_t st);
 
 }  // namespace cg2d

@@ -3,7 +3,8 @@
 //                the face areas, its diagonal exchanged, and the preconditioner pW, pS, pC;
 //   cg2d_rhs     (solve_for_pressure.py:68-106): the right-hand side (fresh-water flux, the divergence of the g-hat
 //                transports summed from level Nr up to 1, the exactConserv etaH term) and the first guess;
-//   post-solve   (solve_for_pressure.py:116-121): the exchange of the solution and etaN = recip_Bo x.
+//   post-solve   (solve_for_pressure.py:116-121): the exchange of the solution and etaN = recip_Bo x;
+// and, once at set-up, ini_cg2d_norm (mitgcm_jax/core/cg2d.py:108-134): cg2dNorm from the initial face fractions.
 // Every operation is the reference's, in its order, without contraction (__dmul_rn / __dadd_rn / __ddiv_rn), so
 // results are bit for bit those of the reference. The vertical factors deepFacC, rhoFacC, deepFac2F are all 1 in
 // the reference (free_surface.py:121-125); the products with them are exact and are left out.
@@ -190,6 +191,52 @@ __global__ void k_post(TopoDev tp, const double* x, const double* cg2d_x, const 
   }
 }
 
+// ini_cg2d_norm (mitgcm_jax/core/cg2d.py:108-134, ini_cg2d.F:90-135), first kernel: per instance, the maximum over
+// the interior faces of |aW| and |aS|, aW = sum over k = 1..Nr in order of ((fac ((dyG drF(k)) hFacW(k))) recip_dxC),
+// fac = implicSurfPress implicDiv2DFlow, aS likewise with dxG, hFacS, recip_dyC. The maximum is order-free; it is
+// taken on the IEEE bits of the magnitudes (non-negative doubles order as their bits do) in bits[in], zeroed first.
+__global__ void k_ini_norm_max(TopoDev tp, int Nr, const double* hFacW, const double* hFacS, const double* drF,
+                               const double* dyG, const double* dxG, const double* rdxC, const double* rdyC,
+                               double fac, unsigned long long* bits) {
+  const int in = blockIdx.y;
+  const int plane = tp.npy * tp.npx;
+  unsigned long long m = 0ull;
+  FOR_Q(tp) {
+    const Pt p = decode(tp, q);
+    if (interior(tp, p)) {
+      const long long b3 = ((long long)in * tp.T + p.t) * Nr * plane + (q - p.t * plane);
+      const double* __restrict__ hw = hFacW + b3;
+      const double* __restrict__ hs = hFacS + b3;
+      const double dy = dyG[q], dx = dxG[q], rx = rdxC[q], ry = rdyC[q];
+      double w = 0.0, s = 0.0;
+#pragma unroll 5
+      for (int k = 0; k < Nr; ++k) {
+        const double d = __ldg(drF + k);
+        const double hwk = __ldg(hw + (long long)k * plane), hsk = __ldg(hs + (long long)k * plane);
+        w = add(w, mul(mul(fac, mul(mul(dy, d), hwk)), rx));
+        s = add(s, mul(mul(fac, mul(mul(dx, d), hsk)), ry));
+      }
+      const unsigned long long bw = (unsigned long long)__double_as_longlong(fabs(w));
+      const unsigned long long bs = (unsigned long long)__double_as_longlong(fabs(s));
+      m = bw > m ? bw : m;
+      m = bs > m ? bs : m;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
+    m = y > m ? y : m;
+  }
+  if ((threadIdx.x & 31) == 0 && m != 0ull) atomicMax(bits + in, m);
+}
+
+// second kernel: cg2dNorm = 1 / myNorm, 1 where myNorm is 0 (cg2d.py:131-134), in place over the bits
+__global__ void k_ini_norm_fin(int batch, unsigned long long* bits) {
+  const int in = blockIdx.x * blockDim.x + threadIdx.x;
+  if (in >= batch) return;
+  const double my = __longlong_as_double((long long)bits[in]);
+  reinterpret_cast<double*>(bits)[in] = my != 0.0 ? dvd(1.0, my) : 1.0;
+}
+
 dim3 grid_of(const TopoDev& tp, int batch) {
   const int pe = tp.T * tp.npy * tp.npx;
   return dim3((unsigned)((pe + 255) / 256), (unsigned)batch);
@@ -231,6 +278,23 @@ cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st) {
   A.fresh_water = R.useRealFreshWaterFlux;
   A.Nr = R.Nr;
   k_rhs<<<grid_of(tp, R.batch), 256, 0, st>>>(tp, A, R.cg2d_b, R.cg2d_x);
+  return cudaGetLastError();
+}
+
+cudaError_t pressure_ini_norm(const TopoDev& tp, int batch, int Nr, double implicSurfPress, double implicDiv2DFlow,
+                              const double* hFacW, const double* hFacS, const double* drF, const double* dyG,
+                              const double* dxG, const double* recip_dxC, const double* recip_dyC, double* norm,
+                              cudaStream_t st) {
+  if (batch < 1 || batch > 65535 || Nr < 1) return cudaErrorInvalidValue;
+  unsigned long long* bits = reinterpret_cast<unsigned long long*>(norm);
+  cudaError_t e = cudaMemsetAsync(bits, 0, sizeof(double) * (size_t)batch, st);
+  if (e != cudaSuccess) return e;
+  // fac = implicSurfPress * implicDiv2DFlow, formed once as the reference does (cg2d.py:124)
+  k_ini_norm_max<<<grid_of(tp, batch), 256, 0, st>>>(tp, Nr, hFacW, hFacS, drF, dyG, dxG, recip_dxC, recip_dyC,
+                                                     implicSurfPress * implicDiv2DFlow, bits);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_ini_norm_fin<<<(batch + 127) / 128, 128, 0, st>>>(batch, bits);
   return cudaGetLastError();
 }
 

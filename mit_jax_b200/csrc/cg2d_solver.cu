@@ -29,6 +29,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "cg2d_internal.cuh"
 
@@ -902,18 +903,69 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
 }
 
 // compute one chunk from its stage buffer: warp w owns row jc + w, lane owns i = lane + 32m, m = 0, 1, ...
-// (MAXM > 0: exactly MAXM column steps, unrolled; 0: any width). Both right-hand sides of the instance are
-// processed in the same step, sharing the coefficient loads. In shared memory point (w, i) of a vector is
-// element (w + 1) P + i + 1 (its neighbours at -1, +1, -P, +P) and of the packed coefficients element
+// (MAXM > 0: exactly MAXM column steps, unrolled; 0: any width). The right-hand sides of the instance active in
+// the pass are processed in the same step, sharing the coefficient loads. In shared memory point (w, i) of a
+// vector is element (w + 1) P + i + 1 (its neighbours at -1, +1, -P, +P) and of the packed coefficients element
 // w 3 ldc + i (columns: W/pW, +ldc S/pS, +2 ldc C/pC; east face +1, north face +3 ldc). A point pushes its new
 // values to the rings of the tiles that read it when it lies on the tile's edge (every point of the first and
 // last row, the first and last point of the others).
-template <bool MIXED, int MAXM, bool ONE>
+//
+// Each lane addresses its rows through base pointers set once per chunk (the point's row and the rows above and
+// below, in shared memory; the output rows in global memory), so that a column step m is an immediate offset.
+// MIXED fuses the FP32 stencils and vector updates (fmaf: a multiply-add rounded once) and the FP64 solution
+// update; the dot products are FP32 products, exact in FP64, accumulated with FP64 fused multiply-adds, which is
+// the same arithmetic as a rounded product and a rounded sum. FP64 rounds every product and every sum as the
+// reference does. SERIAL (the FORTRAN sum order) writes every product into the product rows instead of the lane
+// partials.
+
+template <bool MIXED> struct Ar;
+template <> struct Ar<false> {   // FP64: rounded product, rounded sum (no contraction)
+  __device__ static __forceinline__ double madd(double a, double b, double c) { return add(mul(a, b), c); }
+  __device__ static __forceinline__ double dot(double a, double b, double c) { return add(c, mul(a, b)); }
+};
+template <> struct Ar<true> {    // MIXED: FP32 stencils and updates fused; FP64 solution update and dots fused
+  __device__ static __forceinline__ float madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+  __device__ static __forceinline__ double madd(double a, double b, double c) { return __fma_rn(a, b, c); }
+  __device__ static __forceinline__ double dot(double a, double b, double c) { return __fma_rn(a, b, c); }
+};
+
+// apply_operator / apply_preconditioner with the arithmetic of Ar (same terms in the same order as op_A / op_M)
+template <bool MIXED, class T>
+__device__ __forceinline__ T stencil5(T c0, T c1, T c2, T c3, T c4, T v0, T v1, T v2, T v3, T v4) {
+  using A = Ar<MIXED>;
+  T t = mul(c0, v0);
+  t = A::madd(c1, v1, t);
+  t = A::madd(c2, v2, t);
+  t = A::madd(c3, v3, t);
+  return A::madd(c4, v4, t);
+}
+
+// one right-hand side's rows in a pipelined pass, set once per chunk: the two staged stencil inputs (point row
+// and the rows above and below, shared memory), the global output rows, the pass coefficient and the product rows
+// (SERIAL)
+template <class V>
+struct RowSet {
+  const V *a_c, *a_s, *a_n;      // stencil input 0 (z in S, r in X / Z), rows w, w - 1, w + 1, column of this lane
+  const V *b_c, *b_s, *b_n;      // stencil input 1 (s_{k-1} in S, q_k in X)
+  const double* xo;              // S: staged x_{k-1}, row w, column of this lane
+  V *o1, *o2;                    // S: s_k, q_k; X: r_{k+1}, z_{k+1}; Z: z (o2); rows of this lane's column
+  double* ox;                    // S: x_k
+  double* ck;                    // FP64: the exact-mode checkpoint row of this lane's column, or null
+  double* pr;                    // SERIAL: product rows (kind 0, kind 1 at + kWarps max_ni) of this lane's column
+  V coef;                        // beta_k (S), alpha_k (X)
+  double alpha_prev;             // S: alpha_{k-1}
+  bool upd;                      // S: alpha_{k-1} exists (x update due)
+  V *vs1, *vs2;                  // bases of the output vectors (for the ring pushes)
+  double* vsx;
+};
+
+template <bool MIXED, int MAXM, bool ONE, bool SERIAL>
 __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si, int st,
                                const Smem& sm) {
   Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
   using V = typename Prec<MIXED>::V;
   using C = typename Prec<MIXED>::C;
+  using A = Ar<MIXED>;
   const GroupDev& g = group_of<ONE>(kp, c.gi);
   const TopoDev& tp = g.tp;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -937,174 +989,160 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   const int act0 = si.act(0), act1 = si.act(1);
 
   // pass S after convergence: the pending x update, un-normalised (cg2d.py:254, 266)
-  for (int s = 0; s < g.nrhs; ++s) {
-    if ((s == 0 ? act0 : act1) != A_FIN) continue;
-    const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
-    const double* x = vec_ptr<double>(g, c.inst, s, V_X);
-    for (int i = lane; i < ni; i += 32) {
-      double xv = ldcg(x + grow + i);
-      if (si.has_alpha(s)) xv = add(xv, mul(si.c2(s), (double)ldcg(so + grow + i)));
-      const double xf = __ddiv_rn(xv, si.rnorm(s));
-      g.x_out[s][prow + i] = xf;
-      if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
+  if (pt == P_S && (act0 == A_FIN || act1 == A_FIN)) {
+    for (int s = 0; s < g.nrhs; ++s) {
+      if ((s == 0 ? act0 : act1) != A_FIN) continue;
+      const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
+      const double* x = vec_ptr<double>(g, c.inst, s, V_X);
+      for (int i = lane; i < ni; i += 32) {
+        double xv = ldcg(x + grow + i);
+        if (si.has_alpha(s)) xv = A::madd(si.c2(s), (double)ldcg(so + grow + i), xv);
+        const double xf = __ddiv_rn(xv, si.rnorm(s));
+        g.x_out[s][prow + i] = xf;
+        if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
+      }
     }
   }
   const bool on0 = act0 == A_ACTIVE, on1 = act1 == A_ACTIVE;
   if (!on0 && !on1) return lp;
 
-  // products of slot s at point i into the lane partials (ROWBLOCK) or the product rows (FORTRAN)
-  auto emit = [&](int s, int i, double p0, double p1) {
-    if (kp.serial) {
-      double* pr = sm.prod() + ((s * 2) * kWarps + w) * kp.max_ni;
-      pr[i] = p0;
-      pr[kWarps * kp.max_ni + i] = p1;
-    } else if (s == 0) {
-      lp.v[0] = add(lp.v[0], p0);
-      lp.v[1] = add(lp.v[1], p1);
-    } else {
-      lp.v[2] = add(lp.v[2], p0);
-      lp.v[3] = add(lp.v[3], p1);
-    }
-  };
-  // the same for passes that form one sum per solve (the second kind is never read there)
-  auto emit1 = [&](int s, int i, double p0) {
-    if (kp.serial) sm.prod()[((s * 2) * kWarps + w) * kp.max_ni + i] = p0;
-    else if (s == 0) lp.v[0] = add(lp.v[0], p0);
-    else lp.v[2] = add(lp.v[2], p0);
-  };
-  // runs f(i) for this lane's columns
-  auto columns = [&](auto&& f) {
-    if (MAXM > 0) {
-#pragma unroll
-      for (int m = 0; m < (MAXM > 0 ? MAXM : 1); ++m) {
-        const int i = lane + 32 * m;
-        if (i < ni) f(i);
-      }
-    } else {
-      for (int i = lane; i < ni; i += 32) f(i);
-    }
-  };
-  const C* cp = reinterpret_cast<const C*>(sb + L.coef);
+  // coefficient rows of this lane's column: W (and the east face at +1), S, N (the south face of row w + 1), C
+  const C* cw = reinterpret_cast<const C*>(sb + L.coef) + w * CR + lane;
+  const C* cs = cw + CL;
+  const C* cn = cs + CR;
+  const C* cc = cw + 2 * CL;
+  const int off_c = (w + 1) * P + 1 + lane;   // this lane's column of row w in a staged vector
 
-  if (pt == P_S) {
-    // s_k = z_k + beta_k s_{k-1} (cg2d.py:249), formed for the point and its neighbours alike (MIXED: in FP32);
-    // q_k = A s_k (cg2d.py:251); x_k = x_{k-1} + alpha_{k-1} s_{k-1} (cg2d.py:254); s_k.q_k (cg2d.py:252)
-    struct SlotS {
-      const V *zr, *so;
-      const double* xo;
-      V *s_out, *q_out;
-      double* x_out;
-      double* ck;     // checkpoint of s_k for the exact-mode adjoint, or null
-      V beta;
-      double alpha_prev;
-      bool upd;
-    };
-    auto slot = [&](int s) {
-      SlotS q;
-      q.zr = reinterpret_cast<const V*>(sb + L.vec[s][0]);
-      q.so = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      q.xo = reinterpret_cast<const double*>(sb + L.xo[s]);
-      q.s_out = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0) + grow;
-      q.q_out = vec_ptr<V>(g, c.inst, s, V_Q) + grow;
-      q.x_out = vec_ptr<double>(g, c.inst, s, V_X) + grow;
-      q.beta = (V)si.c1(s);
+  auto rows = [&](int s) {
+    RowSet<V> q;
+    const V* a = reinterpret_cast<const V*>(sb + L.vec[s][0]) + off_c;
+    const V* b = reinterpret_cast<const V*>(sb + L.vec[s][1]) + off_c;
+    q.a_c = a; q.a_s = a - P; q.a_n = a + P;
+    q.b_c = b; q.b_s = b - P; q.b_n = b + P;
+    q.xo = reinterpret_cast<const double*>(sb + L.xo[s]) + w * P + 1 + lane;
+    q.pr = SERIAL ? sm.prod() + ((s * 2) * kWarps + w) * kp.max_ni + lane : nullptr;
+    q.ck = nullptr;
+    q.ox = nullptr;
+    q.vsx = nullptr;
+    q.alpha_prev = 0.0;
+    q.upd = false;
+    if (pt == P_S) {
+      q.vs1 = vec_ptr<V>(g, c.inst, s, (k & 1) ? V_S1 : V_S0);
+      q.vs2 = vec_ptr<V>(g, c.inst, s, V_Q);
+      q.vsx = vec_ptr<double>(g, c.inst, s, V_X);
+      q.ox = q.vsx + grow + lane;
+      q.coef = (V)si.c1(s);
       q.alpha_prev = si.c2(s);
       q.upd = si.has_alpha(s) != 0;
-      q.ck = (!MIXED && kp.ck_s && ((k + 1) % kp.ck_every) == 0) ? kp.ck_s + ((k + 1) / kp.ck_every) * kp.ck_stride
-                                                                 : nullptr;
-      return q;
-    };
-    const SlotS q0 = slot(0), q1 = slot(g.nrhs > 1 ? 1 : 0);
-    auto body = [&](const SlotS& q, int s, int i, int rc, C aw, C ae, C as, C an, C ac, bool edge) {
-      auto sn = [&](V zz, V ss) -> V { return add(zz, mul(q.beta, ss)); };
-      const V vc = sn(q.zr[rc], q.so[rc]);
-      const V vw = sn(q.zr[rc - 1], q.so[rc - 1]);
-      const V ve = sn(q.zr[rc + 1], q.so[rc + 1]);
-      const V vs = sn(q.zr[rc - P], q.so[rc - P]);
-      const V vn = sn(q.zr[rc + P], q.so[rc + P]);
-      const V qv = (V)op_A<C>(aw, ae, as, an, ac, (C)vw, (C)ve, (C)vs, (C)vn, (C)vc);
-      stcg(q.s_out + i, vc);
-      stcg(q.q_out + i, qv);
-      if constexpr (!MIXED) {
-        if (q.ck) q.ck[prow + i] = (double)vc;                                   // checkpoint s_k
-      }
-      double xn = 0.0;
-      if (q.upd) {
-        xn = add(q.xo[w * P + i + 1], mul(q.alpha_prev, (double)q.so[rc]));
-        stcg(q.x_out + i, xn);
-      }
-      if (edge) {
-        push_s(ptab, q.s_out - grow, j, w, i, vc);
-        push_s(ptab, q.q_out - grow, j, w, i, qv);
-        if (MIXED && q.upd) push_s(ptab, q.x_out - grow, j, w, i, xn);   // x's neighbours: replacement pass only
-      }
-      emit1(s, i, mul((double)vc, (double)qv));
-    };
-    columns([&](int i) {
-      const int rc = (w + 1) * P + i + 1;
-      const int cr = w * CR + i;
-      const C aw = cp[cr], ae = cp[cr + 1], as = cp[cr + CL], an = cp[cr + CL + CR], ac = cp[cr + 2 * CL];
+      if (!MIXED && kp.ck_s && ((k + 1) % kp.ck_every) == 0)
+        q.ck = kp.ck_s + ((k + 1) / kp.ck_every) * kp.ck_stride + prow + lane;
+    } else {
+      q.vs1 = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
+      q.vs2 = vec_ptr<V>(g, c.inst, s, V_Z);
+      q.coef = (V)si.c1(s);
+      if (!MIXED && pt == P_X && kp.ck_r && ((k + 1) % kp.ck_every) == 0)
+        q.ck = kp.ck_r + ((k + 1) / kp.ck_every) * kp.ck_stride + prow + lane;
+    }
+    q.o1 = q.vs1 + grow + lane;
+    q.o2 = q.vs2 + grow + lane;
+    return q;
+  };
+
+  // NS right-hand sides q[0..NS-1]; sums into acc[s][kind]
+  auto run = [&](auto ns_tag, const RowSet<V>* q, double (&acc)[2][2]) {
+    constexpr int NS = decltype(ns_tag)::value;
+    auto col = [&](int m) {
+      const int i = lane + 32 * m;
+      const int o = 32 * m;
       const bool edge = er | (i == 0) | (i == ni - 1);
-      if (on0) body(q0, 0, i, rc, aw, ae, as, an, ac, edge);
-      if (on1) body(q1, 1, i, rc, aw, ae, as, an, ac, edge);
-    });
-  } else if (pt == P_X || pt == P_Z) {
-    // X: r_{k+1} = r_k - alpha_k q_k (cg2d.py:255, MIXED: in FP32) at the point and its neighbours;
-    //    z_{k+1} = M r_{k+1} (cg2d.py:245); r.r and z.r (cg2d.py:256, 246)
-    // Z: z = M r and z.r
-    struct SlotX {
-      const V *ro, *qv;
-      V *r_out, *z_out;
-      double* ck;     // checkpoint of r_{k+1} for the exact-mode adjoint, or null
-      V alpha;
-    };
-    const bool xp = pt == P_X;
-    auto slot = [&](int s) {
-      SlotX q;
-      q.ro = reinterpret_cast<const V*>(sb + L.vec[s][0]);
-      q.qv = reinterpret_cast<const V*>(sb + L.vec[s][1]);
-      q.r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0) + grow;
-      q.z_out = vec_ptr<V>(g, c.inst, s, V_Z) + grow;
-      q.alpha = (V)si.c1(s);
-      q.ck = (!MIXED && xp && kp.ck_r && ((k + 1) % kp.ck_every) == 0)
-                 ? kp.ck_r + ((k + 1) / kp.ck_every) * kp.ck_stride : nullptr;
-      return q;
-    };
-    const SlotX q0 = slot(0), q1 = slot(g.nrhs > 1 ? 1 : 0);
-    auto body = [&](const SlotX& q, int s, int i, int rc, C pw, C pe_, C ps, C pn, C pc, bool edge) {
-      V vc, vw, ve, vs, vn;
-      if (xp) {
-        auto rn = [&](V rr, V qq) -> V { return sub(rr, mul(q.alpha, qq)); };
-        vc = rn(q.ro[rc], q.qv[rc]);
-        vw = rn(q.ro[rc - 1], q.qv[rc - 1]);
-        ve = rn(q.ro[rc + 1], q.qv[rc + 1]);
-        vs = rn(q.ro[rc - P], q.qv[rc - P]);
-        vn = rn(q.ro[rc + P], q.qv[rc + P]);
+      if (pt == P_S) {
+        // s_k = z_k + beta_k s_{k-1} (cg2d.py:249) at the point and its neighbours; q_k = A s_k (cg2d.py:251);
+        // x_k = x_{k-1} + alpha_{k-1} s_{k-1} (cg2d.py:254); s_k.q_k (cg2d.py:252)
+        const C aw = cw[o], ae = cw[o + 1], as = cs[o], an = cn[o], ac = cc[o];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const RowSet<V>& r = q[s];
+          const V be = r.coef;
+          const V sp = r.b_c[o];
+          const V vc = A::madd(be, sp, r.a_c[o]);
+          const V vw = A::madd(be, r.b_c[o - 1], r.a_c[o - 1]);
+          const V ve = A::madd(be, r.b_c[o + 1], r.a_c[o + 1]);
+          const V vs = A::madd(be, r.b_s[o], r.a_s[o]);
+          const V vn = A::madd(be, r.b_n[o], r.a_n[o]);
+          const V qv = stencil5<MIXED, C>(aw, ae, as, an, ac, vw, ve, vs, vn, vc);
+          stcg(r.o1 + o, vc);
+          stcg(r.o2 + o, qv);
+          if constexpr (!MIXED) {
+            if (r.ck) r.ck[o] = (double)vc;                                      // checkpoint s_k
+          }
+          double xn = 0.0;
+          if (r.upd) {
+            xn = A::madd(r.alpha_prev, (double)sp, r.xo[o]);
+            stcg(r.ox + o, xn);
+          }
+          if (edge) {
+            push_s(ptab, r.vs1, j, w, i, vc);
+            push_s(ptab, r.vs2, j, w, i, qv);
+            if (MIXED && r.upd) push_s(ptab, r.vsx, j, w, i, xn);   // x's neighbours: replacement pass only
+          }
+          if constexpr (SERIAL) r.pr[o] = mul((double)vc, (double)qv);
+          else acc[s][0] = A::dot((double)vc, (double)qv, acc[s][0]);
+        }
       } else {
-        vc = q.ro[rc]; vw = q.ro[rc - 1]; ve = q.ro[rc + 1]; vs = q.ro[rc - P]; vn = q.ro[rc + P];
+        // X: r_{k+1} = r_k - alpha_k q_k (cg2d.py:255) at the point and its neighbours; z_{k+1} = M r_{k+1}
+        //    (cg2d.py:245); r.r and z.r (cg2d.py:256, 246).  Z: z = M r and z.r
+        const C pw = cw[o], pe_ = cw[o + 1], ps = cs[o], pn = cn[o], pc = cc[o];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const RowSet<V>& r = q[s];
+          V vc, vw, ve, vs, vn;
+          if (pt == P_X) {
+            const V na = -r.coef;
+            vc = A::madd(na, r.b_c[o], r.a_c[o]);
+            vw = A::madd(na, r.b_c[o - 1], r.a_c[o - 1]);
+            ve = A::madd(na, r.b_c[o + 1], r.a_c[o + 1]);
+            vs = A::madd(na, r.b_s[o], r.a_s[o]);
+            vn = A::madd(na, r.b_n[o], r.a_n[o]);
+          } else {
+            vc = r.a_c[o]; vw = r.a_c[o - 1]; ve = r.a_c[o + 1]; vs = r.a_s[o]; vn = r.a_n[o];
+          }
+          const V z = stencil5<MIXED, C>(pc, pw, pe_, ps, pn, vc, vw, ve, vs, vn);
+          if (pt == P_X) stcg(r.o1 + o, vc);
+          if constexpr (!MIXED) {
+            if (r.ck) r.ck[o] = (double)vc;                                      // checkpoint r_{k+1}
+          }
+          stcg(r.o2 + o, z);
+          if (edge) {
+            if (pt == P_X) push_s(ptab, r.vs1, j, w, i, vc);
+            push_s(ptab, r.vs2, j, w, i, z);
+          }
+          if constexpr (SERIAL) {
+            if (pt == P_X) {
+              r.pr[o] = mul((double)vc, (double)vc);
+              r.pr[o + kWarps * kp.max_ni] = mul((double)z, (double)vc);
+            } else {
+              r.pr[o] = mul((double)z, (double)vc);
+            }
+          } else if (pt == P_X) {
+            acc[s][0] = A::dot((double)vc, (double)vc, acc[s][0]);
+            acc[s][1] = A::dot((double)z, (double)vc, acc[s][1]);
+          } else {
+            acc[s][0] = A::dot((double)z, (double)vc, acc[s][0]);
+          }
+        }
       }
-      const V z = (V)op_M<C>(pc, pw, pe_, ps, pn, (C)vc, (C)vw, (C)ve, (C)vs, (C)vn);
-      if (xp) stcg(q.r_out + i, vc);
-      if constexpr (!MIXED) {
-        if (q.ck) q.ck[prow + i] = (double)vc;                                   // checkpoint r_{k+1}
-      }
-      stcg(q.z_out + i, z);
-      if (edge) {
-        if (xp) push_s(ptab, q.r_out - grow, j, w, i, vc);
-        push_s(ptab, q.z_out - grow, j, w, i, z);
-      }
-      if (xp) emit(s, i, mul((double)vc, (double)vc), mul((double)z, (double)vc));
-      else emit1(s, i, mul((double)z, (double)vc));
     };
-    columns([&](int i) {
-      const int rc = (w + 1) * P + i + 1;
-      const int cr = w * CR + i;
-      const C pw = cp[cr], pe_ = cp[cr + 1], ps = cp[cr + CL], pn = cp[cr + CL + CR], pc = cp[cr + 2 * CL];
-      const bool edge = er | (i == 0) | (i == ni - 1);
-      if (on0) body(q0, 0, i, rc, pw, pe_, ps, pn, pc, edge);
-      if (on1) body(q1, 1, i, rc, pw, pe_, ps, pn, pc, edge);
-    });
-  } else {  // P_R: the FP64 true residual b - A x_{k+1}, x_{k+1} = x_k + alpha_k s_k formed on the fly
+    if constexpr (MAXM > 0) {
+#pragma unroll
+      for (int m = 0; m < MAXM; ++m)
+        if (lane + 32 * m < ni) col(m);
+    } else {
+      for (int m = 0; lane + 32 * m < ni; ++m) col(m);
+    }
+  };
+
+  if (pt == P_R) {
+    // the FP64 true residual b - A x_{k+1}, x_{k+1} = x_k + alpha_k s_k formed on the fly (cg2d.py:232, 254)
     const double* aw = reinterpret_cast<const double*>(sb + L.coef);
     const double* as = reinterpret_cast<const double*>(sb + L.coef + L.coef_stride);
     const double* ac = reinterpret_cast<const double*>(sb + L.coef + 2 * L.coef_stride);
@@ -1115,7 +1153,8 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       const V* sk = reinterpret_cast<const V*>(sb + L.vec[s][1]);
       const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
-      auto x1 = [&](double xx, V ss) -> double { return add(xx, mul(alpha, (double)ss)); };
+      double* pr = SERIAL ? sm.prod() + ((s * 2) * kWarps + w) * kp.max_ni : nullptr;
+      auto x1 = [&](double xx, V ss) -> double { return A::madd(alpha, (double)ss, xx); };
       for (int i = lane; i < ni; i += 32) {
         const int rc = (w + 1) * P + i + 1;
         const double vc = x1(xr[rc], sk[rc]);
@@ -1128,9 +1167,25 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
         const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + NP], ac[cr], vw, ve, vs, vn, vc));
         stcg(r_out + grow + i, r);
         if (er | (i == 0) | (i == ni - 1)) push_s(ptab, r_out, j, w, i, r);
-        emit1(s, i, mul((double)r, (double)r));
+        if constexpr (SERIAL) pr[i] = mul((double)r, (double)r);
+        else if (s == 0) lp.v[0] = A::dot((double)r, (double)r, lp.v[0]);
+        else lp.v[2] = A::dot((double)r, (double)r, lp.v[2]);
       }
     }
+    return lp;
+  }
+
+  double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  if (on0 && on1) {
+    const RowSet<V> q[2] = {rows(0), rows(1)};
+    run(std::integral_constant<int, 2>{}, q, acc);
+    lp.v[0] = acc[0][0]; lp.v[1] = acc[0][1]; lp.v[2] = acc[1][0]; lp.v[3] = acc[1][1];
+  } else {
+    const int s = on0 ? 0 : 1;
+    const RowSet<V> q[1] = {rows(s)};
+    run(std::integral_constant<int, 1>{}, q, acc);
+    if (s == 0) { lp.v[0] = acc[0][0]; lp.v[1] = acc[0][1]; }
+    else { lp.v[2] = acc[0][0]; lp.v[3] = acc[0][1]; }
   }
   return lp;
 }
@@ -1210,7 +1265,7 @@ __device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const S
   return ok;
 }
 
-template <bool MIXED, int MAXM, bool ONE>
+template <bool MIXED, int MAXM, bool ONE, bool SERIAL>
 __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, Pipe& pp) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ns = kp.nstage[pt];
@@ -1230,8 +1285,8 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
     const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
     const GroupDev& g = group_of<ONE>(kp, c.gi);
     const Slots si = slots_of(g, c.inst, sm);
-    const Lanes lp = compute_chunk<MIXED, MAXM, ONE>(kp, c, pt, k, si, st, sm);
-    if (warp < c.nr && !kp.serial) row_sums(g, lp, sm, st, pt == P_X);
+    const Lanes lp = compute_chunk<MIXED, MAXM, ONE, SERIAL>(kp, c, pt, k, si, st, sm);
+    if (!SERIAL && warp < c.nr) row_sums(g, lp, sm, st, pt == P_X);
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty()[st]);
     PROF_ADD(kp, sm, PR_COMP, t0);
@@ -1241,11 +1296,11 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
   return true;
 }
 
-template <bool MIXED, int MAXM, bool ONE>
+template <bool MIXED, int MAXM, bool ONE, bool SERIAL>
 __device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const Smem& sm, Pipe& pp) {
   bool ok;
   if ((threadIdx.x >> 5) == kProducer) ok = produce_pass(kp, pt, k, hidx, sm, pp);
-  else ok = consume_pass<MIXED, MAXM, ONE>(kp, pt, k, sm, pp);
+  else ok = consume_pass<MIXED, MAXM, ONE, SERIAL>(kp, pt, k, sm, pp);
   const unsigned long long td = PROF_T0(kp);
   const int bad = __syncthreads_or(!ok);
   PROF_ADD(kp, sm, PR_DRAIN, td);
@@ -1295,7 +1350,7 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
   PROF_ADD(kp, sm, PR_CTRL, t0);
 }
 
-template <bool MIXED, int MAXM, bool ONE, int CPS>
+template <bool MIXED, int MAXM, bool ONE, int CPS, bool SERIAL>
 __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_constant__ KParams kp) {
   const Smem sm = carve(kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
@@ -1352,7 +1407,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
   if (own) S->rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_Z, 0, 0, sm, pp);
+  ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_Z, 0, 0, sm, pp);
   ok = grid_sync(kp, target, P_Z, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
@@ -1376,7 +1431,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
-    ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_S, k, k, sm, pp);
+    ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_S, k, k, sm, pp);
     ok = grid_sync(kp, target, P_S, k, sm) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
@@ -1394,7 +1449,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
     }
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, own ? S->alpha : 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_X, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_X, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_X, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
@@ -1404,7 +1459,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
     }
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, own ? S->alpha : 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_R, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_R, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_R, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
@@ -1412,7 +1467,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
         ++S->nrep;
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM, ONE>(kp, P_Z, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_Z, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_Z, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
@@ -1628,15 +1683,18 @@ static int grid_for(long long work) {
 template <bool ONE, int CPS>
 static const void* solver_fn_of(int mixed, int max_ni) {
   if (mixed) {
-    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE, 2>;
-    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE, 2>;
-    return (const void*)cg2d_persistent<true, 0, ONE, 2>;
+    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE, 2, false>;
+    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE, 2, false>;
+    return (const void*)cg2d_persistent<true, 0, ONE, 2, false>;
   }
-  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE, CPS>;
-  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE, CPS>;
-  return (const void*)cg2d_persistent<false, 0, ONE, CPS>;
+  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE, CPS, false>;
+  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE, CPS, false>;
+  return (const void*)cg2d_persistent<false, 0, ONE, CPS, false>;
 }
 static const void* solver_fn(const KParams& kp) {
+  // the FORTRAN sum order (bitwise parity, not speed): one generic build per precision
+  if (kp.serial) return kp.mixed ? (const void*)cg2d_persistent<true, 0, false, 2, true>
+                                 : (const void*)cg2d_persistent<false, 0, false, 1, true>;
   const bool two = !kp.mixed && kp.fp64_cps == 2;
   if (kp.ngroups == 1) return two ? solver_fn_of<true, 2>(kp.mixed, kp.max_ni) : solver_fn_of<true, 1>(kp.mixed, kp.max_ni);
   return two ? solver_fn_of<false, 2>(kp.mixed, kp.max_ni) : solver_fn_of<false, 1>(kp.mixed, kp.max_ni);

@@ -1,4 +1,7 @@
-"""SOLVE_FOR_PRESSURE on the GPU with the reference's call signatures (mitgcm_jax/core/solve_for_pressure.py):
+"""SOLVE_FOR_PRESSURE on the GPU with the reference's call signatures (mitgcm_jax/core/solve_for_pressure.py), and
+the operator normalisation it starts from (mitgcm_jax/core/cg2d.py:108-134):
+
+    ini_cg2d_norm(g, hFacW, hFacS, implicSurfPress, implicDiv2DFlow) -> cg2dNorm                          (:108-134)
 
     update_cg2d(p, cp, g, ex, hFacW, hFacS, recip_Bo, pW, pS, pC) -> (aW2d, aS2d, aC2d, pW, pS, pC)     (:29-65)
     cg2d_rhs(p, g, gU, gV, hFacW, hFacS, EmPmR, etaN, etaH, Bo_surf) -> (cg2d_b, cg2d_x)               (:68-106)
@@ -85,6 +88,34 @@ def _norm(cg2dNorm, dev, B):
             raise ValueError("one cg2dNorm per instance")
         return 0.0, t
     return float(cg2dNorm), None
+
+
+def ini_cg2d_norm(g, hFacW, hFacS, implicSurfPress, implicDiv2DFlow, *, ex=None):
+    """ini_cg2d_norm (mitgcm_jax/core/cg2d.py:108-134) on the GPU: cg2dNorm = 1 / max|aW, aS| of the un-normalised
+    initial operator (cg2d_ini_norm), bit for bit the reference's. hFacW, hFacS: the initial face fractions
+    [T, Nr, ny, nx] (a float is returned, as the reference returns) or [batch, T, Nr, ny, nx] (one value per
+    instance: a tensor, or an array for numpy input). The layout comes from g.layout, or from the Exchanger ex."""
+    if ex is None:
+        ex = default_exchanger(g.layout)
+    shape2d = tuple(ex.L.shape2d)
+    hW, back = _dev(hFacW)
+    dev = hW.device
+    single = hW.dim() == 4
+    hW, lead = _batch3(hW, dev, shape2d)
+    hS, _ = _batch3(hFacS, dev, shape2d)
+    B, Nr = hW.shape[0], hW.shape[2]
+    drF = _dev(np.asarray(g.drF, np.float64) if not isinstance(g.drF, torch.Tensor) else g.drF, dev)[0]
+    if drF.numel() != Nr:
+        raise ValueError("drF has one entry per level")
+    grid = [_grid(getattr(g, k), dev, shape2d) for k in ("dyG", "dxG", "recip_dxC", "recip_dyC")]
+    out = torch.empty(B, dtype=torch.float64, device=dev)
+    capi.check(capi.lib().cg2d_ini_norm(ex.handle(dev), B, Nr, float(implicSurfPress), float(implicDiv2DFlow),
+                                        hW.data_ptr(), hS.data_ptr(), drF.contiguous().data_ptr(),
+                                        *(t.data_ptr() for t in grid), out.data_ptr(), _stream(dev)),
+               "cg2d_ini_norm")
+    if single:
+        return float(out[0].item())
+    return back(out.reshape(lead))
 
 
 def update_cg2d(p, cp, g, ex, hFacW, hFacS, recip_Bo, pW, pS, pC):

@@ -1,7 +1,8 @@
 """CPU oracle of the steps either side of the CG2D solve -- TEST INFRASTRUCTURE ONLY (tests/, smoke() and bench.py's
 CPU legs import it; the library never does).
 
-Numpy restatements, operation for operation, of mitgcm_jax/core/solve_for_pressure.py:
+Numpy restatements, operation for operation, of mitgcm_jax/core/cg2d.py:108-134 (ini_cg2d_norm, the operator
+normalisation set up once) and of mitgcm_jax/core/solve_for_pressure.py:
 * update_cg2d (:29-65): the operator aW2d, aS2d, aC2d and the preconditioner pW, pS, pC from the level-summed
   face areas;
 * cg2d_rhs (:68-106): the right-hand side cg2d_b (fresh-water flux, the divergence of the g-hat transports summed
@@ -23,6 +24,20 @@ def _ksum(terms):
     for t in terms:
         out = out + t
     return out
+
+
+def ini_cg2d_norm(L, *, hFacW, hFacS, drF, dyG, dxG, recip_dxC, recip_dyC, implicSurfPress, implicDiv2DFlow):
+    """ini_cg2d_norm (mitgcm_jax/core/cg2d.py:108-134, ini_cg2d.F:90-135) for one instance: cg2dNorm =
+    1 / max|aW, aS| over the interior faces, aW = sum over k = 1..Nr in order of
+    (fac ((dyG drF(k)) hFacW(k))) recip_dxC with fac = implicSurfPress implicDiv2DFlow, aS likewise (1 where the
+    maximum is 0). hFacW/S [T, Nr, ny, nx]; 2-D fields [T, ny, nx]."""
+    J, I = L.js(1, L.sNy), L.is_(1, L.sNx)
+    fac = implicSurfPress * implicDiv2DFlow
+    tW = [fac * (dyG[:, J, I] * drF[k] * hFacW[:, k, J, I]) * recip_dxC[:, J, I] for k in range(len(drF))]
+    tS = [fac * (dxG[:, J, I] * drF[k] * hFacS[:, k, J, I]) * recip_dyC[:, J, I] for k in range(len(drF))]
+    aW, aS = _ksum(tW), _ksum(tS)
+    my = max(np.abs(aW).max(), np.abs(aS).max())
+    return 1.0 / my if my != 0.0 else 1.0
 
 
 def update_cg2d(L, tmap, *, hFacW, hFacS, drF, dyG, dxG, recip_dxC, recip_dyC, rA, recip_Bo, pW, pS, pC,

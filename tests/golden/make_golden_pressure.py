@@ -4,7 +4,8 @@ the reference source is available; the fixtures are committed and the tests neve
     python tests/golden/make_golden_pressure.py [--reference /root/reference]
 
 pressure_<case>.npz: outputs of mitgcm_jax.core.solve_for_pressure.update_cg2d (:29-65), cg2d_rhs (:68-106) and
-solve_for_pressure (:109-123, with cg2d_solve in sum_order="fortran"), executed by the reference module itself
+solve_for_pressure (:109-123, with cg2d_solve in sum_order="fortran"), and of mitgcm_jax.core.cg2d.ini_cg2d_norm
+(:108-134) on the same face fractions, executed by the reference module itself
 through the numpy stand-in for JAX (jax_standin.py), on seeded synthetic model fields
 (mit_jax_b200.synthetic.LLCSynthetic.model_fields) with exchange maps from mit_jax_b200.topology. The inputs are
 regenerated by the tests from the stored case parameters; their SHA-256 is stored to catch a changed generator.
@@ -89,11 +90,17 @@ def main():
         x_int = np.where(O.interior_mask(L), xs, 0.0)
         o_eta = P.solve_for_pressure_post(L, tmap, x_int, cg2d_x, f["recip_Bo"])
         assert np.array_equal(o_eta, etaN_new) and ds["numIters"] == it, name
+        # ini_cg2d_norm (cg2d.py:108-134) on the same face fractions
+        ini = refcg.ini_cg2d_norm(g, f["hFacW"], f["hFacS"], f["implicSurfPress"], f["implicDiv2DFlow"])
+        o_ini = P.ini_cg2d_norm(L, **{k: f[k] for k in ("hFacW", "hFacS", "drF", "dyG", "dxG", "recip_dxC",
+                                                         "recip_dyC", "implicSurfPress", "implicDiv2DFlow")})
+        assert float(o_ini) == float(ini), name
 
         np.savez_compressed(HERE / f"pressure_{name}.npz", **{k: v for k, v in c.items() if v is not None},
                             inputs_sha=pressure_sha(f, prev),
                             aW2d=ops[0], aS2d=ops[1], aC2d=ops[2], pW=ops[3], pS=ops[4], pC=ops[5],
-                            cg2d_b=cg2d_b, cg2d_x=cg2d_x, etaN=etaN_new, diag=diag, numIters=it)
+                            cg2d_b=cg2d_b, cg2d_x=cg2d_x, etaN=etaN_new, diag=diag, numIters=it,
+                            ini_cg2d_norm=np.float64(ini))
         print(f"{name}: Nr={c['Nr']} iters={it} last={diag[1]:.3e}")
 
 

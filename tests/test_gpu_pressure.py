@@ -54,6 +54,32 @@ def test_pressure_steps_match_reference_bitwise(name):
     np.testing.assert_array_equal(eta, z["etaN"])
 
 
+INI_KEYS = ("hFacW", "hFacS", "drF", "dyG", "dxG", "recip_dxC", "recip_dyC", "implicSurfPress", "implicDiv2DFlow")
+
+
+@pytest.mark.parametrize("name", list(PRESSURE_CASES))
+def test_ini_cg2d_norm_matches_reference_bitwise(name):
+    """ini_cg2d_norm on the GPU (cg2d_ini_norm): the reference's cg2dNorm bit for bit, as a float."""
+    syn, f, prev, z = load_pressure(name)
+    got = pr.ini_cg2d_norm(_grid(syn, f), f["hFacW"], f["hFacS"], f["implicSurfPress"], f["implicDiv2DFlow"])
+    assert isinstance(got, float) and got == float(z["ini_cg2d_norm"])
+
+
+def test_ini_cg2d_norm_batched_llc90_nr50():
+    """Three LLC90 members with 50 levels in one call: each member's cg2dNorm equals the oracle's bit for bit."""
+    from mit_jax_b200.synthetic import LLCSynthetic
+    syn = LLCSynthetic(90)
+    fs = [syn.model_fields(50, m) for m in range(3)]
+    g = _grid(syn, fs[0])
+    hW = np.stack([f["hFacW"] for f in fs])
+    hS = np.stack([f["hFacS"] for f in fs])
+    got = pr.ini_cg2d_norm(g, hW, hS, fs[0]["implicSurfPress"], fs[0]["implicDiv2DFlow"])
+    assert got.shape == (3,)
+    for m, f in enumerate(fs):
+        ref = P.ini_cg2d_norm(syn.L, **{k: (f if k.startswith("hFac") else fs[0])[k] for k in INI_KEYS})
+        assert got[m] == ref, (m, got[m], ref)
+
+
 def test_pressure_steps_batched_llc90_nr50():
     """Three LLC90 members with 50 levels in one call of each step, one cg2dNorm per member; every member equals
     its oracle bit for bit; then a batched mixed-precision solve_for_pressure converges for every member."""

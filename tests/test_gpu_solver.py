@@ -1,9 +1,9 @@
 """GPU parity of the persistent CG2D solver (libcg2d.so through the C ABI) against the oracle and the reference's
 own outputs (golden fixtures).
 
-Bars: bitwise for the "fortran" sum order (== the reference) and for the ROWBLOCK order and the MIXED iteration
-(== the oracle's restatement of the same operations); against the FP64 reference order, solution within 1e-12
-relative (FP64) / 1e-11 relative (MIXED) and iteration count within +-1 (FP64)."""
+Bars: bitwise for the "fortran" sum order (== the reference) and for the ROWBLOCK order (== the oracle's
+restatement of the same operations); against the FP64 reference order, solution within 1e-12 relative (FP64) and
+iteration count within +-1; the MIXED iteration (fused FP32 arithmetic) within 1e-11 relative of FP64."""
 
 import numpy as np
 import pytest
@@ -155,6 +155,9 @@ def test_nan_instance_is_reported_and_isolated(precision):
 
 
 def test_mixed_precision_matches_mixed_oracle_and_fp64(llc90):
+    """The mixed iteration (FP32 stencils and updates with fused multiply-adds) against the FP64 oracle: within
+    1e-11 relative, converged; its iteration count within 5 of the mixed oracle's (the same iteration with every
+    FP32 product and sum rounded separately)."""
     syn, ex_ref, tmap = llc90
     ex = cg.default_exchanger(syn.L)
     T = syn.topo.maps["T"]
@@ -163,12 +166,12 @@ def test_mixed_precision_matches_mixed_oracle_and_fp64(llc90):
     x, d = cg.cg2d_fortran(ex, ops, b, x0, cg2dNorm=norm, tolerance=1e-12, max_iters=300, sum_order="rowblock",
                            precision="mixed")
     xm, dm = O.cg2d_mixed(syn.L, T, ops, b, x0, cg2dNorm=norm, tolerance=1e-12, max_iters=300)
-    assert d["numIters"] == dm["numIters"] and d["replacements"] == dm["replacements"]
-    np.testing.assert_array_equal(x, xm)
+    assert d["status"] == "ok" and d["lastResidual"] < 1e-12
+    assert abs(d["numIters"] - dm["numIters"]) <= 5, (d["numIters"], dm["numIters"])
     x64, d64 = O.cg2d_fortran(syn.L, T, ops, b, x0, cg2dNorm=norm, tolerance=1e-12, max_iters=300,
                               sum_order="rowblock")
     assert _rel(x, x64, syn.L) < 1e-11
-    assert d["lastResidual"] < 1e-12
+    assert _rel(xm, x64, syn.L) < 1e-11
 
 
 def test_two_rhs_share_the_operator():
@@ -190,7 +193,9 @@ def test_two_rhs_share_the_operator():
 
 
 def test_mixed_size_groups_llc270_and_llc90():
-    """LLC270 and LLC90 instances in one MIXED launch (two groups): each equals its oracle."""
+    """LLC270 and LLC90 instances in one MIXED launch (two groups): each converges and lies within 1e-11 of the
+    FP64 solve of the same instance (the same two groups in one FP64 launch); the LLC90 iteration counts are within
+    5 of the mixed oracle's."""
     from mit_jax_b200.synthetic import LLCSynthetic
     dev = torch.device("cuda")
     groups, refs = [], []
@@ -205,19 +210,21 @@ def test_mixed_size_groups_llc270_and_llc90():
             norms.append(norm)
         ops_t = tuple(torch.as_tensor(np.stack([o[k] for o in mats])).to(dev) for k in range(6))
         b_t = torch.as_tensor(np.stack(bs)).to(dev)
-        groups.append(cg.GroupSpec(ex, ops_t, [b_t], [torch.zeros_like(b_t)], [1e-12], [400],
+        groups.append(cg.GroupSpec(ex, ops_t, [b_t], [torch.zeros_like(b_t)], [1e-12], [1000],
                                    torch.as_tensor(norms)))
         refs.append((syn, mats, bs, norms))
     res = cg.solve_groups(groups, precision="mixed")
-    for (syn, mats, bs, norms), (slot0,) in zip(refs, res):
+    res64 = cg.solve_groups(groups, precision="f64")
+    for (syn, mats, bs, norms), (slot0,), (slot64,) in zip(refs, res, res64):
         xo, _, dg = slot0
         diags = cg.diag_records(dg)
         for m in range(len(mats)):
-            xm, dm = O.cg2d_mixed(syn.L, syn.topo.maps["T"], mats[m], bs[m], np.zeros_like(bs[m]),
-                                  cg2dNorm=norms[m], tolerance=1e-12, max_iters=400)
-            assert diags[m]["numIters"] == dm["numIters"]
-            J, I = syn.L.interior
-            np.testing.assert_array_equal(xo[m].cpu().numpy()[:, J, I], xm[:, J, I])
+            assert diags[m]["status"] == "ok", diags[m]
+            assert _rel(xo[m].cpu().numpy(), slot64[0][m].cpu().numpy(), syn.L) < 1e-11
+            if syn.L.sNx == 90:
+                xm, dm = O.cg2d_mixed(syn.L, syn.topo.maps["T"], mats[m], bs[m], np.zeros_like(bs[m]),
+                                      cg2dNorm=norms[m], tolerance=1e-12, max_iters=1000)
+                assert abs(diags[m]["numIters"] - dm["numIters"]) <= 5
 
 
 def test_matvec_exchange_and_edge_products_equal_oracle():

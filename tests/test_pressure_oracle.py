@@ -1,6 +1,7 @@
 """The CPU oracle of the steps either side of the solve (oracle/pressure_oracle.py) against the reference's own
-update_cg2d, cg2d_rhs and solve_for_pressure (golden fixtures made by running mitgcm_jax through a numpy stand-in
-for JAX): bitwise, including the preconditioner points update_cg2d keeps and both fresh-water-flux branches."""
+update_cg2d, cg2d_rhs, solve_for_pressure and ini_cg2d_norm (golden fixtures made by running mitgcm_jax through a
+numpy stand-in for JAX): bitwise, including the preconditioner points update_cg2d keeps and both fresh-water-flux
+branches."""
 
 import numpy as np
 import pytest
@@ -33,6 +34,17 @@ def test_pressure_oracle_matches_reference_bitwise(name):
     assert d["numIters"] == int(z["numIters"])
     eta = P.solve_for_pressure_post(L, tmap, np.where(O.interior_mask(L), x, 0.0), x0, f["recip_Bo"])
     np.testing.assert_array_equal(eta, z["etaN"])
+
+
+INI_KEYS = ("hFacW", "hFacS", "drF", "dyG", "dxG", "recip_dxC", "recip_dyC", "implicSurfPress", "implicDiv2DFlow")
+
+
+@pytest.mark.parametrize("name", list(PRESSURE_CASES))
+def test_ini_cg2d_norm_oracle_matches_reference(name):
+    """ini_cg2d_norm (cg2d.py:108-134): the oracle's cg2dNorm equals the reference's bit for bit."""
+    syn, f, prev, z = load_pressure(name)
+    got = P.ini_cg2d_norm(syn.L, **{k: f[k] for k in INI_KEYS})
+    assert got == float(z["ini_cg2d_norm"])
 
 
 def test_update_keeps_preconditioner_outside_its_range():
