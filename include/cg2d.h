@@ -63,7 +63,9 @@ typedef enum {
 typedef struct {
   int precision;       /* cg2d_precision_t */
   int sum_order;       /* cg2d_sum_order_t */
-  int rows_per_block;  /* ROWBLOCK block height in rows (multiple of 8; default 8) */
+  int rows_per_block;  /* ROWBLOCK block height in rows (multiple of 8; default 8). A mixed-precision single-group
+                          launch whose 15-row chunks fit in shared memory (tiles up to about 130 points wide) runs on
+                          the 16-warp build and uses blocks of 15 rows instead */
   int replace_every;   /* MIXED: FP64 true-residual replacement period in iterations (default 25) */
   double replace_above;/* MIXED: replace only while the residual is above replace_above * tolerance (default 100) */
   int grid_ctas;       /* 0 = as many as can be co-resident (capped by the work units) */

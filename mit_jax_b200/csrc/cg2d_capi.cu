@@ -53,7 +53,7 @@ struct WsLayout {
   long long vec_off[kMaxGroups][V_NVEC];
   int hist_len, part_units, total_rhs, total_ops, total_units, max_ni;
   int nblk[kMaxGroups], units[kMaxGroups];
-  int ch, nstage[P_NPASS];
+  int ch, nw, rpb, nstage[P_NPASS];   // chunk rows, compute warps, ROWBLOCK block rows
   unsigned stage_bytes;
   size_t smem;
 };
@@ -74,27 +74,35 @@ cg2d_status_t check_params(const cg2d_params_t* p) {
   return CG2D_OK;
 }
 
-// chunk height and stage buffers: the largest chunk (8, else 4 rows) whose `ns` stage buffers fit
-cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial, int ns, WsLayout* L) {
+// mixed precision with two right-hand sides in the ROWBLOCK order keeps both solves of an instance interleaved
+// (GroupDev::pair)
+inline int paired(int mixed, int serial, int nrhs) { return mixed && !serial && nrhs == 2 ? 1 : 0; }
+
+// chunk height and stage buffers for nw compute warps: the largest chunk (nw rows; with 8 warps 8, else 4 rows)
+// whose `ns` stage buffers fit
+cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial, int ns, int nw, WsLayout* L) {
   const size_t fixed = fixed_smem_bytes(L->max_ni, serial);
-  for (int ch : {8, 4}) {
+  const int chs[2] = {nw, nw == kWarps ? 4 : 0};
+  for (int ch : chs) {
+    if (ch == 0) break;
     unsigned hot = 0, rep = 0;
     for (int g = 0; g < ng; ++g) {
       const cg2d_topology* tp = gr[g].topo;
       const int npx = tp->sNx + 2 * tp->OLx;
+      const int pair = paired(mixed, serial, gr[g].nrhs);
       for (int pt : {P_S, P_X, P_Z}) {
-        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, tp->sNx, npx);
+        const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, tp->sNx, npx, pair);
         if (S.total > hot) hot = S.total;
       }
       if (mixed) {
-        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, tp->sNx, npx);
+        const StageLay S = stage_layout(P_R, mixed, ch, gr[g].nrhs, tp->sNx, npx, pair);
         if (S.total > rep) rep = S.total;
       }
     }
-    // the direct-load passes stage (8 + 2) rows of (max_ni + 2) doubles per solve slot in the same area
-    const unsigned direct = (unsigned)(2 * (kWarps + 2) * (L->max_ni + 2) * sizeof(double));
+    // the direct-load passes stage (nw + 2) rows of (max_ni + 2) doubles per solve slot in the same area
+    const unsigned direct = (unsigned)(2 * (nw + 2) * (L->max_ni + 2) * sizeof(double));
     // the sums of a pass are formed with a tile-sum buffer per warp in the same area
-    const unsigned sums = (unsigned)(kAllWarps * kMaxTiles * sizeof(double));
+    const unsigned sums = (unsigned)((nw + 1) * kMaxTiles * sizeof(double));
     // the stage area (ns buffers) also holds a replacement pass's single stage, the direct passes' staging and the
     // tile-sum buffers
     unsigned sb = hot;
@@ -105,6 +113,7 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
     const size_t smem = fixed + (size_t)ns * sb;
     if (smem <= (size_t)kSmemLimit) {
       L->ch = ch;
+      L->nw = nw;
       L->stage_bytes = sb;
       L->smem = smem;
       // FORTRAN order keeps every element product of a chunk in one buffer: one stage
@@ -130,14 +139,33 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     if (tp->nTiles > kMaxTiles || tp->sNx > kMaxNi || tp->sNy > kMaxNi) return CG2D_UNSUPPORTED;
     // bulk copies move whole padded coefficient rows: 16-byte multiples
     if (((tp->sNx + 2 * tp->OLx) * 8) % 16 != 0) return CG2D_UNSUPPORTED;
+    if (tp->sNx > L->max_ni) L->max_ni = tp->sNx;
+  }
+  // Mixed precision in the ROWBLOCK order runs a single group on the 16-warp build when two stages of its 15-row
+  // chunks fit: blocks (work units) of kMixedWarps rows, one chunk each, with the deepest pipeline up to the one
+  // asked for that fits (so that the pipeline depth, a schedule option, never changes the sum order). Otherwise 8
+  // compute warps and rows_per_block rows.
+  const int ns = p->stages ? p->stages : 2;
+  cg2d_status_t st = CG2D_UNSUPPORTED;
+  if (mixed && !serial && ng == 1) {
+    for (int n = ns; n >= 2 && st != CG2D_OK; --n) st = size_stages(gr, ng, mixed, serial, n, kMixedWarps, L);
+    if (st == CG2D_OK) L->rpb = kMixedWarps;
+  }
+  if (st != CG2D_OK) {
+    st = size_stages(gr, ng, mixed, serial, ns, kWarps, L);
+    if (st != CG2D_OK) return st;
+    L->rpb = p->rows_per_block;
+  }
+  for (int g = 0; g < ng; ++g) {
+    const cg2d_group_t& G = gr[g];
+    const cg2d_topology* tp = G.topo;
     for (int s = 0; s < G.nrhs; ++s) {
       if (G.max_iters[s] < 0 || !(G.tolerance[s] >= 0.0)) return CG2D_BAD_ARG;
       if (G.max_iters[s] > max_iters) max_iters = G.max_iters[s];
     }
-    L->nblk[g] = serial ? 1 : (tp->sNy + p->rows_per_block - 1) / p->rows_per_block;
+    L->nblk[g] = serial ? 1 : (tp->sNy + L->rpb - 1) / L->rpb;
     L->units[g] = L->nblk[g] * tp->nTiles;
     if (L->units[g] > L->part_units) L->part_units = L->units[g];
-    if (tp->sNx > L->max_ni) L->max_ni = tp->sNx;
     L->total_rhs += G.count * G.nrhs;
     L->total_ops += G.count;
     const long long tu = (long long)L->total_units + (long long)G.count * L->units[g];
@@ -145,8 +173,6 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     L->total_units = (int)tu;
   }
   if (L->total_rhs > kMaxSolves || L->total_ops > kMaxOps) return CG2D_UNSUPPORTED;
-  cg2d_status_t st = size_stages(gr, ng, mixed, serial, p->stages ? p->stages : 2, L);
-  if (st != CG2D_OK) return st;
   L->hist_len = max_iters + 2;
   size_t o = 0;
   L->gs = o; o += al(8 * sizeof(unsigned));
@@ -158,13 +184,14 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
   L->part = o; o += al(sizeof(double) * (size_t)L->total_rhs * 2 * L->part_units);
   for (int g = 0; g < ng; ++g) {
     const cg2d_topology* tp = gr[g].topo;
-    // ringed vector tiles [T][sNy+2][P]
+    // ringed vector tiles [T][sNy+2][P]; paired: one block per instance with both solves in every element
     const long long elems = (long long)tp->nTiles * (tp->sNy + 2) * vec_pitch(tp->sNx);
+    const int pair = paired(mixed, serial, gr[g].nrhs), per = pair ? 2 : 1;
     long long off = 0;
-    L->vec_off[g][V_X] = off; off += (long long)al(sizeof(double) * elems);
-    for (int v = 1; v < V_NVEC; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * elems); }
+    L->vec_off[g][V_X] = off; off += (long long)al(sizeof(double) * per * elems);
+    for (int v = 1; v < V_NVEC; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * per * elems); }
     L->vec_stride[g] = off;
-    L->vec[g] = o; o += al((size_t)off * gr[g].count * gr[g].nrhs);
+    L->vec[g] = o; o += al((size_t)off * gr[g].count * (pair ? 1 : gr[g].nrhs));
     // packed coefficients [count][2][T][sNy+1][3][ldc] (the solver's precision)
     L->cpk[g] = o;
     o += al(vsz * 2 * (size_t)tp->nTiles * (tp->sNy + 1) * 3 * coef_pitch(tp->sNx) * gr[g].count);
@@ -363,7 +390,8 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
   kp.total_ops = L.total_ops;
   kp.mixed = params->precision == CG2D_PREC_MIXED;
   kp.serial = params->sum_order == CG2D_SUM_FORTRAN;
-  kp.rows_per_block = params->rows_per_block;
+  kp.rows_per_block = L.rpb;
+  kp.nw = L.nw;
   kp.replace_every = params->replace_every;
   kp.replace_above = params->replace_above;
   kp.max_ni = L.max_ni;
@@ -393,7 +421,8 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
   for (int g = 0; g < ngroups; ++g) {
     const cg2d_topology* tp = groups[g].topo;
     for (int pt = 0; pt < P_NPASS; ++pt)
-      kp.lay[g][pt] = stage_layout(pt, kp.mixed, L.ch, groups[g].nrhs, tp->sNx, tp->sNx + 2 * tp->OLx);
+      kp.lay[g][pt] = stage_layout(pt, kp.mixed, L.ch, groups[g].nrhs, tp->sNx, tp->sNx + 2 * tp->OLx,
+                                   paired(kp.mixed, kp.serial, groups[g].nrhs));
   }
   int unit_base = 0, op_base = 0, rhs_base = 0;
   for (int g = 0; g < ngroups; ++g) {
@@ -426,6 +455,7 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
     }
     d.vec = ws + L.vec[g];
     d.vec_stride = L.vec_stride[g];
+    d.pair = paired(kp.mixed, kp.serial, G.nrhs);
     for (int v = 0; v < V_NVEC; ++v) d.vec_off[v] = L.vec_off[g][v];
     unit_base += G.count * d.units;
     op_base += G.count;

@@ -8,10 +8,15 @@
 
 namespace cg2d {
 
-constexpr int kWarps = 8;                  // compute warps per CTA; a chunk has at most kWarps rows (one warp per row)
-constexpr int kProducer = kWarps;          // index of the warp that issues the bulk copies and folds the row sums
+// Compute warps per CTA (a chunk has at most as many rows, one warp per row; the next warp issues the bulk copies
+// and folds the row sums): kWarps in the FP64 and FORTRAN-order builds (two CTAs of 9 warps per SM), kMixedWarps in
+// the mixed-precision ROWBLOCK build for tiles whose 15-row chunks fit (one CTA of 16 warps per SM, 128 registers a
+// thread: the register file splits evenly over the SM's four schedulers). KParams::nw holds the launch's count.
+constexpr int kWarps = 8;
 constexpr int kThreads = (kWarps + 1) * 32;
-constexpr int kAllWarps = kThreads / 32;
+constexpr int kMixedWarps = 15;
+constexpr int kMixedThreads = (kMixedWarps + 1) * 32;
+constexpr int kMaxWarps = kMixedWarps;
 constexpr int kMaxStages = 4;              // stage buffers of the copy pipeline (cg2d_params_t.stages)
 constexpr int kMaxUnitsPerCta = 512;       // work units one CTA owns in a launch (its unit table)
 constexpr int kMaxGroups = CG2D_MAX_GROUPS;
@@ -73,9 +78,12 @@ struct GroupDev {
   cg2d_diag_t* diag[2];
   double tol[2];
   int max_iters[2];
-  char* vec;                // [count][nrhs] vector blocks
+  char* vec;                // [count][nrhs] vector blocks, or [count] blocks of pairs (pair)
   long long vec_stride;     // bytes per vector block
   long long vec_off[V_NVEC];
+  // MIXED with two right-hand sides: both solves of an instance interleaved point by point (float2 vectors, x as
+  // double2), so that one load or store moves a point of both; element e of slot s's vector is scalar 2 e + s
+  int pair;
 };
 
 // Shared-memory image of one chunk for a pipelined pass (offsets in bytes from the stage buffer).
@@ -94,7 +102,9 @@ struct StageLay {
 __host__ __device__ inline unsigned al128(unsigned x) { return (x + 127u) & ~127u; }
 __host__ __device__ inline unsigned al16(unsigned x) { return (x + 15u) & ~15u; }
 
-__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int ni, int npx) {
+// pair: the group's two right-hand sides interleaved (GroupDev::pair): each staged vector holds both (vec[1][v] is
+// slot 1's first scalar inside vec[0][v]'s rows; element e of slot s at scalar 2 e of vec[s][v])
+__host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int nrhs, int ni, int npx, int pair = 0) {
   StageLay L;
   const int P = vec_pitch(ni), ldc = coef_pitch(ni);
   unsigned o = 0;
@@ -112,14 +122,27 @@ __host__ __device__ inline StageLay stage_layout(int pt, int mixed, int ch, int 
   L.nvec = (pt == P_Z) ? 1 : 2;
   const int vs = mixed ? 4 : 8;
   for (int v = 0; v < 2; ++v) L.vsize[v] = (pt == P_R && v == 0) ? 8 : vs;
-  for (int s = 0; s < 2; ++s)
+  if (pair) {
     for (int v = 0; v < 2; ++v) {
-      L.vec[s][v] = 0;
-      if (s < nrhs && v < L.nvec) { L.vec[s][v] = o; o += al128((unsigned)((ch + 2) * P * L.vsize[v])); }
+      L.vec[0][v] = L.vec[1][v] = 0;
+      if (v < L.nvec) {
+        L.vec[0][v] = o;
+        L.vec[1][v] = o + (unsigned)L.vsize[v];
+        o += al128((unsigned)((ch + 2) * P * 2 * L.vsize[v]));
+      }
     }
-  for (int s = 0; s < 2; ++s) {
-    L.xo[s] = 0;
-    if (pt == P_S && s < nrhs) { L.xo[s] = o; o += al128((unsigned)(ch * P * 8)); }
+    L.xo[0] = L.xo[1] = 0;
+    if (pt == P_S) { L.xo[0] = o; L.xo[1] = o + 8u; o += al128((unsigned)(ch * P * 16)); }
+  } else {
+    for (int s = 0; s < 2; ++s)
+      for (int v = 0; v < 2; ++v) {
+        L.vec[s][v] = 0;
+        if (s < nrhs && v < L.nvec) { L.vec[s][v] = o; o += al128((unsigned)((ch + 2) * P * L.vsize[v])); }
+      }
+    for (int s = 0; s < 2; ++s) {
+      L.xo[s] = 0;
+      if (pt == P_S && s < nrhs) { L.xo[s] = o; o += al128((unsigned)(ch * P * 8)); }
+    }
   }
   L.twe = o; o += al128((unsigned)(ch * 16));
   L.ts = o; o += al128(al16((unsigned)(ni * 8)));
@@ -135,7 +158,8 @@ struct KParams {
   double replace_above;
   int max_ni;
   int fp64_cps;             // FP64: the kernel built for 1 or 2 CTAs per SM (96 registers a thread at 2)
-  int ch;                   // rows per chunk (<= kWarps)
+  int ch;                   // rows per chunk (<= nw)
+  int nw;                   // compute warps per CTA (kWarps or kMixedWarps); warp nw is the copy warp
   int nstage[P_NPASS];      // pipeline depth of each pass kind (1 or 2)
   unsigned stage_bytes;     // bytes of one stage buffer
   double* hist;             // [total_rhs][H_NKIND][hist_len]

@@ -133,40 +133,75 @@ struct RhsArgs {
   int fresh_water, Nr;
 };
 
-// cg2d_x = Bo_surf etaN everywhere (:76); cg2d_b on the interior (:77-106), 0 on halos
-__global__ void k_rhs(TopoDev tp, RhsArgs A, double* cg2d_b, double* cg2d_x) {
+// cg2d_x = Bo_surf etaN everywhere (:76); cg2d_b = 0 on halos (the interior is k_rhs's)
+__global__ void k_rhs_fill(TopoDev tp, const double* Bo_surf, const double* etaN, double* cg2d_b, double* cg2d_x) {
   const int in = blockIdx.y;
-  const int plane = tp.npy * tp.npx;
-  const long long o = (long long)in * tp.T * plane;
+  const long long o = (long long)in * tp.T * tp.npy * tp.npx;
   FOR_Q(tp) {
-    const Pt p = decode(tp, q);
-    cg2d_x[o + q] = mul(A.Bo_surf[q], A.etaN[o + q]);
-    double b = 0.0;
-    if (interior(tp, p)) {
-      if (A.fresh_water) b = mul(dvd(mul(mul(A.tmpFac, A.rA[q]), A.EmPmR[o + q]), A.dTm), A.maskInC[q]);
-      const long long b3 = ((long long)in * tp.T + p.t) * A.Nr * plane + (q - p.t * plane);
-      const double* __restrict__ hw = A.hFacW + b3;
-      const double* __restrict__ hs = A.hFacS + b3;
-      const double* __restrict__ gu = A.gU + b3;
-      const double* __restrict__ gv = A.gV + b3;
-      const int n = tp.npx;
-      const double dyc = A.dyG[q], dye = A.dyG[q + 1], dxc = A.dxG[q], dxn = A.dxG[q + n], dTm = A.dTm;
-      // unrolled so that several levels' loads are in flight while the ordered sum proceeds
-#pragma unroll 4
-      for (int k = A.Nr - 1; k >= 0; --k) {                                     // :95-101, k = Nr..1
-        const long long c = (long long)k * plane;
-        const double d = __ldg(A.drF + k);
-        const double hw0 = __ldg(hw + c), hw1 = __ldg(hw + c + 1), u0 = __ldg(gu + c), u1 = __ldg(gu + c + 1);
-        const double hs0 = __ldg(hs + c), hs1 = __ldg(hs + c + n), v0 = __ldg(gv + c), v1 = __ldg(gv + c + n);
-        const double pu0 = dvd(mul(mul(mul(dyc, d), hw0), u0), dTm);                                // :90, :92
-        const double pu1 = dvd(mul(mul(mul(dye, d), hw1), u1), dTm);
-        b = sub(add(b, pu1), pu0);                                                                // :97
-        const double pv0 = dvd(mul(mul(mul(dxc, d), hs0), v0), dTm);                                // :91, :93
-        const double pv1 = dvd(mul(mul(mul(dxn, d), hs1), v1), dTm);
-        b = sub(add(b, pv1), pv0);                                                                // :98
-      }
-      b = sub(b, mul(dvd(dvd(mul(A.fsf, A.rA[q]), A.dTm), A.dTfs), A.etaH[o + q]));          // :103-105
+    cg2d_x[o + q] = mul(Bo_surf[q], etaN[o + q]);
+    if (!interior(tp, decode(tp, q))) cg2d_b[o + q] = 0.0;
+  }
+}
+
+// cg2d_b on the interior (:77-106): the fresh-water term, then for k = Nr..1 in order (:95-101)
+//   b = (b + pu(i+1)) - pu(i),  b = (b + pv(j+1)) - pv(j),
+// pu(i) = ((dyG(i) drF(k)) hFacW(i, k)) gU(i, k) / deltaTMom the transport through the west face of point i (:90, :92),
+// pv(j) likewise through the south face; then the etaH term (:103-105). A face is shared by the two points on either
+// side: each thread forms the terms of its own west and south faces once per level, and takes its east and north
+// face's terms from the threads that own those faces (the next lane by shuffle, the next row through shared memory).
+// A block of 32 lanes x kRhsRows rows owns 31 columns x (kRhsRows - 1) rows of points; its last lane and last row
+// only form faces (the east / north faces of the block's points; the next block owns their points). The terms are
+// the same floating-point operations on the same operands whichever thread forms them, so the sums are the
+// reference's bit for bit, with about 2.2 divisions per point and level instead of 4.
+constexpr int kRhsRows = 8;
+constexpr int kRhsCols = 31, kRhsOwnRows = kRhsRows - 1;   // points a block owns
+__global__ void __launch_bounds__(32 * kRhsRows, 4) k_rhs(TopoDev tp, RhsArgs A, double* cg2d_b) {
+  __shared__ double pvs[2][kRhsRows][32];
+  const int in = blockIdx.z;
+  const int nrb = (tp.nj + kRhsOwnRows - 1) / kRhsOwnRows;   // row blocks per tile
+  const int t = blockIdx.y / nrb, jb = blockIdx.y - t * nrb;
+  const int lane = threadIdx.x, y = threadIdx.y;
+  const int i = blockIdx.x * kRhsCols + lane, j = jb * kRhsOwnRows + y;
+  const bool face = i <= tp.ni && j <= tp.nj;             // forms the terms of its west / south face
+  const bool own = lane < kRhsCols && y < kRhsOwnRows && i < tp.ni && j < tp.nj;   // sums cg2d_b
+  const int plane = tp.npy * tp.npx;
+  const int q = t * plane + (j + tp.OLy) * tp.npx + i + tp.OLx;   // padded point (in bounds when face)
+  const long long o = (long long)in * tp.T * plane;
+  const long long b3 = ((long long)in * tp.T + t) * A.Nr * plane + (q - t * plane);
+  const double dTm = A.dTm;
+  const double dyc = face ? A.dyG[q] : 0.0, dxc = face ? A.dxG[q] : 0.0;
+  double b = 0.0;
+  if (own && A.fresh_water) b = mul(dvd(mul(mul(A.tmpFac, A.rA[q]), A.EmPmR[o + q]), A.dTm), A.maskInC[q]);
+  // the level's face fractions and transports, loaded one level ahead of their use (the level loop is a chain of
+  // ordered sums with a block barrier per level, so the next level's loads are put in flight before it)
+  double hw = 0.0, u = 0.0, hs = 0.0, v = 0.0;
+  auto load = [&](int k) {
+    if (face) {
+      const long long c = b3 + (long long)k * plane;
+      hw = __ldg(A.hFacW + c); u = __ldg(A.gU + c); hs = __ldg(A.hFacS + c); v = __ldg(A.gV + c);
     }
+  };
+  load(A.Nr - 1);
+  for (int k = A.Nr - 1; k >= 0; --k) {                                       // :95-101, k = Nr..1
+    const double hw0 = hw, u0 = u, hs0 = hs, v0 = v;
+    if (k > 0) load(k - 1);
+    const double d = __ldg(A.drF + k);
+    double pu0 = 0.0, pv0 = 0.0;
+    if (face) {
+      pu0 = dvd(mul(mul(mul(dyc, d), hw0), u0), dTm);                                        // :90, :92
+      pv0 = dvd(mul(mul(mul(dxc, d), hs0), v0), dTm);                                        // :91, :93
+    }
+    const int buf = k & 1;
+    pvs[buf][y][lane] = pv0;
+    const double pu1 = __shfl_down_sync(0xffffffffu, pu0, 1);
+    __syncthreads();
+    if (own) {
+      b = sub(add(b, pu1), pu0);                                                              // :97
+      b = sub(add(b, pvs[buf][y + 1][lane]), pv0);                                            // :98
+    }
+  }
+  if (own) {
+    b = sub(b, mul(dvd(dvd(mul(A.fsf, A.rA[q]), A.dTm), A.dTfs), A.etaH[o + q]));            // :103-105
     cg2d_b[o + q] = b;
   }
 }
@@ -277,7 +312,12 @@ cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st) {
   A.dTfs = R.deltaTFreeSurf;
   A.fresh_water = R.useRealFreshWaterFlux;
   A.Nr = R.Nr;
-  k_rhs<<<grid_of(tp, R.batch), 256, 0, st>>>(tp, A, R.cg2d_b, R.cg2d_x);
+  k_rhs_fill<<<grid_of(tp, R.batch), 256, 0, st>>>(tp, R.Bo_surf, R.etaN, R.cg2d_b, R.cg2d_x);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int nrb = (tp.nj + kRhsOwnRows - 1) / kRhsOwnRows;
+  const dim3 grid((unsigned)((tp.ni + kRhsCols - 1) / kRhsCols), (unsigned)(tp.T * nrb), (unsigned)R.batch);
+  k_rhs<<<grid, dim3(32, kRhsRows), 0, st>>>(tp, A, R.cg2d_b);
   return cudaGetLastError();
 }
 

@@ -75,6 +75,8 @@ __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 __device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ void stcg(double* p, double v) { __stcg(p, v); }
 __device__ __forceinline__ void stcg(float* p, float v) { __stcg(p, v); }
+__device__ __forceinline__ void stcg(float2* p, float2 v) { __stcg(p, v); }
+__device__ __forceinline__ void stcg(double2* p, double2 v) { __stcg(p, v); }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
@@ -185,8 +187,8 @@ constexpr size_t rnorm = c2 + a16(sizeof(double) * kMaxSolves);             // d
 constexpr size_t norm = rnorm + a16(sizeof(double) * kMaxSolves);           // double [kMaxSolves] cg2dNorm
 constexpr size_t has_alpha = norm + a16(sizeof(double) * kMaxSolves);       // int [kMaxSolves]
 constexpr size_t opp = has_alpha + a16(sizeof(int) * kMaxSolves);           // int [kMaxOps] operator in the pass
-constexpr size_t rowsum = opp + a16(sizeof(int) * kMaxOps);                 // double [kMaxStages][4][kWarps]
-constexpr size_t misc = rowsum + a16(sizeof(double) * kMaxStages * 4 * kWarps);   // int [4]
+constexpr size_t rowsum = opp + a16(sizeof(int) * kMaxOps);                 // double [kMaxStages][4][kMaxWarps]
+constexpr size_t misc = rowsum + a16(sizeof(double) * kMaxStages * 4 * kMaxWarps);   // int [4]
 constexpr size_t full = misc + a16(sizeof(int) * 4);                        // mbarrier [kMaxStages]
 constexpr size_t empty = full + a16(8 * kMaxStages);                        // mbarrier [kMaxStages]
 constexpr size_t pacc = empty + a16(8 * kMaxStages);                        // u64 [kProfSlots]
@@ -201,13 +203,13 @@ constexpr size_t end = state + a16(40 * (kMaxSolves + 1));                   // 
 //   act, c1, c2, rnorm, norm, has_alpha   per solve: action in the pass, pass coefficients, rhsNorm, cg2dNorm,
 //                                          whether alpha_{k-1} exists
 //   opp                                    per operator: takes part in the pass
-//   rowsum                                 row sums of the chunk in each stage [stage][4 sums][kWarps]
+//   rowsum                                 row sums of the chunk in each stage [stage][4 sums][kMaxWarps]
 //   misc                                   [0] grid-wide wait ok, [3] units in utab
 //   full, empty                            stage mbarriers: copies landed / compute warps done with the stage
 //   pacc, uacc                             phase times (profiling); the current unit's partial sums
 //   utab, pend                             this CTA's work units; the chunk in each stage awaiting its row sums
 //   state                                  CG scalars of each solve (SolveState), one spare entry
-// then prod (FORTRAN order: [2 slots][2 kinds][kWarps][max_ni]) and the stage buffers at `stage` (kMaxStages x
+// then prod (FORTRAN order, kWarps compute warps: [2 slots][2 kinds][kWarps][max_ni]) and the stage buffers at `stage` (kMaxStages x
 // stage_bytes, 128-aligned; also the direct-pass staging area and the tile-sum buffers of the pass sums).
 struct Smem {
   unsigned stage;
@@ -295,8 +297,9 @@ __device__ __forceinline__ void locate(const KParams& kp, int r, int& gi, int& i
 __device__ void form_sums(const KParams& kp, int pt, int hidx, const Smem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* tbuf = reinterpret_cast<double*>(smem_raw + sm.stage) + warp * kMaxTiles;   // free between passes
-  const int nw = (int)gridDim.x * kAllWarps;
-  for (int s = (int)blockIdx.x * kAllWarps + warp; s < 2 * kp.total_rhs; s += nw) {
+  const int wpc = (int)(blockDim.x >> 5);   // warps per CTA
+  const int nw = (int)gridDim.x * wpc;
+  for (int s = (int)blockIdx.x * wpc + warp; s < 2 * kp.total_rhs; s += nw) {
     const int r = s >> 1, q = s & 1;
     if (q >= nsums(pt, sm.act()[r])) continue;
     int gi, inst, slot;
@@ -337,11 +340,15 @@ __device__ __forceinline__ double* hist_ptr(const KParams& kp, int rid, int kind
   return kp.hist + ((size_t)rid * H_NKIND + kind) * (size_t)kp.hist_len + idx;
 }
 
-// a solve's vector (ringed tiles, [T][nj+2][P])
+// a solve's vector (ringed tiles, [T][nj+2][P]): element e is at [e] or, paired (GroupDev::pair), at [2 e]
 template <class T>
 __device__ __forceinline__ T* vec_ptr(const GroupDev& g, int inst, int slot, int which) {
+  if (g.pair)
+    return reinterpret_cast<T*>(g.vec + (long long)inst * g.vec_stride + g.vec_off[which]) + slot;
   return reinterpret_cast<T*>(g.vec + (long long)(inst * g.nrhs + slot) * g.vec_stride + g.vec_off[which]);
 }
+// the element stride of a group's vectors (1, or 2 when both solves are interleaved)
+__device__ __forceinline__ int vstride(const GroupDev& g) { return g.pair ? 2 : 1; }
 // element of point (t, j, i) in a ringed vector; -1 <= j <= nj, -1 <= i <= ni
 __device__ __forceinline__ long long vidx(const TopoDev& tp, int t, int j, int i) {
   return ((long long)t * (tp.nj + 2) + j + 1) * tp.P + i + 1;
@@ -349,15 +356,16 @@ __device__ __forceinline__ long long vidx(const TopoDev& tp, int t, int j, int i
 
 // one push store: target a (-1 = none) must lie inside the vector (lim elements); anything else is an internal
 // inconsistency, recorded in the error word instead of stored
+// (es: the vector's element stride in T)
 template <class T>
-__device__ __forceinline__ void push_one(T* vec, int a, T v, unsigned lim, unsigned* gs) {
-  if ((unsigned)a < lim) stcg(vec + a, v);
+__device__ __forceinline__ void push_one(T* vec, int a, T v, unsigned lim, unsigned* gs, int es = 1) {
+  if ((unsigned)a < lim) stcg(vec + (long long)a * es, v);
   else if (a != -1) atomicCAS(&gs[1], 0u, (unsigned)CG2D_INTERNAL_ERROR);
 }
 
 // store the value of point (t, j, i) into the ring cells of the tiles that read it across an edge
 template <class T>
-__device__ __forceinline__ void push(const TopoDev& tp, T* vec, int t, int j, int i, T v, unsigned* gs) {
+__device__ __forceinline__ void push(const TopoDev& tp, T* vec, int t, int j, int i, T v, unsigned* gs, int es = 1) {
   const int* e;
   if (i == 0) e = tp.tg + ((size_t)t * tp.nj + j) * 4;
   else if (i == tp.ni - 1) e = tp.tg + ((size_t)t * tp.nj + j) * 4 + 2;
@@ -365,8 +373,8 @@ __device__ __forceinline__ void push(const TopoDev& tp, T* vec, int t, int j, in
   else if (j == tp.nj - 1) e = tp.tg + (size_t)tp.T * tp.nj * 4 + ((size_t)(tp.T + t) * tp.nip + i) * 2;
   else return;
   const unsigned lim = (unsigned)tp.T * (unsigned)(tp.nj + 2) * (unsigned)tp.P;
-  push_one(vec, __ldg(e), v, lim, gs);
-  push_one(vec, __ldg(e + 1), v, lim, gs);
+  push_one(vec, __ldg(e), v, lim, gs, es);
+  push_one(vec, __ldg(e + 1), v, lim, gs, es);
 }
 
 // the same with the chunk's target lists staged in shared memory (row w of the chunk = tile row j)
@@ -378,15 +386,15 @@ struct PushTab {
   unsigned* gs;
 };
 template <class T>
-__device__ __forceinline__ void push_s(const PushTab& pt, T* vec, int j, int w, int i, T v) {
+__device__ __forceinline__ void push_s(const PushTab& pt, T* vec, int j, int w, int i, T v, int es = 1) {
   int a, b;
   if (i == 0) { const int4 e = pt.twe[w]; a = e.x; b = e.y; }
   else if (i == pt.ni - 1) { const int4 e = pt.twe[w]; a = e.z; b = e.w; }
   else if (j == 0) { const int2 e = pt.ts[i]; a = e.x; b = e.y; }
   else if (j == pt.nj - 1) { const int2 e = pt.tn[i]; a = e.x; b = e.y; }
   else return;
-  push_one(vec, a, v, pt.lim, pt.gs);
-  push_one(vec, b, v, pt.lim, pt.gs);
+  push_one(vec, a, v, pt.lim, pt.gs, es);
+  push_one(vec, b, v, pt.lim, pt.gs, es);
 }
 
 // compact index -> padded index of the same point
@@ -449,25 +457,49 @@ __device__ __forceinline__ Slots slots_of(const GroupDev& g, int inst, const Sme
 struct Lanes {
   double v[4];   // (slot 0, kind 0), (0, 1), (1, 0), (1, 1): always indexed with constants
 };
+// The row sums of a warp's lane partials: for each sum, the xor butterfly over the 32 lanes (lane l adds the
+// partner l ^ o's value for o = 16, 8, 4, 2, 1). With several sums the butterflies share their first levels: at
+// level o a lane keeps half of its sums and hands the other half to its partner, which keeps those (the partner of a
+// lane that keeps sum q keeps q too, so every addition is the one the sum's own butterfly makes: the results are
+// the same bit for bit), so that two sums cost 5 exchanges instead of 10 and four 7 instead of 20 (each exchange of
+// a double is two shuffles). Sum q of 2 ends in lanes 16q..16q+15, of 4 in lanes 8q..8q+7.
+__device__ __forceinline__ double xchg(double v, int o) { return __shfl_xor_sync(0xffffffffu, v, o); }
 __device__ __forceinline__ double butterfly(double v) {
-  for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = add(v, xchg(v, o));
+  return v;
+}
+// two sums: the result of a in lanes 0..15, of b in lanes 16..31
+__device__ __forceinline__ double butterfly2(double a, double b) {
+  const bool lo = (threadIdx.x & 16) == 0;
+  double v = add(lo ? a : b, xchg(lo ? b : a, 16));
+  for (int o = 8; o > 0; o >>= 1) v = add(v, xchg(v, o));
+  return v;
+}
+// four sums: the result of sum q in lanes 8q..8q+7
+__device__ __forceinline__ double butterfly4(double a0, double a1, double a2, double a3) {
+  const bool lo16 = (threadIdx.x & 16) == 0, lo8 = (threadIdx.x & 8) == 0;
+  const double b0 = add(lo16 ? a0 : a2, xchg(lo16 ? a2 : a0, 16));
+  const double b1 = add(lo16 ? a1 : a3, xchg(lo16 ? a3 : a1, 16));
+  double v = add(lo8 ? b0 : b1, xchg(lo8 ? b1 : b0, 8));
+  for (int o = 4; o > 0; o >>= 1) v = add(v, xchg(v, o));
   return v;
 }
 // (two: the pass forms two sums per solve; otherwise the second kind is not read and not reduced)
 __device__ __forceinline__ void row_sums(const GroupDev& g, const Lanes& lp, const Smem& sm, int st, bool two) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const double r0 = butterfly(lp.v[0]), r1 = two ? butterfly(lp.v[1]) : 0.0;
-  double r2 = 0.0, r3 = 0.0;
-  if (g.nrhs > 1) {
-    r2 = butterfly(lp.v[2]);
-    if (two) r3 = butterfly(lp.v[3]);
-  }
-  if (lane == 0) {
-    double* rs = sm.rowsum() + st * 4 * kWarps;
-    rs[0 * kWarps + warp] = r0;
-    rs[1 * kWarps + warp] = r1;
-    rs[2 * kWarps + warp] = r2;
-    rs[3 * kWarps + warp] = r3;
+  double* rs = sm.rowsum() + st * 4 * kMaxWarps + warp;
+  if (g.nrhs > 1 && two) {          // (slot, kind) = (0, 0), (0, 1), (1, 0), (1, 1)
+    const double v = butterfly4(lp.v[0], lp.v[1], lp.v[2], lp.v[3]);
+    if ((lane & 7) == 0) rs[(lane >> 3) * kMaxWarps] = v;
+  } else if (g.nrhs > 1) {          // (0, 0), (1, 0)
+    const double v = butterfly2(lp.v[0], lp.v[2]);
+    if ((lane & 15) == 0) rs[(lane >> 3) * kMaxWarps] = v;
+  } else if (two) {                 // (0, 0), (0, 1)
+    const double v = butterfly2(lp.v[0], lp.v[1]);
+    if ((lane & 15) == 0) rs[(lane >> 4) * kMaxWarps] = v;
+  } else {
+    const double v = butterfly(lp.v[0]);
+    if (lane == 0) rs[0] = v;
   }
 }
 
@@ -485,12 +517,12 @@ __device__ __forceinline__ void accumulate_chunk(const KParams& kp, const GroupD
       for (int w = 0; w < nr; ++w)
         for (int i = 0; i < g.tp.ni; ++i) a = add(a, pr[w * kp.max_ni + i]);   // s = s + a(i,j), j outer
     } else {
-      const double* rs = sm.rowsum() + (st * 4 + lane) * kWarps;
-      double v[kWarps];
+      const double* rs = sm.rowsum() + (st * 4 + lane) * kMaxWarps;
+      double v[kMaxWarps];
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w) v[w] = rs[w];
+      for (int w = 0; w < kMaxWarps; ++w) v[w] = w < nr ? rs[w] : 0.0;
 #pragma unroll
-      for (int w = 0; w < kWarps; ++w)
+      for (int w = 0; w < kMaxWarps; ++w)
         if (w < nr) a = add(a, v[w]);
     }
     sm.uacc()[lane] = a;
@@ -525,7 +557,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
   const int j0 = blk * R, j1 = min(nj, j0 + R);
   const long long pe = g.pad_elems;
   const int W = ni + 2;
-  const int SW = (kWarps + 2) * (kp.max_ni + 2);
+  const int SW = (kp.nw + 2) * (kp.max_ni + 2);
   double* stage = reinterpret_cast<double*>(smem_raw + sm.stage);
   const Slots si = slots_of(g, inst, sm);
   const int ns0 = nsums(pt, si.act(0));
@@ -545,7 +577,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
     const int nrow = j1 - j0;
     const int n_we = 2 * nrow, n_s = (j0 == 0) ? P : 0, n_n = (j1 == nj) ? P : 0;
     const int per = n_we + n_s + n_n;
-    for (int idx = tid; idx < per * g.nrhs * (V_NVEC - 1); idx += kThreads) {
+    for (int idx = tid; idx < per * g.nrhs * (V_NVEC - 1); idx += (int)blockDim.x) {
       const int sv = idx / per, e = idx - (idx / per) * per;
       const int s = sv / (V_NVEC - 1), v = 1 + sv - (sv / (V_NVEC - 1)) * (V_NVEC - 1);
       V* vb = vec_ptr<V>(g, inst, s, v);
@@ -553,17 +585,17 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
       if (e < n_we) o = vidx(tp, t, j0 + (e >> 1), (e & 1) ? ni : -1);
       else if (e < n_we + n_s) o = ((long long)t * (nj + 2)) * P + (e - n_we);
       else o = ((long long)t * (nj + 2) + nj + 1) * P + (e - n_we - n_s);
-      vb[o] = (V)0;
+      vb[o * vstride(g)] = (V)0;
     }
   }
 
-  for (int jc = j0; jc < j1; jc += kWarps) {
-    const int nr = min(kWarps, j1 - jc);
+  for (int jc = j0; jc < j1; jc += kp.nw) {
+    const int nr = min(kp.nw, j1 - jc);
     if (pt == P_INIT) {
       // x0 scaled by rhsNorm at the chunk's rows and neighbours (cg2d.py:227-228): interior points are
       // scaled, unwritten halo points keep cg2d_x
       const int total = (nr + 2) * W;
-      for (int idx = tid; idx < total; idx += kThreads) {
+      for (int idx = tid; idx < total; idx += (int)blockDim.x) {
         const int rr = idx / W, cc = idx - (idx / W) * W;
         const int j = jc + rr - 1, i = cc - 1;
         const bool own = (rr >= 1 && rr <= nr), iin = (i >= 0 && i < ni);
@@ -607,7 +639,8 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
             const double* st = stage + s * SW;
             const int sc = (warp + 1) * W + (i + 1);
             const double vc = st[sc], vw = st[sc - 1], ve = st[sc + 1], vs = st[sc - W], vn = st[sc + W];
-            const long long vo = vidx(tp, t, j, i);
+            const int es = vstride(g);
+            const long long vo = vidx(tp, t, j, i) * es;
             stcg(vec_ptr<double>(g, inst, s, V_X) + vo, vc);
             const double bn = mul(mul(__ldg(g.b[s] + inst * pe + po), si.norm(s)), si.rnorm(s));   // cg2d.py:221,226
             const double ax = op_A<double>(__ldg(aW + po), __ldg(aW + po + 1), __ldg(aS + po), __ldg(aS + po + npx),
@@ -615,7 +648,7 @@ __device__ void process_unit_direct(const KParams& kp, const GroupDev& g, int in
             const V r0 = (V)sub(bn, ax);                                                   // cg2d.py:232
             V* rv = vec_ptr<V>(g, inst, s, V_R0);
             stcg(rv + vo, r0);
-            push(tp, rv, t, j, i, r0, kp.gs);
+            push(tp, rv, t, j, i, r0, kp.gs, es);
             stcg(vec_ptr<V>(g, inst, s, V_S1) + vo, (V)0);                               // s = 0 (cg2d.py:231)
             p0 = mul((double)r0, (double)r0);
             p1 = bn;
@@ -678,14 +711,14 @@ __device__ bool run_pass_direct(const KParams& kp, int pt, const Smem& sm) {
 // x ring cells at the start: the exchanged normalised first guess; unwritten points keep cg2d_x
 // (cg2d.py:227-228). Later values are pushed by the owners as x is updated.
 __device__ void init_x_ring(const KParams& kp, const Smem& sm) {
-  const long long gstride = (long long)gridDim.x * kThreads;
+  const long long gstride = (long long)gridDim.x * blockDim.x;
   for (int gg = 0; gg < kp.ngroups; ++gg) {
     const GroupDev& g = kp.g[gg];
     const TopoDev& tp = g.tp;
     const int T = tp.T, nj = tp.nj, ni = tp.ni;
     const long long per = (long long)T * (2 * nj + 2 * ni);   // W, E [T][nj], S, N [T][ni]
     const long long tot = per * g.count * g.nrhs;
-    for (long long idx = (long long)blockIdx.x * kThreads + threadIdx.x; idx < tot; idx += gstride) {
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < tot; idx += gstride) {
       const long long ins_slot = idx / per;
       const int h = (int)(idx - ins_slot * per);
       const int inst = (int)(ins_slot / g.nrhs), s = (int)(ins_slot - (long long)inst * g.nrhs);
@@ -708,7 +741,7 @@ __device__ void init_x_ring(const KParams& kp, const Smem& sm) {
       const double rn = sm.rnorm()[g.rhs_base + inst * g.nrhs + s];
       const double v = (src >= 0) ? mul(__ldg(x0 + cmp_to_pad(tp, src)), rn)
                                   : __ldg(x0 + ((long long)t * tp.npy + (j + tp.OLy)) * tp.npx + (i + tp.OLx));
-      vec_ptr<double>(g, inst, s, V_X)[vidx(tp, t, j, i)] = v;
+      vec_ptr<double>(g, inst, s, V_X)[vidx(tp, t, j, i) * vstride(g)] = v;
     }
   }
 }
@@ -742,7 +775,7 @@ __device__ void build_unit_table(const KParams& kp, const Smem& sm) {
   const int lo = (int)((long long)blockIdx.x * kp.total_units / gridDim.x);
   const int hi = (int)((long long)(blockIdx.x + 1) * kp.total_units / gridDim.x);
   const int n = kp.unit_deal ? hi - lo : (kp.total_units - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
-  for (int q = threadIdx.x; q < n; q += kThreads) {
+  for (int q = threadIdx.x; q < n; q += (int)blockDim.x) {
     int o = kp.unit_deal ? lo + q : (int)blockIdx.x + q * (int)gridDim.x;
     const bool full = o < nfull;
     if (!full) o -= nfull;
@@ -880,9 +913,11 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
       }
     }
   } else if (lane < 10) {
+    // (paired: slot 0's lanes copy the rows of both solves)
     const int s = (lane - 6) >> 1, v = (lane - 6) & 1;
-    if (s < g.nrhs && (s == 0 ? act0 : act1) && v < L.nvec) {
-      const int sz = L.vsize[v];
+    const bool on = g.pair ? (s == 0 && any) : (s < g.nrhs && (s == 0 ? act0 : act1));
+    if (on && v < L.nvec) {
+      const int sz = L.vsize[v] * (g.pair ? 2 : 1);
       src = vec_ptr<const char>(g, c.inst, s, pass_vector(pt, k, hidx, v)) +
             ((long long)c.t * (nj + 2) + c.jc) * P * sz;
       dst = sb + L.vec[s][v];
@@ -890,10 +925,12 @@ __device__ void issue_chunk(const KParams& kp, const Chunk& c, int pt, int k, in
     }
   } else if (lane < 12) {
     const int s = lane - 10;
-    if (pt == P_S && s < g.nrhs && (s == 0 ? act0 : act1) && sm.has_alpha()[rid0 + s]) {
-      src = vec_ptr<const char>(g, c.inst, s, V_X) + ((long long)c.t * (nj + 2) + c.jc + 1) * P * 8;
+    const bool on = g.pair ? (s == 0 && any) : (s < g.nrhs && (s == 0 ? act0 : act1));
+    if (pt == P_S && on) {   // every S pass (before alpha_{k-1}: x unchanged)
+      const int sz = g.pair ? 16 : 8;
+      src = vec_ptr<const char>(g, c.inst, s, V_X) + ((long long)c.t * (nj + 2) + c.jc + 1) * P * sz;
       dst = sb + L.xo[s];
-      bytes = (unsigned)(c.nr * P * 8);
+      bytes = (unsigned)(c.nr * P * sz);
     }
   }
   const unsigned total = __reduce_add_sync(0xffffffffu, bytes);
@@ -959,7 +996,183 @@ struct RowSet {
   double* vsx;
 };
 
-template <bool MIXED, int MAXM, bool ONE, bool SERIAL>
+// ---- both right-hand sides of an instance at once (MIXED, GroupDev::pair): every vector element is a float2 of the
+// two solves (x a double2), so one shared-memory load, one packed FP32 multiply-add (fma.rn.f32x2) and one store
+// serve both. The arithmetic of each solve is that of compute_chunk's MIXED path, term for term.
+
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// stencil5 (apply_operator / apply_preconditioner terms in the reference's order) on both solves
+__device__ __forceinline__ float2 stencil5p(float c0, float c1, float c2, float c3, float c4, float2 v0, float2 v1,
+                                           float2 v2, float2 v3, float2 v4) {
+  float2 t = mul2(f2(c0), v0);
+  t = fma2(f2(c1), v1, t);
+  t = fma2(f2(c2), v2, t);
+  t = fma2(f2(c3), v3, t);
+  return fma2(f2(c4), v4, t);
+}
+__device__ __forceinline__ void stcg2(float2* p, float2 v) { stcg(p, v); }
+__device__ __forceinline__ void stcg2(double2* p, double2 v) { stcg(p, v); }
+template <class T>
+__device__ __forceinline__ void push_pair(const PushTab& pt, T* vec, int j, int w, int i, T v) {
+  push_s(pt, vec, j, w, i, v);   // an element of the pair vector is the pair itself
+}
+
+template <int MAXM, bool ONE>
+__device__ Lanes compute_pair(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si, int st,
+                              const Smem& sm) {
+  Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
+  const GroupDev& g = group_of<ONE>(kp, c.gi);
+  const TopoDev& tp = g.tp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const StageLay& L = stage_lay<ONE>(kp, c.gi, pt);
+  const unsigned char* sb = smem_raw + sm.stage + st * kp.stage_bytes;
+  const int ni = tp.ni, nj = tp.nj, t = c.t, w = warp, j = c.jc + w;
+  const int P = tp.P, CL = g.ldc, CR = 3 * g.ldc;
+  const long long grow = ((long long)t * (nj + 2) + j + 1) * P + 1 + lane;   // element of (t, j, lane)
+  const bool er = (j == 0) | (j == nj - 1);
+  PushTab ptab;
+  ptab.twe = reinterpret_cast<const int4*>(sb + L.twe);
+  ptab.ts = reinterpret_cast<const int2*>(sb + L.ts);
+  ptab.tn = reinterpret_cast<const int2*>(sb + L.tn);
+  ptab.ni = ni;
+  ptab.nj = nj;
+  ptab.lim = (unsigned)tp.T * (unsigned)(nj + 2) * (unsigned)P;
+  ptab.gs = kp.gs;
+  const float* cw = reinterpret_cast<const float*>(sb + L.coef) + w * CR + lane;
+  const float* cs = cw + CL;
+  const float* cn = cs + CR;
+  const float* cc = cw + 2 * CL;
+  const int off_c = (w + 1) * P + 1 + lane;
+  // rows w, w - 1, w + 1 of the two staged vectors at this lane's column
+  const float2* A = reinterpret_cast<const float2*>(sb + L.vec[0][0]) + off_c;   // z (S), r (X, Z)
+  const float2* B = reinterpret_cast<const float2*>(sb + L.vec[0][1]) + off_c;   // s_{k-1} (S), q_k (X)
+  const float2 *As = A - P, *An = A + P, *Bs = B - P, *Bn = B + P;
+  const double2* XO = reinterpret_cast<const double2*>(sb + L.xo[0]) + w * P + 1 + lane;
+  const float2 coef = make_float2((float)si.c1(0), (float)si.c1(1));   // beta_k (S), alpha_k (X)
+  const double ap0 = si.c2(0), ap1 = si.c2(1);                          // S: alpha_{k-1}
+  const bool up0 = si.has_alpha(0) != 0, up1 = si.has_alpha(1) != 0;
+  float2 *o1, *o2;   // S: s_k, q_k; X: r_{k+1}, z_{k+1}; Z: z (o2)
+  double2* ox = nullptr;
+  if (pt == P_S) {
+    o1 = reinterpret_cast<float2*>(vec_ptr<float>(g, c.inst, 0, (k & 1) ? V_S1 : V_S0));
+    o2 = reinterpret_cast<float2*>(vec_ptr<float>(g, c.inst, 0, V_Q));
+    ox = reinterpret_cast<double2*>(vec_ptr<double>(g, c.inst, 0, V_X));
+  } else {
+    o1 = reinterpret_cast<float2*>(vec_ptr<float>(g, c.inst, 0, ((k + 1) & 1) ? V_R1 : V_R0));
+    o2 = reinterpret_cast<float2*>(vec_ptr<float>(g, c.inst, 0, V_Z));
+  }
+  // this lane's column of the row in the output vectors (the ring pushes take the vectors' bases)
+  float2* const r1 = o1 + grow;
+  float2* const r2 = o2 + grow;
+  double2* const rx = pt == P_S ? ox + grow : nullptr;
+  double a00 = 0.0, a01 = 0.0, a10 = 0.0, a11 = 0.0;   // sums (slot, kind)
+  const bool whole = MAXM > 0 && ni > 32 * (MAXM - 1);
+
+  // one column step: o the lane's column offset from m = 0; valid: the column lies in the row; push: a tile-edge
+  // point (every point of the tile's first and last row, the row's first and last point)
+  auto col = [&](auto pt_tag, int m, int o, bool valid, bool push) {
+    constexpr int PT = decltype(pt_tag)::value;
+    const int i = lane + 32 * m;
+    if constexpr (PT == P_S) {
+      // s_k = z_k + beta_k s_{k-1} (cg2d.py:249) at the point and its neighbours; q_k = A s_k (cg2d.py:251);
+      // x_k = x_{k-1} + alpha_{k-1} s_{k-1} (cg2d.py:254); s_k.q_k (cg2d.py:252)
+      const float2 sp = B[o];
+      const float2 vc = fma2(coef, sp, A[o]);
+      const float2 vw = fma2(coef, B[o - 1], A[o - 1]);
+      const float2 ve = fma2(coef, B[o + 1], A[o + 1]);
+      const float2 vs = fma2(coef, Bs[o], As[o]);
+      const float2 vn = fma2(coef, Bn[o], An[o]);
+      const float2 qv = stencil5p(cw[o], cw[o + 1], cs[o], cn[o], cc[o], vw, ve, vs, vn, vc);
+      const double2 xo = XO[o];
+      double2 xn;
+      xn.x = up0 ? __fma_rn(ap0, (double)sp.x, xo.x) : xo.x;
+      xn.y = up1 ? __fma_rn(ap1, (double)sp.y, xo.y) : xo.y;
+      if (valid) {
+        stcg2(r1 + o, vc);
+        stcg2(r2 + o, qv);
+        stcg2(rx + o, xn);
+        a00 = __fma_rn((double)vc.x, (double)qv.x, a00);
+        a10 = __fma_rn((double)vc.y, (double)qv.y, a10);
+      }
+      if (push) {
+        push_pair(ptab, o1, j, w, i, vc);
+        push_pair(ptab, o2, j, w, i, qv);
+        push_pair(ptab, ox, j, w, i, xn);   // x's neighbours: read by the replacement pass only
+      }
+    } else {
+      // X: r_{k+1} = r_k - alpha_k q_k (cg2d.py:255) at the point and its neighbours; z_{k+1} = M r_{k+1}
+      //    (cg2d.py:245); r.r and z.r (cg2d.py:256, 246).  Z: z = M r and z.r
+      float2 vc, vw, ve, vs, vn;
+      if constexpr (PT == P_X) {
+        const float2 na = make_float2(-coef.x, -coef.y);
+        vc = fma2(na, B[o], A[o]);
+        vw = fma2(na, B[o - 1], A[o - 1]);
+        ve = fma2(na, B[o + 1], A[o + 1]);
+        vs = fma2(na, Bs[o], As[o]);
+        vn = fma2(na, Bn[o], An[o]);
+      } else {
+        vc = A[o]; vw = A[o - 1]; ve = A[o + 1]; vs = As[o]; vn = An[o];
+      }
+      const float2 z = stencil5p(cc[o], cw[o], cw[o + 1], cs[o], cn[o], vc, vw, ve, vs, vn);
+      if (valid) {
+        if constexpr (PT == P_X) stcg2(r1 + o, vc);
+        stcg2(r2 + o, z);
+        if constexpr (PT == P_X) {
+          a00 = __fma_rn((double)vc.x, (double)vc.x, a00);
+          a01 = __fma_rn((double)z.x, (double)vc.x, a01);
+          a10 = __fma_rn((double)vc.y, (double)vc.y, a10);
+          a11 = __fma_rn((double)z.y, (double)vc.y, a11);
+        } else {
+          a00 = __fma_rn((double)z.x, (double)vc.x, a00);
+          a10 = __fma_rn((double)z.y, (double)vc.y, a10);
+        }
+      }
+      if (push) {
+        if constexpr (PT == P_X) push_pair(ptab, o1, j, w, i, vc);
+        push_pair(ptab, o2, j, w, i, z);
+      }
+    }
+  };
+  // the row: whole steps with immediate offsets and no tests; the last (or every) step partial: a lane past the
+  // row reads its last column again and stores and sums nothing
+  auto row = [&](auto pt_tag, auto edge_tag, auto mf_tag) {
+    constexpr bool EDGE = decltype(edge_tag)::value;
+    constexpr int MF = decltype(mf_tag)::value;
+    auto part = [&](int m) {
+      const int i = lane + 32 * m;
+      const bool valid = i < ni;
+      col(pt_tag, m, min(i, ni - 1) - lane, valid, EDGE ? valid : ((i == 0) | (i == ni - 1)));
+    };
+    if constexpr (MF >= 0) {
+#pragma unroll
+      for (int m = 0; m < MF; ++m) {
+        const int i = lane + 32 * m;
+        col(pt_tag, m, 32 * m, true, EDGE || (i == 0) || (i == ni - 1));
+      }
+#pragma unroll
+      for (int m = MF; m < (MAXM > 0 ? MAXM : 1); ++m)
+        if (32 * m < ni) part(m);
+    } else {
+      for (int m = 0; 32 * m < ni; ++m) part(m);
+    }
+  };
+  auto by_edge = [&](auto pt_tag) {
+    using F = std::integral_constant<int, (MAXM > 0 ? MAXM - 1 : 0)>;
+    using G = std::integral_constant<int, -1>;
+    if (er) row(pt_tag, std::true_type{}, G{});
+    else if (whole) row(pt_tag, std::false_type{}, F{});
+    else row(pt_tag, std::false_type{}, G{});
+  };
+  if (pt == P_S) by_edge(std::integral_constant<int, P_S>{});
+  else if (pt == P_X) by_edge(std::integral_constant<int, P_X>{});
+  else by_edge(std::integral_constant<int, P_Z>{});
+  lp.v[0] = a00; lp.v[1] = a01; lp.v[2] = a10; lp.v[3] = a11;
+  return lp;
+}
+
+template <bool MIXED, int MAXM, bool ONE, bool SERIAL, bool WIDE>
 __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k, const Slots& si, int st,
                                const Smem& sm) {
   Lanes lp = {{0.0, 0.0, 0.0, 0.0}};
@@ -994,9 +1207,10 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       if ((s == 0 ? act0 : act1) != A_FIN) continue;
       const V* so = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_S1 : V_S0);
       const double* x = vec_ptr<double>(g, c.inst, s, V_X);
+      const int es = vstride(g);
       for (int i = lane; i < ni; i += 32) {
-        double xv = ldcg(x + grow + i);
-        if (si.has_alpha(s)) xv = A::madd(si.c2(s), (double)ldcg(so + grow + i), xv);
+        double xv = ldcg(x + (grow + i) * es);
+        if (si.has_alpha(s)) xv = A::madd(si.c2(s), (double)ldcg(so + (grow + i) * es), xv);
         const double xf = __ddiv_rn(xv, si.rnorm(s));
         g.x_out[s][prow + i] = xf;
         if (g.x_fortran[s]) g.x_fortran[s][prow + i] = xf;
@@ -1005,6 +1219,9 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   }
   const bool on0 = act0 == A_ACTIVE, on1 = act1 == A_ACTIVE;
   if (!on0 && !on1) return lp;
+  if constexpr (MIXED && !SERIAL) {
+    if (g.pair && pt != P_R) return compute_pair<MAXM, ONE>(kp, c, pt, k, si, st, sm);
+  }
 
   // coefficient rows of this lane's column: W (and the east face at +1), S, N (the south face of row w + 1), C
   const C* cw = reinterpret_cast<const C*>(sb + L.coef) + w * CR + lane;
@@ -1048,14 +1265,24 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
     return q;
   };
 
-  // NS right-hand sides q[0..NS-1]; sums into acc[s][kind]
-  auto run = [&](auto ns_tag, const RowSet<V>* q, double (&acc)[2][2]) {
+  // NS right-hand sides q[0..NS-1] in pass PT (S, X or Z); sums into acc[s][kind]. A separate loop body per pass
+  // kind, right-hand-side count and edge mode, so that the column loop tests none of them:
+  //   EDGE   the tile's first or last row: every point pushes its new values to the rings of the tiles that read it;
+  //   else   only the row's first and last points push (one test per column step, not per right-hand side).
+  // Column steps m < MF are whole (every lane's column lies in the row: offsets are immediates and nothing is
+  // tested); the steps from MF on are partial: a lane past the row's end reads the row's last column again (in
+  // bounds) and stores and sums nothing. MF < 0: every step is partial (any width).
+  auto run = [&](auto ns_tag, auto pt_tag, auto edge_tag, auto mf_tag, const RowSet<V>* q, double (&acc)[2][2]) {
     constexpr int NS = decltype(ns_tag)::value;
-    auto col = [&](int m) {
+    constexpr int PT = decltype(pt_tag)::value;
+    constexpr bool EDGE = decltype(edge_tag)::value;
+    constexpr int MF = decltype(mf_tag)::value;
+    auto col = [&](int m, int o, bool valid) {
       const int i = lane + 32 * m;
-      const int o = 32 * m;
-      const bool edge = er | (i == 0) | (i == ni - 1);
-      if (pt == P_S) {
+      const bool push = EDGE ? valid : ((i == 0) | (i == ni - 1));
+      V v1[NS], v2[NS];      // S: s_k, q_k; X: r_{k+1}, z_{k+1}; Z: z (v2)
+      double xn[NS];         // S: x_k
+      if constexpr (PT == P_S) {
         // s_k = z_k + beta_k s_{k-1} (cg2d.py:249) at the point and its neighbours; q_k = A s_k (cg2d.py:251);
         // x_k = x_{k-1} + alpha_{k-1} s_{k-1} (cg2d.py:254); s_k.q_k (cg2d.py:252)
         const C aw = cw[o], ae = cw[o + 1], as = cs[o], an = cn[o], ac = cc[o];
@@ -1070,23 +1297,22 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
           const V vs = A::madd(be, r.b_s[o], r.a_s[o]);
           const V vn = A::madd(be, r.b_n[o], r.a_n[o]);
           const V qv = stencil5<MIXED, C>(aw, ae, as, an, ac, vw, ve, vs, vn, vc);
-          stcg(r.o1 + o, vc);
-          stcg(r.o2 + o, qv);
-          if constexpr (!MIXED) {
-            if (r.ck) r.ck[o] = (double)vc;                                      // checkpoint s_k
+          // the x update is due once alpha_{k-1} exists; before it x is stored back unchanged
+          const double xo = r.xo[o];
+          const double x1 = r.upd ? A::madd(r.alpha_prev, (double)sp, xo) : xo;
+          if (valid) {
+            stcg(r.o1 + o, vc);
+            stcg(r.o2 + o, qv);
+            stcg(r.ox + o, x1);
+            if constexpr (!MIXED) {
+              if (r.ck) r.ck[o] = (double)vc;                                    // checkpoint s_k
+            }
+            if constexpr (SERIAL) r.pr[o] = mul((double)vc, (double)qv);
+            else acc[s][0] = A::dot((double)vc, (double)qv, acc[s][0]);
           }
-          double xn = 0.0;
-          if (r.upd) {
-            xn = A::madd(r.alpha_prev, (double)sp, r.xo[o]);
-            stcg(r.ox + o, xn);
-          }
-          if (edge) {
-            push_s(ptab, r.vs1, j, w, i, vc);
-            push_s(ptab, r.vs2, j, w, i, qv);
-            if (MIXED && r.upd) push_s(ptab, r.vsx, j, w, i, xn);   // x's neighbours: replacement pass only
-          }
-          if constexpr (SERIAL) r.pr[o] = mul((double)vc, (double)qv);
-          else acc[s][0] = A::dot((double)vc, (double)qv, acc[s][0]);
+          v1[s] = vc;
+          v2[s] = qv;
+          xn[s] = x1;
         }
       } else {
         // X: r_{k+1} = r_k - alpha_k q_k (cg2d.py:255) at the point and its neighbours; z_{k+1} = M r_{k+1}
@@ -1096,7 +1322,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
         for (int s = 0; s < NS; ++s) {
           const RowSet<V>& r = q[s];
           V vc, vw, ve, vs, vn;
-          if (pt == P_X) {
+          if constexpr (PT == P_X) {
             const V na = -r.coef;
             vc = A::madd(na, r.b_c[o], r.a_c[o]);
             vw = A::madd(na, r.b_c[o - 1], r.a_c[o - 1]);
@@ -1107,37 +1333,55 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
             vc = r.a_c[o]; vw = r.a_c[o - 1]; ve = r.a_c[o + 1]; vs = r.a_s[o]; vn = r.a_n[o];
           }
           const V z = stencil5<MIXED, C>(pc, pw, pe_, ps, pn, vc, vw, ve, vs, vn);
-          if (pt == P_X) stcg(r.o1 + o, vc);
-          if constexpr (!MIXED) {
-            if (r.ck) r.ck[o] = (double)vc;                                      // checkpoint r_{k+1}
-          }
-          stcg(r.o2 + o, z);
-          if (edge) {
-            if (pt == P_X) push_s(ptab, r.vs1, j, w, i, vc);
-            push_s(ptab, r.vs2, j, w, i, z);
-          }
-          if constexpr (SERIAL) {
-            if (pt == P_X) {
-              r.pr[o] = mul((double)vc, (double)vc);
-              r.pr[o + kWarps * kp.max_ni] = mul((double)z, (double)vc);
-            } else {
-              r.pr[o] = mul((double)z, (double)vc);
+          if (valid) {
+            if constexpr (PT == P_X) stcg(r.o1 + o, vc);
+            if constexpr (!MIXED) {
+              if (r.ck) r.ck[o] = (double)vc;                                    // checkpoint r_{k+1}
             }
-          } else if (pt == P_X) {
-            acc[s][0] = A::dot((double)vc, (double)vc, acc[s][0]);
-            acc[s][1] = A::dot((double)z, (double)vc, acc[s][1]);
-          } else {
-            acc[s][0] = A::dot((double)z, (double)vc, acc[s][0]);
+            stcg(r.o2 + o, z);
+            if constexpr (SERIAL) {
+              if constexpr (PT == P_X) {
+                r.pr[o] = mul((double)vc, (double)vc);
+                r.pr[o + kWarps * kp.max_ni] = mul((double)z, (double)vc);
+              } else {
+                r.pr[o] = mul((double)z, (double)vc);
+              }
+            } else if constexpr (PT == P_X) {
+              acc[s][0] = A::dot((double)vc, (double)vc, acc[s][0]);
+              acc[s][1] = A::dot((double)z, (double)vc, acc[s][1]);
+            } else {
+              acc[s][0] = A::dot((double)z, (double)vc, acc[s][0]);
+            }
           }
+          v1[s] = vc;
+          v2[s] = z;
+          xn[s] = 0.0;
+        }
+      }
+      // ring pushes of the tile-edge points
+      if (push) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const RowSet<V>& r = q[s];
+          if constexpr (PT != P_Z) push_s(ptab, r.vs1, j, w, i, v1[s]);
+          push_s(ptab, r.vs2, j, w, i, v2[s]);
+          if constexpr (MIXED && PT == P_S) push_s(ptab, r.vsx, j, w, i, xn[s]);   // read by the R pass only
         }
       }
     };
-    if constexpr (MAXM > 0) {
+    // a partial step: lanes past the row read its last column (offset relative to the lane's column at m = 0)
+    auto part = [&](int m) {
+      const int i = lane + 32 * m;
+      col(m, min(i, ni - 1) - lane, i < ni);
+    };
+    if constexpr (MF >= 0) {
 #pragma unroll
-      for (int m = 0; m < MAXM; ++m)
-        if (lane + 32 * m < ni) col(m);
+      for (int m = 0; m < MF; ++m) col(m, 32 * m, true);
+#pragma unroll
+      for (int m = MF; m < (MAXM > 0 ? MAXM : 1); ++m)
+        if (32 * m < ni) part(m);
     } else {
-      for (int m = 0; lane + 32 * m < ni; ++m) col(m);
+      for (int m = 0; 32 * m < ni; ++m) part(m);
     }
   };
 
@@ -1153,20 +1397,22 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
       const V* sk = reinterpret_cast<const V*>(sb + L.vec[s][1]);
       const double alpha = si.c1(s);
       V* r_out = vec_ptr<V>(g, c.inst, s, ((k + 1) & 1) ? V_R1 : V_R0);
+      const int es = vstride(g);   // paired: element e of this solve at scalar 2 e (staged and in the workspace)
       double* pr = SERIAL ? sm.prod() + ((s * 2) * kWarps + w) * kp.max_ni : nullptr;
       auto x1 = [&](double xx, V ss) -> double { return A::madd(alpha, (double)ss, xx); };
       for (int i = lane; i < ni; i += 32) {
         const int rc = (w + 1) * P + i + 1;
-        const double vc = x1(xr[rc], sk[rc]);
-        const double vw = x1(xr[rc - 1], sk[rc - 1]);
-        const double ve = x1(xr[rc + 1], sk[rc + 1]);
-        const double vs = x1(xr[rc - P], sk[rc - P]);
-        const double vn = x1(xr[rc + P], sk[rc + P]);
+        auto X1 = [&](int e) -> double { return x1(xr[e * es], sk[e * es]); };
+        const double vc = X1(rc);
+        const double vw = X1(rc - 1);
+        const double ve = X1(rc + 1);
+        const double vs = X1(rc - P);
+        const double vn = X1(rc + P);
         const int cr = w * NP + col0 + i;
         const double bn = mul(mul(__ldg(g.b[s] + prow + i), si.norm(s)), si.rnorm(s));
         const V r = (V)sub(bn, op_A<double>(aw[cr], aw[cr + 1], as[cr], as[cr + NP], ac[cr], vw, ve, vs, vn, vc));
-        stcg(r_out + grow + i, r);
-        if (er | (i == 0) | (i == ni - 1)) push_s(ptab, r_out, j, w, i, r);
+        stcg(r_out + (grow + i) * es, r);
+        if (er | (i == 0) | (i == ni - 1)) push_s(ptab, r_out, j, w, i, r, es);
         if constexpr (SERIAL) pr[i] = mul((double)r, (double)r);
         else if (s == 0) lp.v[0] = A::dot((double)r, (double)r, lp.v[0]);
         else lp.v[2] = A::dot((double)r, (double)r, lp.v[2]);
@@ -1176,14 +1422,36 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   }
 
   double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+  // whole column steps: all but the last when the row is longer than MAXM - 1 steps (then every lane's column of
+  // those steps lies in the row), none otherwise (a group narrower than the build's width, or any width). WIDE
+  // builds compile the unrolled whole-step loop; the FP64 build for two CTAs per SM does not (its 96 registers a
+  // thread would spill it), and takes the step loop for every row.
+  const bool whole = WIDE && MAXM > 0 && ni > 32 * (MAXM - 1);
+  auto pass_e = [&](auto ns_tag, auto pt_tag, const RowSet<V>* q) {
+    using F = std::integral_constant<int, (MAXM > 0 ? MAXM - 1 : 0)>;
+    using G = std::integral_constant<int, -1>;
+    if (er) {
+      run(ns_tag, pt_tag, std::true_type{}, G{}, q, acc);
+    } else if constexpr (WIDE) {
+      if (whole) run(ns_tag, pt_tag, std::false_type{}, F{}, q, acc);
+      else run(ns_tag, pt_tag, std::false_type{}, G{}, q, acc);
+    } else {
+      run(ns_tag, pt_tag, std::false_type{}, G{}, q, acc);
+    }
+  };
+  auto pass = [&](auto ns_tag, const RowSet<V>* q) {
+    if (pt == P_S) pass_e(ns_tag, std::integral_constant<int, P_S>{}, q);
+    else if (pt == P_X) pass_e(ns_tag, std::integral_constant<int, P_X>{}, q);
+    else pass_e(ns_tag, std::integral_constant<int, P_Z>{}, q);
+  };
   if (on0 && on1) {
     const RowSet<V> q[2] = {rows(0), rows(1)};
-    run(std::integral_constant<int, 2>{}, q, acc);
+    pass(std::integral_constant<int, 2>{}, q);
     lp.v[0] = acc[0][0]; lp.v[1] = acc[0][1]; lp.v[2] = acc[1][0]; lp.v[3] = acc[1][1];
   } else {
     const int s = on0 ? 0 : 1;
     const RowSet<V> q[1] = {rows(s)};
-    run(std::integral_constant<int, 1>{}, q, acc);
+    pass(std::integral_constant<int, 1>{}, q);
     if (s == 0) { lp.v[0] = acc[0][0]; lp.v[1] = acc[0][1]; }
     else { lp.v[2] = acc[0][0]; lp.v[3] = acc[0][1]; }
   }
@@ -1265,7 +1533,7 @@ __device__ bool produce_pass(const KParams& kp, int pt, int k, int hidx, const S
   return ok;
 }
 
-template <bool MIXED, int MAXM, bool ONE, bool SERIAL>
+template <bool MIXED, int MAXM, bool ONE, bool SERIAL, bool WIDE>
 __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, Pipe& pp) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ns = kp.nstage[pt];
@@ -1285,7 +1553,7 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
     const Chunk c = chunk_at(kp, sm, cur.ui, cur.jc);
     const GroupDev& g = group_of<ONE>(kp, c.gi);
     const Slots si = slots_of(g, c.inst, sm);
-    const Lanes lp = compute_chunk<MIXED, MAXM, ONE, SERIAL>(kp, c, pt, k, si, st, sm);
+    const Lanes lp = compute_chunk<MIXED, MAXM, ONE, SERIAL, WIDE>(kp, c, pt, k, si, st, sm);
     if (!SERIAL && warp < c.nr) row_sums(g, lp, sm, st, pt == P_X);
     __syncwarp();
     if (lane == 0) mbar_arrive(&sm.empty()[st]);
@@ -1296,11 +1564,11 @@ __device__ bool consume_pass(const KParams& kp, int pt, int k, const Smem& sm, P
   return true;
 }
 
-template <bool MIXED, int MAXM, bool ONE, bool SERIAL>
+template <bool MIXED, int MAXM, bool ONE, bool SERIAL, bool WIDE>
 __device__ bool run_pass_pipe(const KParams& kp, int pt, int k, int hidx, const Smem& sm, Pipe& pp) {
   bool ok;
-  if ((threadIdx.x >> 5) == kProducer) ok = produce_pass(kp, pt, k, hidx, sm, pp);
-  else ok = consume_pass<MIXED, MAXM, ONE, SERIAL>(kp, pt, k, sm, pp);
+  if ((int)(threadIdx.x >> 5) == kp.nw) ok = produce_pass(kp, pt, k, hidx, sm, pp);
+  else ok = consume_pass<MIXED, MAXM, ONE, SERIAL, WIDE>(kp, pt, k, sm, pp);
   const unsigned long long td = PROF_T0(kp);
   const int bad = __syncthreads_or(!ok);
   PROF_ADD(kp, sm, PR_DRAIN, td);
@@ -1350,8 +1618,8 @@ __device__ void set_actions(const KParams& kp, const Smem& sm, int my_act, doubl
   PROF_ADD(kp, sm, PR_CTRL, t0);
 }
 
-template <bool MIXED, int MAXM, bool ONE, int CPS, bool SERIAL>
-__global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_constant__ KParams kp) {
+template <bool MIXED, int MAXM, bool ONE, int CPS, bool SERIAL, int NT>
+__global__ void __launch_bounds__(NT, CPS) cg2d_persistent(const __grid_constant__ KParams kp) {
   const Smem sm = carve(kp.max_ni, kp.serial);
   const int tid = threadIdx.x;
   unsigned target = (unsigned)kp.test_missing;
@@ -1361,7 +1629,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
   if (tid == 0) {
     for (int s = 0; s < kMaxStages; ++s) {
       mbar_init(&sm.full()[s], 1);          // the producer's arrive (with the copies' byte count)
-      mbar_init(&sm.empty()[s], kWarps);    // one arrive per compute warp
+      mbar_init(&sm.empty()[s], kp.nw);     // one arrive per compute warp
     }
     fence_mbar_init();
   }
@@ -1407,7 +1675,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
   if (own) S->rr = __ldcg(hist_ptr(kp, tid, H_RRR, 0));
   // ---- z = M r and eta for the first iteration
   set_actions(kp, sm, own ? A_ACTIVE : A_NONE, 0.0, 0.0);
-  ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_Z, 0, 0, sm, pp);
+  ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL, (MIXED || CPS == 1)>(kp, P_Z, 0, 0, sm, pp);
   ok = grid_sync(kp, target, P_Z, 0, sm) && ok;
   if (!ok) goto epilogue;
   if (own) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, 0));
@@ -1431,7 +1699,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
     const int any_active = __syncthreads_or(a == A_ACTIVE);
     const int any_fin = __syncthreads_or(a == A_FIN);
     if (!any_active && !any_fin) break;
-    ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_S, k, k, sm, pp);
+    ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL, (MIXED || CPS == 1)>(kp, P_S, k, k, sm, pp);
     ok = grid_sync(kp, target, P_S, k, sm) && ok;
     if (!ok) goto epilogue;
     if (!any_active) break;
@@ -1449,7 +1717,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
     }
     if (__syncthreads_or(ax != A_NONE)) {
       set_actions(kp, sm, ax, own ? S->alpha : 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_X, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL, (MIXED || CPS == 1)>(kp, P_X, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_X, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ax == A_ACTIVE) {
@@ -1459,7 +1727,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
     }
     if (__syncthreads_or(ar != A_NONE)) {
       set_actions(kp, sm, ar, own ? S->alpha : 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_R, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL, (MIXED || CPS == 1)>(kp, P_R, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_R, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) {
@@ -1467,7 +1735,7 @@ __global__ void __launch_bounds__(kThreads, CPS) cg2d_persistent(const __grid_co
         ++S->nrep;
       }
       set_actions(kp, sm, ar, 0.0, 0.0);
-      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL>(kp, P_Z, k, k + 1, sm, pp);
+      ok = run_pass_pipe<MIXED, MAXM, ONE, SERIAL, (MIXED || CPS == 1)>(kp, P_Z, k, k + 1, sm, pp);
       ok = grid_sync(kp, target, P_Z, k + 1, sm) && ok;
       if (!ok) goto epilogue;
       if (ar == A_ACTIVE) S->eta = __ldcg(hist_ptr(kp, tid, H_ETAZ, k + 1));
@@ -1478,13 +1746,13 @@ epilogue:
   // ---- halo points of the outputs: x_out 0; x_fortran = exchanged normalised first guess, unwritten
   //      points keep cg2d_x (cg2d.py:208-210, 227-228)
   {
-    const long long gstride = (long long)gridDim.x * kThreads;
+    const long long gstride = (long long)gridDim.x * blockDim.x;
     for (int gg = 0; gg < kp.ngroups; ++gg) {
       const GroupDev& g = kp.g[gg];
       const TopoDev& tp = g.tp;
       const long long per = g.pad_elems;
       const long long tot = per * g.count * g.nrhs;
-      for (long long idx = (long long)blockIdx.x * kThreads + tid; idx < tot; idx += gstride) {
+      for (long long idx = (long long)blockIdx.x * blockDim.x + tid; idx < tot; idx += gstride) {
         const long long ins_slot = idx / per;
         const long long p = idx - ins_slot * per;
         const int in = (int)(ins_slot / g.nrhs);
@@ -1679,38 +1947,46 @@ static int grid_for(long long work) {
 
 // the kernel instantiation for a launch: precision, the column steps per row (ceil(max_ni / 32), unrolled for
 // tiles up to 96 and 288 points wide), whether the launch has a single group and, FP64, the CTAs per SM it is
-// built for (MIXED: always 2)
+// built for; mixed precision has the 16-warp build (15 compute warps, one CTA per SM) for single-group launches whose
+// 15-row chunks fit, and the 9-warp build (two CTAs per SM) otherwise
 template <bool ONE, int CPS>
-static const void* solver_fn_of(int mixed, int max_ni) {
+static const void* solver_fn_of(int mixed, int nw, int max_ni) {
   if (mixed) {
-    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE, 2, false>;
-    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE, 2, false>;
-    return (const void*)cg2d_persistent<true, 0, ONE, 2, false>;
+    if (ONE && nw == kMixedWarps) {
+      if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, true, 1, false, kMixedThreads>;
+      return (const void*)cg2d_persistent<true, 0, true, 1, false, kMixedThreads>;
+    }
+    if (max_ni <= 96) return (const void*)cg2d_persistent<true, 3, ONE, 2, false, kThreads>;
+    if (max_ni <= 288) return (const void*)cg2d_persistent<true, 9, ONE, 2, false, kThreads>;
+    return (const void*)cg2d_persistent<true, 0, ONE, 2, false, kThreads>;
   }
-  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE, CPS, false>;
-  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE, CPS, false>;
-  return (const void*)cg2d_persistent<false, 0, ONE, CPS, false>;
+  if (max_ni <= 96) return (const void*)cg2d_persistent<false, 3, ONE, CPS, false, kThreads>;
+  if (max_ni <= 288) return (const void*)cg2d_persistent<false, 9, ONE, CPS, false, kThreads>;
+  return (const void*)cg2d_persistent<false, 0, ONE, CPS, false, kThreads>;
 }
 static const void* solver_fn(const KParams& kp) {
   // the FORTRAN sum order (bitwise parity, not speed): one generic build per precision
-  if (kp.serial) return kp.mixed ? (const void*)cg2d_persistent<true, 0, false, 2, true>
-                                 : (const void*)cg2d_persistent<false, 0, false, 1, true>;
+  if (kp.serial) return kp.mixed ? (const void*)cg2d_persistent<true, 0, false, 2, true, kThreads>
+                                 : (const void*)cg2d_persistent<false, 0, false, 1, true, kThreads>;
   const bool two = !kp.mixed && kp.fp64_cps == 2;
-  if (kp.ngroups == 1) return two ? solver_fn_of<true, 2>(kp.mixed, kp.max_ni) : solver_fn_of<true, 1>(kp.mixed, kp.max_ni);
-  return two ? solver_fn_of<false, 2>(kp.mixed, kp.max_ni) : solver_fn_of<false, 1>(kp.mixed, kp.max_ni);
+  if (kp.ngroups == 1)
+    return two ? solver_fn_of<true, 2>(kp.mixed, kp.nw, kp.max_ni) : solver_fn_of<true, 1>(kp.mixed, kp.nw, kp.max_ni);
+  return two ? solver_fn_of<false, 2>(kp.mixed, kp.nw, kp.max_ni) : solver_fn_of<false, 1>(kp.mixed, kp.nw, kp.max_ni);
 }
+
+int solver_threads(const KParams& kp) { return (kp.nw + 1) * 32; }
 
 cudaError_t solver_occupancy(const KParams& kp, size_t smem, int* blocks_per_sm) {
   const void* fn = solver_fn(kp);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, kThreads, smem);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, fn, solver_threads(kp), smem);
 }
 
 cudaError_t launch_solver(const KParams& kp, int grid, size_t smem, cudaStream_t stream) {
   const void* fn = solver_fn(kp);
   void* args[] = {const_cast<KParams*>(&kp)};
-  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream);
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(solver_threads(kp)), args, smem, stream);
 }
 
 cudaError_t launch_pack_coef(const GroupDev& g, int mixed, cudaStream_t stream) {
