@@ -81,8 +81,9 @@ typedef struct {
                           0 = round-robin (default), 1 = contiguous runs. Like grid_ctas and ctas_per_sm it moves
                           work between CTAs only: every sum is formed in the same fixed order, so results are the
                           same bit for bit whatever the schedule (the autotuner's search space) */
-  int stages;          /* depth of the copy pipeline of a CTA: 0 = 2 (default), or 2..4 stage buffers; deeper
-                          pipelines need more shared memory per CTA (fewer CTAs per SM). Also results-neutral */
+  int stages;          /* depth of the copy pipeline of a CTA: 0 = the default (3 on the 16-warp mixed build, else
+                          2), or 2..4 stage buffers, capped at what fits on the 16-warp build; deeper pipelines need
+                          more shared memory per CTA (fewer CTAs per SM). Also results-neutral */
 } cg2d_params_t;
 
 /* Per-solve diagnostics: the diag dict of cg2d_fortran (cg2d.py:267-268) plus a status. */

@@ -75,8 +75,11 @@ cg2d_status_t check_params(const cg2d_params_t* p) {
 }
 
 // mixed precision with two right-hand sides in the ROWBLOCK order keeps both solves of an instance interleaved
-// (GroupDev::pair)
-inline int paired(int mixed, int serial, int nrhs) { return mixed && !serial && nrhs == 2 ? 1 : 0; }
+// (GroupDev::pair) in single-group launches (the builds for several groups leave the paired path out: its
+// registers would make them spill)
+inline int paired(int mixed, int serial, int nrhs, int ngroups) {
+  return mixed && !serial && nrhs == 2 && ngroups == 1 ? 1 : 0;
+}
 
 // chunk height and stage buffers for nw compute warps: the largest chunk (nw rows; with 8 warps 8, else 4 rows)
 // whose `ns` stage buffers fit
@@ -89,7 +92,7 @@ cg2d_status_t size_stages(const cg2d_group_t* gr, int ng, int mixed, int serial,
     for (int g = 0; g < ng; ++g) {
       const cg2d_topology* tp = gr[g].topo;
       const int npx = tp->sNx + 2 * tp->OLx;
-      const int pair = paired(mixed, serial, gr[g].nrhs);
+      const int pair = paired(mixed, serial, gr[g].nrhs, ng);
       for (int pt : {P_S, P_X, P_Z}) {
         const StageLay S = stage_layout(pt, mixed, ch, gr[g].nrhs, tp->sNx, npx, pair);
         if (S.total > hot) hot = S.total;
@@ -145,10 +148,12 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
   // chunks fit: blocks (work units) of kMixedWarps rows, one chunk each, with the deepest pipeline up to the one
   // asked for that fits (so that the pipeline depth, a schedule option, never changes the sum order). Otherwise 8
   // compute warps and rows_per_block rows.
+  // (default depth: 3 stages on the 16-warp build, where one CTA per SM leaves the room, 2 elsewhere)
   const int ns = p->stages ? p->stages : 2;
   cg2d_status_t st = CG2D_UNSUPPORTED;
   if (mixed && !serial && ng == 1) {
-    for (int n = ns; n >= 2 && st != CG2D_OK; --n) st = size_stages(gr, ng, mixed, serial, n, kMixedWarps, L);
+    for (int n = p->stages ? p->stages : 3; n >= 2 && st != CG2D_OK; --n)
+      st = size_stages(gr, ng, mixed, serial, n, kMixedWarps, L);
     if (st == CG2D_OK) L->rpb = kMixedWarps;
   }
   if (st != CG2D_OK) {
@@ -186,7 +191,7 @@ cg2d_status_t compute_layout(const cg2d_group_t* gr, int ng, const cg2d_params_t
     const cg2d_topology* tp = gr[g].topo;
     // ringed vector tiles [T][sNy+2][P]; paired: one block per instance with both solves in every element
     const long long elems = (long long)tp->nTiles * (tp->sNy + 2) * vec_pitch(tp->sNx);
-    const int pair = paired(mixed, serial, gr[g].nrhs), per = pair ? 2 : 1;
+    const int pair = paired(mixed, serial, gr[g].nrhs, ng), per = pair ? 2 : 1;
     long long off = 0;
     L->vec_off[g][V_X] = off; off += (long long)al(sizeof(double) * per * elems);
     for (int v = 1; v < V_NVEC; ++v) { L->vec_off[g][v] = off; off += (long long)al(vsz * per * elems); }
@@ -422,7 +427,7 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
     const cg2d_topology* tp = groups[g].topo;
     for (int pt = 0; pt < P_NPASS; ++pt)
       kp.lay[g][pt] = stage_layout(pt, kp.mixed, L.ch, groups[g].nrhs, tp->sNx, tp->sNx + 2 * tp->OLx,
-                                   paired(kp.mixed, kp.serial, groups[g].nrhs));
+                                   paired(kp.mixed, kp.serial, groups[g].nrhs, ngroups));
   }
   int unit_base = 0, op_base = 0, rhs_base = 0;
   for (int g = 0; g < ngroups; ++g) {
@@ -455,7 +460,7 @@ static cg2d_status_t solve_groups_impl(const cg2d_group_t* groups, int ngroups, 
     }
     d.vec = ws + L.vec[g];
     d.vec_stride = L.vec_stride[g];
-    d.pair = paired(kp.mixed, kp.serial, G.nrhs);
+    d.pair = paired(kp.mixed, kp.serial, G.nrhs, ngroups);
     for (int v = 0; v < V_NVEC; ++v) d.vec_off[v] = L.vec_off[g][v];
     unit_base += G.count * d.units;
     op_base += G.count;

@@ -15,6 +15,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "cg2d_internal.cuh"
 
 namespace cg2d {
@@ -46,38 +48,65 @@ __device__ __forceinline__ bool interior(const TopoDev& tp, const Pt& p) {
   const int pe_ = (tp).T * (tp).npy * (tp).npx;                                            \
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pe_; q += gridDim.x * blockDim.x)
 
+// Asynchronous 8-byte copies global -> shared (cp.async), counted per thread in commit groups: the level loops
+// below stream their per-level fields a few levels ahead of use through shared memory, each thread copying and
+// later reading only its own slots (so the copies need no block barrier).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // aW2d, aS2d on j, i = 1..sNy+1, 1..sNx+1 (0 elsewhere): sum over k = 1..Nr in order of
-// ((dyG drF(k)) hFacW(k)) recip_dxC, then times cg2dNorm, implicSurfPress, implicDiv2DFlow (:41-47)
-__global__ void k_update_faces(TopoDev tp, int Nr, const double* hFacW, const double* hFacS, const double* drF,
-                               const double* dyG, const double* dxG, const double* rdxC, const double* rdyC,
-                               double norm, const double* norm_arr, double isp, double idf, double* aW2d,
-                               double* aS2d) {
+// ((dyG drF(k)) hFacW(k)) recip_dxC, then times cg2dNorm, implicSurfPress, implicDiv2DFlow (:41-47). One thread per
+// padded point (blockIdx.x blocks of kUfThreads cover an instance, blockIdx.y = instance); hFacW and hFacS stream
+// kUfStages levels ahead of the ordered sums.
+constexpr int kUfThreads = 256, kUfStages = 8;
+constexpr size_t kUfSmem = sizeof(double) * kUfStages * 2 * kUfThreads;
+__global__ void __launch_bounds__(kUfThreads) k_update_faces(TopoDev tp, int Nr, const double* hFacW,
+                                                             const double* hFacS, const double* drF, const double* dyG,
+                                                             const double* dxG, const double* rdxC, const double* rdyC,
+                                                             double norm, const double* norm_arr, double isp,
+                                                             double idf, double* aW2d, double* aS2d) {
+  extern __shared__ double stage[];   // [kUfStages][2][kUfThreads]: hFacW, hFacS
   const int in = blockIdx.y;
   const int plane = tp.npy * tp.npx;
+  const int q = blockIdx.x * kUfThreads + threadIdx.x;
+  if (q >= tp.T * plane) return;
   const long long o2 = (long long)in * tp.T * plane;
-  FOR_Q(tp) {
-    const Pt p = decode(tp, q);
-    double w = 0.0, s = 0.0;
-    if (p.j >= 0 && p.j <= tp.nj && p.i >= 0 && p.i <= tp.ni) {
-      const long long b3 = ((long long)in * tp.T + p.t) * Nr * plane + (q - p.t * plane);
-      const double* __restrict__ hw = hFacW + b3;
-      const double* __restrict__ hs = hFacS + b3;
-      const double dy = dyG[q], dx = dxG[q], rx = rdxC[q], ry = rdyC[q];
-      // unrolled so that several levels' loads are in flight while the ordered sums proceed
-#pragma unroll 5
-      for (int k = 0; k < Nr; ++k) {
-        const double d = __ldg(drF + k);
-        const double hwk = __ldg(hw + (long long)k * plane), hsk = __ldg(hs + (long long)k * plane);
-        w = add(w, mul(mul(mul(dy, d), hwk), rx));
-        s = add(s, mul(mul(mul(dx, d), hsk), ry));
+  const Pt p = decode(tp, q);
+  const bool face = p.j >= 0 && p.j <= tp.nj && p.i >= 0 && p.i <= tp.ni;
+  double w = 0.0, s = 0.0;
+  if (face) {
+    const long long b3 = ((long long)in * tp.T + p.t) * Nr * plane + (q - p.t * plane);
+    const double* hw = hFacW + b3;
+    const double* hs = hFacS + b3;
+    auto slot = [&](int k, int f) { return stage + ((k % kUfStages) * 2 + f) * kUfThreads + threadIdx.x; };
+    auto issue = [&](int k) {   // level k into its stage (one commit group, maybe empty)
+      if (k < Nr) {
+        cp_async8(slot(k, 0), hw + (long long)k * plane);
+        cp_async8(slot(k, 1), hs + (long long)k * plane);
       }
-      const double nrm = norm_arr ? norm_arr[in] : norm;
-      w = mul(mul(mul(w, nrm), isp), idf);
-      s = mul(mul(mul(s, nrm), isp), idf);
+      cp_async_commit();
+    };
+    for (int k = 0; k < kUfStages; ++k) issue(k);
+    const double dy = dyG[q], dx = dxG[q], rx = rdxC[q], ry = rdyC[q];
+    for (int k = 0; k < Nr; ++k) {
+      cp_async_wait<kUfStages - 1>();   // level k's group (the oldest pending) has landed
+      const double d = __ldg(drF + k);
+      const double hwk = *slot(k, 0), hsk = *slot(k, 1);
+      issue(k + kUfStages);             // into the stage just read
+      w = add(w, mul(mul(mul(dy, d), hwk), rx));
+      s = add(s, mul(mul(mul(dx, d), hsk), ry));
     }
-    aW2d[o2 + q] = w;
-    aS2d[o2 + q] = s;
+    const double nrm = norm_arr ? norm_arr[in] : norm;
+    w = mul(mul(mul(w, nrm), isp), idf);
+    s = mul(mul(mul(s, nrm), isp), idf);
   }
+  aW2d[o2 + q] = w;
+  aS2d[o2 + q] = s;
 }
 
 struct DiagArgs {
@@ -130,8 +159,24 @@ struct RhsArgs {
   const double *gU, *gV, *hFacW, *hFacS, *EmPmR, *etaN, *etaH;   // per instance
   const double *drF, *dyG, *dxG, *rA, *maskInC, *Bo_surf;         // shared
   double tmpFac, fsf, dTm, dTfs;
+  double rdTm;   // RN(1 / deltaTMom) for div_fixed, or 0 (deltaTMom outside [2^-64, 2^64]: plain divisions)
   int fresh_water, Nr;
 };
+
+// a / b correctly rounded (the IEEE quotient, bit for bit) for a divisor b fixed over the launch, given y = RN(1/b):
+// q = RN(a y) is within an ulp of a / b, the remainder r = a - q b is exact by FMA, and RN(q + r y) is RN(a / b)
+// when y is within half an ulp of 1 / b (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Dev. 34 (1990) 111-119; J.-M. Muller et al., Handbook of Floating-Point
+// Arithmetic, the division section). Intermediates stay normal for 2^-900 <= |a| <= 2^900 and 2^-64 <= |b| <= 2^64;
+// zero returns the exact signed zero a y, anything else (tiny, huge, inf, NaN, y = 0) takes the division itself.
+// One multiply and two FMAs in place of a division: the level loop of k_rhs does two per face and level.
+__device__ __forceinline__ double div_fixed(double a, double b, double y) {
+  if (a == 0.0) return mul(a, y);
+  const double m = fabs(a);
+  if (!(m >= 0x1p-900 && m <= 0x1p900) || y == 0.0) return dvd(a, b);
+  const double q = mul(a, y);
+  return __fma_rn(__fma_rn(-q, b, a), y, q);
+}
 
 // cg2d_x = Bo_surf etaN everywhere (:76); cg2d_b = 0 on halos (the interior is k_rhs's)
 __global__ void k_rhs_fill(TopoDev tp, const double* Bo_surf, const double* etaN, double* cg2d_b, double* cg2d_x) {
@@ -152,11 +197,20 @@ __global__ void k_rhs_fill(TopoDev tp, const double* Bo_surf, const double* etaN
 // A block of 32 lanes x kRhsRows rows owns 31 columns x (kRhsRows - 1) rows of points; its last lane and last row
 // only form faces (the east / north faces of the block's points; the next block owns their points). The terms are
 // the same floating-point operations on the same operands whichever thread forms them, so the sums are the
-// reference's bit for bit, with about 2.2 divisions per point and level instead of 4.
+// reference's bit for bit, with about 2.2 divisions per point and level instead of 4, each by deltaTMom and so
+// formed by div_fixed.
 constexpr int kRhsRows = 8;
 constexpr int kRhsCols = 31, kRhsOwnRows = kRhsRows - 1;   // points a block owns
+// The four face fields of a level stream through shared memory kRhsStages levels ahead of their use: each thread
+// copies its own four values with asynchronous 8-byte copies (cp.async, one commit group per level) and reads back
+// only what it copied, so the copies need no block barrier; the level chain itself (ordered sums, one barrier per
+// level) then never waits on a load issued less than kRhsStages levels earlier.
+constexpr int kRhsStages = 5;
+constexpr size_t kRhsSmem = sizeof(double) * kRhsStages * 4 * kRhsRows * 32;
+
 __global__ void __launch_bounds__(32 * kRhsRows, 4) k_rhs(TopoDev tp, RhsArgs A, double* cg2d_b) {
-  __shared__ double pvs[2][kRhsRows][32];
+  __shared__ double pvs[2][2][kRhsRows][32];   // [pair buffer][level of the pair][row][lane]
+  extern __shared__ double stage[];   // [kRhsStages][4][kRhsRows][32]: hFacW, gU, hFacS, gV
   const int in = blockIdx.z;
   const int nrb = (tp.nj + kRhsOwnRows - 1) / kRhsOwnRows;   // row blocks per tile
   const int t = blockIdx.y / nrb, jb = blockIdx.y - t * nrb;
@@ -168,36 +222,58 @@ __global__ void __launch_bounds__(32 * kRhsRows, 4) k_rhs(TopoDev tp, RhsArgs A,
   const int q = t * plane + (j + tp.OLy) * tp.npx + i + tp.OLx;   // padded point (in bounds when face)
   const long long o = (long long)in * tp.T * plane;
   const long long b3 = ((long long)in * tp.T + t) * A.Nr * plane + (q - t * plane);
-  const double dTm = A.dTm;
+  const double dTm = A.dTm, rdTm = A.rdTm;
   const double dyc = face ? A.dyG[q] : 0.0, dxc = face ? A.dxG[q] : 0.0;
   double b = 0.0;
   if (own && A.fresh_water) b = mul(dvd(mul(mul(A.tmpFac, A.rA[q]), A.EmPmR[o + q]), A.dTm), A.maskInC[q]);
-  // the level's face fractions and transports, loaded one level ahead of their use (the level loop is a chain of
-  // ordered sums with a block barrier per level, so the next level's loads are put in flight before it)
-  double hw = 0.0, u = 0.0, hs = 0.0, v = 0.0;
-  auto load = [&](int k) {
-    if (face) {
+  // this thread's slot of field f in stage s
+  auto slot = [&](int s, int f) { return stage + ((s * 4 + f) * kRhsRows + y) * 32 + lane; };
+  auto issue = [&](int k) {   // level k's four values into stage k % kRhsStages (one commit group, maybe empty)
+    if (face && k >= 0) {
       const long long c = b3 + (long long)k * plane;
-      hw = __ldg(A.hFacW + c); u = __ldg(A.gU + c); hs = __ldg(A.hFacS + c); v = __ldg(A.gV + c);
+      const int s = k % kRhsStages;
+      cp_async8(slot(s, 0), A.hFacW + c);
+      cp_async8(slot(s, 1), A.gU + c);
+      cp_async8(slot(s, 2), A.hFacS + c);
+      cp_async8(slot(s, 3), A.gV + c);
     }
+    cp_async_commit();
   };
-  load(A.Nr - 1);
-  for (int k = A.Nr - 1; k >= 0; --k) {                                       // :95-101, k = Nr..1
-    const double hw0 = hw, u0 = u, hs0 = hs, v0 = v;
-    if (k > 0) load(k - 1);
-    const double d = __ldg(A.drF + k);
-    double pu0 = 0.0, pv0 = 0.0;
+  for (int s = 0; s < kRhsStages; ++s) issue(A.Nr - 1 - s);
+  // level k's two face terms from its stage (waiting for its copies), then its stage refilled with level k - stages
+  auto terms = [&](int k, double& pu, double& pv) {
+    cp_async_wait<kRhsStages - 1>();   // level k's group (the oldest pending) has landed
+    pu = 0.0;
+    pv = 0.0;
     if (face) {
-      pu0 = dvd(mul(mul(mul(dyc, d), hw0), u0), dTm);                                        // :90, :92
-      pv0 = dvd(mul(mul(mul(dxc, d), hs0), v0), dTm);                                        // :91, :93
+      const double d = __ldg(A.drF + k);
+      const int s = k % kRhsStages;
+      const double hw0 = *slot(s, 0), u0 = *slot(s, 1), hs0 = *slot(s, 2), v0 = *slot(s, 3);
+      pu = div_fixed(mul(mul(mul(dyc, d), hw0), u0), dTm, rdTm);                             // :90, :92
+      pv = div_fixed(mul(mul(mul(dxc, d), hs0), v0), dTm, rdTm);                             // :91, :93
     }
-    const int buf = k & 1;
-    pvs[buf][y][lane] = pv0;
-    const double pu1 = __shfl_down_sync(0xffffffffu, pu0, 1);
+    issue(k - kRhsStages);   // into the stage just read (this thread's own slots, read above)
+  };
+  // two levels per block barrier: their south-face terms through shared memory (double-buffered by pair), their
+  // west-face terms by shuffle, then the sums of both in order
+  for (int k = A.Nr - 1, pair = 0; k >= 0; k -= 2, ++pair) {                  // :95-101, k = Nr..1
+    double pua, pva, pub = 0.0, pvb = 0.0;
+    terms(k, pua, pva);
+    const bool two = k >= 1;
+    if (two) terms(k - 1, pub, pvb);
+    const int buf = pair & 1;
+    pvs[buf][0][y][lane] = pva;
+    pvs[buf][1][y][lane] = pvb;
+    const double pua1 = __shfl_down_sync(0xffffffffu, pua, 1);
+    const double pub1 = __shfl_down_sync(0xffffffffu, pub, 1);
     __syncthreads();
     if (own) {
-      b = sub(add(b, pu1), pu0);                                                              // :97
-      b = sub(add(b, pvs[buf][y + 1][lane]), pv0);                                            // :98
+      b = sub(add(b, pua1), pua);                                                             // :97, level k
+      b = sub(add(b, pvs[buf][0][y + 1][lane]), pva);                                         // :98
+      if (two) {
+        b = sub(add(b, pub1), pub);                                                           // level k - 1
+        b = sub(add(b, pvs[buf][1][y + 1][lane]), pvb);
+      }
     }
   }
   if (own) {
@@ -282,9 +358,13 @@ dim3 grid_of(const TopoDev& tp, int batch) {
 cudaError_t pressure_update(const TopoDev& tp, const UpdateArgs& U, cudaStream_t st) {
   if (U.batch < 1 || U.batch > 65535 || U.Nr < 1) return cudaErrorInvalidValue;
   const dim3 g = grid_of(tp, U.batch);
-  k_update_faces<<<g, 256, 0, st>>>(tp, U.Nr, U.hFacW, U.hFacS, U.drF, U.dyG, U.dxG, U.recip_dxC, U.recip_dyC,
-                                    U.norm, U.norm_arr, U.implicSurfPress, U.implicDiv2DFlow, U.aW2d, U.aS2d);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaFuncSetAttribute(k_update_faces, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUfSmem);
+  if (e != cudaSuccess) return e;
+  const dim3 gf((unsigned)((tp.T * tp.npy * tp.npx + kUfThreads - 1) / kUfThreads), (unsigned)U.batch);
+  k_update_faces<<<gf, kUfThreads, kUfSmem, st>>>(tp, U.Nr, U.hFacW, U.hFacS, U.drF, U.dyG, U.dxG, U.recip_dxC,
+                                                  U.recip_dyC, U.norm, U.norm_arr, U.implicSurfPress,
+                                                  U.implicDiv2DFlow, U.aW2d, U.aS2d);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   DiagArgs D;
   D.aW2d = U.aW2d;
@@ -309,6 +389,10 @@ cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st) {
   A.tmpFac = R.freeSurfFac * R.mass2rUnit * R.implicDiv2DFlow;     // :79, formed once as the reference does
   A.fsf = R.freeSurfFac;
   A.dTm = R.deltaTMom;
+  {
+    const double m = std::fabs(R.deltaTMom);
+    A.rdTm = (m >= 0x1p-64 && m <= 0x1p64) ? 1.0 / R.deltaTMom : 0.0;   // host IEEE division: RN(1 / deltaTMom)
+  }
   A.dTfs = R.deltaTFreeSurf;
   A.fresh_water = R.useRealFreshWaterFlux;
   A.Nr = R.Nr;
@@ -317,7 +401,9 @@ cudaError_t pressure_rhs(const TopoDev& tp, const RhsIn& R, cudaStream_t st) {
   if (e != cudaSuccess) return e;
   const int nrb = (tp.nj + kRhsOwnRows - 1) / kRhsOwnRows;
   const dim3 grid((unsigned)((tp.ni + kRhsCols - 1) / kRhsCols), (unsigned)(tp.T * nrb), (unsigned)R.batch);
-  k_rhs<<<grid, dim3(32, kRhsRows), 0, st>>>(tp, A, R.cg2d_b);
+  e = cudaFuncSetAttribute(k_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRhsSmem);
+  if (e != cudaSuccess) return e;
+  k_rhs<<<grid, dim3(32, kRhsRows), kRhsSmem, st>>>(tp, A, R.cg2d_b);
   return cudaGetLastError();
 }
 

@@ -1219,7 +1219,7 @@ __device__ Lanes compute_chunk(const KParams& kp, const Chunk& c, int pt, int k,
   }
   const bool on0 = act0 == A_ACTIVE, on1 = act1 == A_ACTIVE;
   if (!on0 && !on1) return lp;
-  if constexpr (MIXED && !SERIAL) {
+  if constexpr (MIXED && !SERIAL && ONE) {
     if (g.pair && pt != P_R) return compute_pair<MAXM, ONE>(kp, c, pt, k, si, st, sm);
   }
 
