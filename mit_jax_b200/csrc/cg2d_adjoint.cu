@@ -180,6 +180,38 @@ __device__ double fold(const Geo& G, int R, const double* rs, double* sh) {
   return total;
 }
 
+// The folds of rs0 and rs1 side by side, by the whole thread block: the same additions in the same order as two
+// calls of fold, with both sets of block sums and tile sums formed at once and the two totals by two warps. sh holds
+// 2 T (ceil(nj / R) + 1) doubles. Both totals are valid in thread 0.
+__device__ void fold2(const Geo& G, int R, const double* rs0, const double* rs1, double* sh, double& f0, double& f1) {
+  const int T = G.tp.T, nj = G.tp.nj, nb = (nj + R - 1) / R, per = T * (nb + 1);
+  for (int u = threadIdx.x; u < 2 * T * nb; u += blockDim.x) {
+    const int q = u >= T * nb, w = u - q * T * nb;
+    const int t = w / nb, j0 = (w - t * nb) * R, j1 = min(nj, j0 + R);
+    const double* rs = q ? rs1 : rs0;
+    double v = 0.0;
+    for (int j = j0; j < j1; ++j) v = add(v, rs[t * nj + j]);
+    sh[q * per + w] = v;
+  }
+  __syncthreads();
+  for (int u = threadIdx.x; u < 2 * T; u += blockDim.x) {
+    const int q = u >= T, t = u - q * T;
+    double ts = 0.0;
+    for (int b = 0; b < nb; ++b) ts = add(ts, sh[q * per + t * nb + b]);
+    sh[q * per + T * nb + t] = ts;
+  }
+  __syncthreads();
+  const int q = threadIdx.x == 0 ? 0 : (threadIdx.x == 32 ? 1 : -1);
+  double total = 0.0;
+  if (q >= 0)
+    for (int t = 0; t < T; ++t) total = add(total, sh[q * per + T * nb + t]);
+  __syncthreads();
+  if (q == 1) sh[0] = total;
+  __syncthreads();
+  f0 = total;
+  f1 = sh[0];
+}
+
 // per-instance scalar steps, one thread block per instance (blockIdx.x), thread 0 updating the scalars;
 // S = scalar arrays [kind][Kmax][batch]
 struct Scal {
@@ -213,8 +245,8 @@ __global__ void k_rev_alpha(Geo G, int R, const double* rs, Scal S, const int* K
   const int in = blockIdx.x;
   if (!live(K, in, k)) return;
   const int rows = G.tp.T * G.tp.nj;
-  const double f0 = fold(G, R, rs + (long long)in * 2 * rows, sh);
-  const double f1 = fold(G, R, rs + ((long long)in * 2 + 1) * rows, sh);
+  double f0, f1;
+  fold2(G, R, rs + (long long)in * 2 * rows, rs + ((long long)in * 2 + 1) * rows, sh, f0, f1);
   if (threadIdx.x != 0) return;
   const double abar = f0 - f1;
   const long long o = (long long)k * G.batch + in;
@@ -668,7 +700,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
   const int gi = (A.batch + 127) / 128, nbk = (tp.nj + A.rows_per_block - 1) / A.rows_per_block;
   const size_t fold_sh = sizeof(double) * (size_t)tp.T * (nbk + 1);
   const size_t row_sh = sizeof(double) * 2 * kRows * bp.x * bp.y;   // row_sums: two products per point
-  if (fold_sh > 48 * 1024) return cudaErrorInvalidValue;
+  if (fold_sh > 24 * 1024) return cudaErrorInvalidValue;   // (k_rev_alpha takes two side by side)
   const size_t vb = vecn * sizeof(double);
   cudaError_t e;
 #define CK(x)                              \
@@ -749,7 +781,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
     LK();
     for (int m = len - 1; m >= 0; --m) {
       const int k = c0 + m;
-      k_rev_alpha<<<A.batch, 256, fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
+      k_rev_alpha<<<A.batch, 256, 2 * fold_sh, st>>>(G, A.rows_per_block, rs, S, K, k);
       LK();
       k_rq<<<gm, bp, row_sh, st>>>(G, A.aW, A.aS, A.aC, sg_s[m], sg_q[m], xbar, rbar, sbar, sp(m), qb0 + m * vstr,
                                    rs, S, K, k);
