@@ -576,20 +576,20 @@ __global__ void k_xout(Geo G, const double* x, const double* rn, double* out) {
 // alpha, beta, eta, sigma of every iteration from a forward solve's sum history (one group of one right-hand side:
 // solve index = instance): eta_0 = z.r of the first Z pass, eta_k (k >= 1) = z.r of pass X_{k-1}, sigma_k = s.q
 // of pass S_k; beta_k = eta_k / eta_{k-1} (eta_{-1} = 1) and alpha_k = eta_k / sigma_k with the solver's divisions
+// One thread block per instance (blockIdx.x), its threads over the iterations: every k is independent, since
+// eta_{k-1} is read from the history rather than carried.
 __global__ void k_hist_scalars(Geo G, const double* hist, int hist_len, Scal S, const int* K) {
-  const int in = blockIdx.x * blockDim.x + threadIdx.x;
-  if (in >= G.batch) return;
+  const int in = blockIdx.x;
   const double* h = hist + (size_t)in * H_NKIND * hist_len;
-  double eta_prev = 1.0;
-  for (int k = 0; k < K[in]; ++k) {
-    const double eta = k == 0 ? h[(size_t)H_ETAZ * hist_len] : h[(size_t)H_ETAX * hist_len + k];
+  auto eta_of = [&](int k) { return k == 0 ? h[(size_t)H_ETAZ * hist_len] : h[(size_t)H_ETAX * hist_len + k]; };
+  for (int k = threadIdx.x; k < K[in]; k += blockDim.x) {
+    const double eta = eta_of(k), eta_prev = k > 0 ? eta_of(k - 1) : 1.0;
     const double sig = h[(size_t)H_SQ * hist_len + k];
     const long long o = (long long)k * G.batch + in;
     S.eta[o] = eta;
     S.beta[o] = __ddiv_rn(eta, eta_prev);
     S.sig[o] = sig;
     S.alpha[o] = __ddiv_rn(eta, sig);
-    eta_prev = eta;
   }
 }
 
@@ -725,7 +725,7 @@ cudaError_t exact_adjoint(const TopoDev& tp, const ExactArgs& A, void* ws, cudaS
     CK(cudaMemsetAsync(ck_s[0], 0, vb, st));
     k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, ck_r[0], x);
     LK();
-    k_hist_scalars<<<gi, 128, 0, st>>>(G, A.hist, A.hist_len, S, K);
+    k_hist_scalars<<<A.batch, 256, 0, st>>>(G, A.hist, A.hist_len, S, K);
     LK();
   } else {
     k_init<<<gp, bp, 0, st>>>(G, A.aW, A.aS, A.aC, A.b, A.x0, nrm, rn, r, x);
